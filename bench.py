@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the fine-scale kick (PM3 + PP) on B200.
+
+One step = one full fine-scale kick (PM3 fine-mesh force + PP short-range
+force + velocity update) over the whole image of the chosen workload
+(default ``clustered256``: ~16.8M clustered particles, 512^3 PM3 mesh, PP
+cutoff 2 fine cells; see cube2_b200/workloads.py).
+
+* ``value``   particle kicks/s with the inputs resident in HBM
+  (cube_kick_fine_device), K steps timed with CUDA events on the launching
+  stream, max over ranks; every rank runs its own replica (the kick of one
+  image runs on one GPU; N > 1 = independent replicas).
+* ``e2e``     the same metric through the host C-ABI (cube_kick_fine) with
+  pinned host buffers: every step uploads xp/vp/rhoc/idx_b_r and downloads vp.
+* ``roofline`` the PP force kernel (FP32 CUDA cores): 38 FLOP per accepted
+  ordered pair (pairs counted for this input) / its average launch time,
+  against the FP32 FMA peak measured in the same run.
+* ``cpu_baseline`` / ``--impl reference``: the reference's own CPU PP kernel
+  (pp_force_kernel.c, built from the reference sources into oracle/_ref) plus
+  the CPU restatement of the reference PM3 on the same inputs.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "particle kicks/s (PM3+PP) on 1 B200, learned vs plain at equal rms force error"
+UNIT = "particle-kicks/s"
+PP_FLOP_PER_PAIR = 38  # 3 sub, 5 r^2, rsqrt, 1/r^2, 2 ep, 18 polynomial+reciprocal, 1 diff, 1 scale, 6 accumulate
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="clustered256")
+    ap.add_argument("--truth-targets", type=int, default=10000)
+    ap.add_argument("--no-truth", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks during the timed region
+
+
+class Clocks:
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = []
+        for ln in out.splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            if self.uuid and f[0] != self.uuid:
+                continue
+            rows.append(f)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------------------
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from cube2_b200 import workloads as W
+    from cube2_b200.kick import FineKick, force_truth_fp64
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev)
+    w = W.WORKLOADS[args.workload]
+    img = W.make(args.workload)
+    L = img.layout
+    isort, ires, ix, apm3, rs = W.tables(args.workload)
+    fk = FineKick(L, apm3f=w["apm3f"])
+    N = img.n_particles
+    a_mid, dt = np.float32(6 * np.pi), np.float32(1.0)  # dv = force
+
+    d_rhoc = torch.from_numpy(img.rhoc.reshape(-1).copy()).to(dev)
+    d_idx = torch.from_numpy(img.idx_b_r.reshape(-1).copy()).to(dev)
+    d_xp = torch.from_numpy(img.xp.reshape(-1).copy()).to(dev)
+    vp0 = torch.from_numpy(img.vp.reshape(-1).copy()).to(dev)
+    d_vp = vp0.clone()
+    d_out = torch.zeros(8, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def kick():
+        fk.kick_fine_device(d_rhoc, d_idx, d_xp, img.n_used, d_vp, d_out, isort, ires, ix, apm3, rs, 1.0, a_mid,
+                            dt, stream=stream)
+
+    # algorithmic work of the dominant kernel and the FP32 denominator
+    pairs = fk.pp_pair_count(img, ires, ix, apm3, rs)
+    fp32_peak = fk.fp32_peak_tflops()
+
+    for _ in range(max(args.warmup, 0)):
+        kick()
+    torch.cuda.synchronize()
+    err_word = int(d_out[5:6].cpu().view(torch.int32).item())
+    if err_word:
+        raise RuntimeError(f"device error mask {err_word}")
+    fk.enable_timing(True)
+    fk.timing_read()
+    launches0 = fk.launch_count()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = Clocks(uuid)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        kick()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    launches = fk.launch_count() - launches0
+    stages = fk.timing_read()
+    fk.enable_timing(False)
+    if world > 1:
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_step = ms / max(args.steps, 1)
+    value = N * world * args.steps / (ms * 1e-3)
+
+    # e2e through the host C-ABI with pinned buffers
+    e2e = None
+    if not args.no_e2e:
+        def pinned(a):
+            t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+            return t.numpy()
+        from cube2_b200.layout import Image
+        himg = Image(L, pinned(img.xp), pinned(img.vp), pinned(img.rhoc), pinned(img.idx_b_r), img.pid, img.active,
+                     N)
+        vp_host = pinned(img.vp.copy())
+        fk.kick_fine(himg, isort, ires, ix, apm3, rs, 1.0, a_mid, dt, vp=vp_host)  # warm
+        if world > 1:
+            dist.barrier()
+        te = time.perf_counter()
+        for _ in range(args.steps):
+            fk.kick_fine(himg, isort, ires, ix, apm3, rs, 1.0, a_mid, dt, vp=vp_host)
+        te = time.perf_counter() - te
+        if world > 1:
+            tt = torch.tensor([te], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        h2d = img.xp.nbytes + img.vp.nbytes + img.rhoc.nbytes + img.idx_b_r.nbytes
+        d2h = img.vp.nbytes + 24
+        e2e = {"value": N * world * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * te / args.steps}
+
+    # force error against the FP64 direct sum (outside the timed region)
+    truth = None
+    if not args.no_truth and rank == 0:
+        d_vp.copy_(vp0 * 0)
+        kick()
+        torch.cuda.synchronize()
+        v = d_vp.cpu().numpy().reshape(-1, 3).astype(np.float64)
+        kick_coef = float(np.float32(a_mid * dt / np.float32(6.0))) / np.pi
+        act = np.nonzero(img.active)[0]
+        rng = np.random.default_rng(12345)
+        samp = rng.choice(act, min(args.truth_targets, act.size), replace=False)
+        pos = W.physical_positions(img)
+        t_tr = time.perf_counter()
+        Ft = force_truth_fp64(pos, float(L.ng), L.app, img.pid[samp])
+        t_tr = time.perf_counter() - t_tr
+        F = v[samp] / kick_coef
+        dF = np.linalg.norm(F - Ft, axis=1)
+        Fm = np.linalg.norm(Ft, axis=1)
+        truth = {"rms_rel": float(np.sqrt(np.sum(dF ** 2) / np.sum(Fm ** 2))),
+                 "p99_rel": float(np.percentile(dF / np.maximum(Fm, 1e-30), 99)),
+                 "targets": int(samp.size), "truth": "FP64 Ewald-split periodic direct sum", "seconds": t_tr}
+
+    pm3_ms = float(np.mean(stages[:, 0])) if len(stages) else None
+    ppb_ms = float(np.mean(stages[:, 1])) if len(stages) else None
+    ppf_ms = float(np.mean(stages[:, 2])) if len(stages) else None
+    flops = PP_FLOP_PER_PAIR * pairs
+    achieved = flops / (ppf_ms * 1e-3) / 1e12 if ppf_ms else None
+    roofline = {"kernel": "k_pp_force (PP pair force + kick)", "bound": "fp32", "achieved": achieved,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": (achieved / fp32_peak) if achieved else None,
+                "peak_source": "FP32 FMA probe measured in this run (MEASURED_PEAKS.json has no FP32 figure)",
+                "flops_per_launch": int(flops), "pairs_per_launch": int(pairs), "traffic": None}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference(args.workload, img, sample=True)
+        except Exception as e:  # the baseline must not hide our number
+            cpu = {"error": repr(e)}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32 (int16 fixed-point positions, fp64 Green table)",
+            "data": "synthetic (seeded lognormal Poisson sample; see cube2_b200/workloads.py)",
+            "config": {"workload": args.workload, "particles": N, "n_used_stored": img.n_used,
+                       "pm3_mesh": L.ng * w["rsf"], "pp_cutoff_fine_cells": w["apm3f"] / w["rsf"],
+                       "softening_fine_cells": L.app, "assignment": "TSC", "variant": "plain (no learned shell)",
+                       "layout": L.as_dict(), "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (mesh 512^3 fp32 = 537 MB, particle arrays > 120 MB)"},
+            "stages_ms": {"pm3": pm3_ms, "pp_binning_and_worklist": ppb_ms, "pp_force": ppf_ms},
+            "roofline": roofline, "force_error": truth, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": ck, "cpu_baseline": cpu}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------------------------------------
+# reference CPU path (the baseline leg and the reference arm)
+
+
+def _nnest_for_host():
+    n = os.cpu_count() or 1
+    best = 8
+    for k in (8, 16, 32, 64, 128, 256):
+        if k <= n:
+            best = k
+    return best
+
+
+def cpu_reference(workload: str, img, sample: bool, tile: int = 0):
+    """Time the reference CPU PP kernel + the PM3 restatement on the host cores.
+
+    sample=True times the PP of one parent tile (`tile`, z-major index) and
+    scales it by that tile's share of the interior particles."""
+    from cube2_b200 import workloads as W
+    from cube2_b200.kick import green_table
+    from oracle import oracle as O
+    w = W.WORKLOADS[workload]
+    L = img.layout
+    isort, ires, ix, apm3, rs = W.tables(workload)
+    nnest = _nnest_for_host()
+    ref = O.RefPP(L, nnest=nnest)
+    a_mid, dt = np.float32(6 * np.pi), np.float32(1.0)
+    ntile = L.nnt ** 3
+    t = time.perf_counter()
+    if sample and ntile > 1:
+        # one parent tile of the image, scaled by its share of the interior particles
+        tile = tile % ntile
+        txyz = (tile % L.nnt, (tile // L.nnt) % L.nnt, tile // (L.nnt * L.nnt))
+        out = ref.tile(img, txyz, int(ires[0]), apm3, rs, 1.0, a_mid, dt)
+        t_pp = (time.perf_counter() - t) * (img.n_particles / max(out["ncount"], 1))
+        pp_sample = f"pp_force_kernel.c c_pp_force_kernel_tile on tile {tile} of {ntile} ({out['ncount']} " \
+                    f"particles), scaled by particle share"
+    else:
+        ref.kick(img, [int(ires[0])] * ntile, apm3, rs, 1.0, a_mid, dt)
+        t_pp = time.perf_counter() - t
+        pp_sample = f"pp_force_kernel.c c_pp_force_kernel over all {ntile} tiles"
+    n = L.ng * w["rsf"]
+    G = green_table(n, w["apm3f"], 0.0, 1.0 / w["rsf"]) if _has_gpu() else O.green(n, w["apm3f"], 0.0,
+                                                                                    1.0 / w["rsf"])
+    t = time.perf_counter()
+    O.pm3_periodic(img, w["rsf"], G, 1.0, a_mid, dt, fft_dtype=np.float32)
+    t_pm3 = time.perf_counter() - t
+    value = img.n_particles / (t_pp + t_pm3)
+    return {"value": value, "unit": UNIT, "cores": int(os.cpu_count() or 1), "kind": "reference",
+            "pp_threads": nnest, "pm3_kind": "port", "seconds_pp": t_pp, "seconds_pm3": t_pm3,
+            "sample": f"{pp_sample}; PM3 restatement of kick.f90 pm_thread on the full {n}^3 periodic mesh "
+                      f"(scipy pocketfft float32 standing in for sfftw)"}
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from cube2_b200 import workloads as W
+    img = W.make(args.workload)
+    times = []
+    res = None
+    for s in range(args.warmup + args.steps):
+        # each step samples the next parent tile, so K steps cover the image
+        res = cpu_reference(args.workload, img, sample=True, tile=s)
+        if s >= args.warmup:
+            times.append(img.n_particles / res["value"])
+    sec = float(np.mean(times)) if times else float("nan")
+    value = img.n_particles / sec
+    w = W.WORKLOADS[args.workload]
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": args.workload, "particles": img.n_particles, "pm3_mesh": img.layout.ng * w["rsf"],
+                       "pp_cutoff_fine_cells": w["apm3f"] / w["rsf"], "softening_fine_cells": img.layout.app},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
+                             "sample": res["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank, world, local_rank = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

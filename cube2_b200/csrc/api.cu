@@ -1,0 +1,1127 @@
+// C-ABI of the library: the reference-named entry points bound by kick.f90:12-46
+// and finalize.f90:8-13, their status-returning variants, the fused kick and
+// the inspection calls.  Owns the device context (buffers grown on demand and
+// kept between kicks, cuFFT plans, Green tables), like the reference's static
+// workspaces (pp_force_kernel.cu:467-494, pm3_fft_cuda.cu:56-71), but never
+// aborts: every failure becomes a status code.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace cube {
+
+static thread_local int t_last_error = CUBE_OK;
+
+struct Buf {
+  void *p = nullptr;
+  size_t cap = 0;
+};
+
+struct GreenEntry {
+  int n;
+  float apm_soft, apm_range, gridsize;
+  int p;
+  float *d;
+};
+
+struct HostGreen {  // caller's table cached by pointer and size (pm3_fft_cuda.cu:153-175)
+  const float *host;
+  size_t count;
+  float *d;
+};
+
+struct Plan {
+  int n, batch;
+  cufftType type;
+  cufftHandle h;
+};
+
+struct Ctx {
+  bool configured = false;
+  cube_layout pub{};
+  Lay L{};
+  int device = -1;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  Buf xp, rhoc, idx, vp, cell_base;
+  Buf tiles, count, cell_start, scan_tmp, spos, spill, spill_rank, counters, items, range_loc;
+  Buf rho, rhok, fk, force, dtab, jobs, out;
+  int dtab_n = -1;
+  void *h_stage = nullptr;  // pinned staging for small tables
+  size_t h_stage_cap = 0;
+  float *h_out = nullptr;   // pinned [8]: out[5], err
+  std::vector<GreenEntry> greens;
+  std::vector<HostGreen> hgreens;
+  std::vector<Plan> plans;
+  // Stage events of the last kRing timed calls.  Per call: 0 start, 1 after PM3,
+  // 2 PP start, 4 after the PP force kernel, 5 end, 6 after the PP work list.
+  static constexpr int kRing = 256;
+  cudaEvent_t ring[kRing][7] = {};
+  bool ring_pm3[kRing] = {}, ring_pp[kRing] = {};
+  int ring_cur = 0, ring_next = 0, ring_count = 0;
+  bool timing = false;
+  float stage_ms[4] = {0, 0, 0, 0};
+  long long launches = 0;  // kernels of this library enqueued so far
+  cudaEvent_t stage_ev = nullptr;  // recorded after the last staged upload of a call
+  bool stage_pending = false;
+};
+
+static Ctx g;
+static std::mutex g_mu;
+
+static int fail(int code) {
+  t_last_error = code;
+  return code;
+}
+
+#define CU(x)                                                                          \
+  do {                                                                                 \
+    cudaError_t e_ = (x);                                                              \
+    if (e_ != cudaSuccess) {                                                           \
+      if (getenv("CUBE_VERBOSE"))                                                      \
+        fprintf(stderr, "cube2_b200: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return fail(CUBE_ERR_CUDA);                                                      \
+    }                                                                                  \
+  } while (0)
+
+#define CF(x)                                                                          \
+  do {                                                                                 \
+    cufftResult r_ = (x);                                                              \
+    if (r_ != CUFFT_SUCCESS) {                                                         \
+      if (getenv("CUBE_VERBOSE")) fprintf(stderr, "cube2_b200: %s failed: %d\n", #x, (int)r_); \
+      return fail(CUBE_ERR_CUFFT);                                                     \
+    }                                                                                  \
+  } while (0)
+
+#define CK(x)                    \
+  do {                           \
+    int s_ = (x);                \
+    if (s_ != CUBE_OK) return s_; \
+  } while (0)
+
+static int grow(Buf &b, size_t bytes) {
+  if (bytes <= b.cap) return CUBE_OK;
+  size_t want = std::max(bytes, b.cap + b.cap / 4);
+  if (b.p) {
+    CU(cudaStreamSynchronize(g.stream));
+    CU(cudaFree(b.p));
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  CU(cudaMalloc(&b.p, want));
+  b.cap = want;
+  return CUBE_OK;
+}
+
+static void release(Buf &b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+// Device binding per process, as c_select_gpu_for_image (pp_force_kernel.cu:80-128)
+// does: the node-local rank picks the device when several are visible.
+static int local_rank() {
+  const char *vars[] = {"MPI_LOCALRANKID", "OMPI_COMM_WORLD_LOCAL_RANK", "SLURM_LOCALID", "PMI_LOCAL_RANK",
+                        "LOCAL_RANK"};
+  for (const char *v : vars) {
+    const char *s = getenv(v);
+    if (s) return atoi(s);
+  }
+  return 0;
+}
+
+static int ensure_device() {
+  if (g.device >= 0) {
+    CU(cudaSetDevice(g.device));
+    return CUBE_OK;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) return fail(CUBE_ERR_NO_DEVICE);
+  const int dev = count == 1 ? 0 : local_rank();
+  if (dev < 0 || dev >= count) return fail(CUBE_ERR_NO_DEVICE);
+  CU(cudaSetDevice(dev));
+  g.device = dev;
+  CU(cudaDeviceGetAttribute(&g.num_sms, cudaDevAttrMultiProcessorCount, dev));
+  CU(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+  CU(cudaMallocHost(&g.h_out, sizeof(float) * 8));
+  for (auto &slot : g.ring)
+    for (auto &e : slot) CU(cudaEventCreate(&e));
+  CU(cudaEventCreateWithFlags(&g.stage_ev, cudaEventDisableTiming));
+  return CUBE_OK;
+}
+
+static int stage(size_t bytes) {
+  if (bytes <= g.h_stage_cap) return CUBE_OK;
+  if (g.h_stage) {
+    CU(cudaStreamSynchronize(g.stream));
+    CU(cudaFreeHost(g.h_stage));
+  }
+  g.h_stage_cap = std::max(bytes, (size_t)1 << 20);
+  CU(cudaMallocHost(&g.h_stage, g.h_stage_cap));
+  return CUBE_OK;
+}
+
+// upload a small host table through the pinned staging area (offset in bytes)
+template <class T>
+static int upload(Buf &dst, const T *src, size_t count, size_t &stage_off) {
+  const size_t bytes = sizeof(T) * count;
+  CK(grow(dst, bytes > 0 ? bytes : 16));
+  if (!bytes) return CUBE_OK;
+  stage_off = (stage_off + 255) & ~(size_t)255;
+  if (stage_off + bytes > g.h_stage_cap) return fail(CUBE_ERR_CAPACITY);
+  memcpy((char *)g.h_stage + stage_off, src, bytes);
+  CU(cudaMemcpyAsync(dst.p, (char *)g.h_stage + stage_off, bytes, cudaMemcpyHostToDevice, g.stream));
+  stage_off += bytes;
+  return CUBE_OK;
+}
+
+static int get_plan(int n, int batch, cufftType type, cufftHandle *out) {
+  for (auto &p : g.plans)
+    if (p.n == n && p.batch == batch && p.type == type) {
+      CF(cufftSetStream(p.h, g.stream));
+      *out = p.h;
+      return CUBE_OK;
+    }
+  Plan p{n, batch, type, 0};
+  int dims[3] = {n, n, n};
+  CF(cufftPlanMany(&p.h, 3, dims, nullptr, 1, 0, nullptr, 1, 0, type, batch));
+  CF(cufftSetStream(p.h, g.stream));
+  g.plans.push_back(p);
+  *out = p.h;
+  return CUBE_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// metadata
+
+struct Meta {
+  std::vector<int> ires_loc, owner;  // by subtile location
+  std::vector<float> range_loc;
+  std::vector<TilePP> tiles;
+  int64_t ncells = 0;
+  int max_rcp = 1;
+};
+
+static inline int loc_of(const Lay &L, int sx, int sy, int sz, int tx, int ty, int tz) {
+  return (((tz * L.nnt + ty) * L.nnt + tx) * L.nns + sz) * L.nns * L.nns + sy * L.nns + sx;
+}
+
+// validate and reorder the per-subtile tables by location (pp_force_kernel.cu:987-1004)
+static int build_meta(const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf, const float *apm3,
+                      Meta &m) {
+  const Lay &L = g.L;
+  if (!ires || !ixyz3 || !ratio_sf) return fail(CUBE_ERR_INVALID);
+  m.ires_loc.assign(L.ns3, -1);
+  m.owner.assign(L.ns3, -1);
+  m.range_loc.assign(L.ns3, 0.f);
+  for (int it = 0; it < L.ns3; it++) {
+    const int *r = ixyz3 + 6 * it;
+    const int sx = r[0] - 1, sy = r[1] - 1, sz = r[2] - 1, tx = r[3] - 1, ty = r[4] - 1, tz = r[5] - 1;
+    if (sx < 0 || sx >= L.nns || sy < 0 || sy >= L.nns || sz < 0 || sz >= L.nns || tx < 0 || tx >= L.nnt ||
+        ty < 0 || ty >= L.nnt || tz < 0 || tz >= L.nnt || ires[it] < 2 || ires[it] > 6)
+      return fail(CUBE_ERR_INVALID);
+    const int loc = loc_of(L, sx, sy, sz, tx, ty, tz);
+    if (m.owner[loc] >= 0) return fail(CUBE_ERR_INVALID);
+    m.ires_loc[loc] = ires[it];
+    m.owner[loc] = it;
+    if (apm3) m.range_loc[loc] = apm3[ires[it] - 1];
+  }
+  for (int l = 0; l < 7; l++)
+    if (ratio_sf[l] < 1 || ratio_sf[l] > 64) return fail(CUBE_ERR_INVALID);
+  m.tiles.resize(L.ntile);
+  int64_t cell0 = 0;
+  m.max_rcp = 1;
+  for (int t = 0; t < L.ntile; t++) {
+    int rcp = ratio_sf[1];
+    const int nss = L.nns * L.nns * L.nns;
+    for (int q = 0; q < nss; q++) rcp = std::max(rcp, ratio_sf[m.ires_loc[t * nss + q] - 1]);
+    TilePP tp;
+    tp.rcp = rcp;
+    tp.S = rcp * (L.nt + 2);
+    tp.cell0 = cell0;
+    cell0 += (int64_t)tp.S * tp.S * tp.S;
+    m.tiles[t] = tp;
+    m.max_rcp = std::max(m.max_rcp, rcp);
+  }
+  m.ncells = cell0;
+  if (m.ncells >= ((int64_t)1 << 31)) return fail(CUBE_ERR_CAPACITY);
+  return CUBE_OK;
+}
+
+// particles kicked per subtile = particles of its interior coarse cells (pm3_fft_cuda.cu:437,
+// pp_force_kernel.cu:705-710), written by subtile index it
+static void fill_ptotal(const Meta &m, const int32_t *rhoc, double *ptotal) {
+  const Lay &L = g.L;
+  for (int loc = 0; loc < L.ns3; loc++) {
+    const int nss = L.nns * L.nns * L.nns;
+    const int t = loc / nss, s = loc % nss;
+    const int sx = s % L.nns, sy = (s / L.nns) % L.nns, sz = s / (L.nns * L.nns);
+    double c = 0;
+    for (int k = 0; k < L.ntt; k++)
+      for (int j = 0; j < L.ntt; j++)
+        for (int i = 0; i < L.ntt; i++) {
+          const int ci = L.ncb + sx * L.ntt + i, cj = L.ncb + sy * L.ntt + j, ck = L.ncb + sz * L.ntt + k;
+          c += rhoc[(((int64_t)t * L.nte + ck) * L.nte + cj) * L.nte + ci];
+        }
+    ptotal[m.owner[loc]] = c;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// pipeline stages (device pointers in ctx buffers or caller's)
+
+struct Dev {
+  const int16_t *xp;
+  const int32_t *rhoc;
+  const int64_t *idx;
+  float *vp;
+  int64_t n_used;
+};
+
+static int get_green_periodic(int n, int rsf, float **out) {
+  const Lay &L = g.L;
+  const float gs = 1.0f / (float)rsf;
+  for (auto &e : g.greens)
+    if (e.n == n && e.apm_soft == L.apm3f && e.apm_range == L.apm_range && e.gridsize == gs && e.p == L.p_order) {
+      *out = e.d;
+      return CUBE_OK;
+    }
+  GreenEntry e{n, L.apm3f, L.apm_range, gs, L.p_order, nullptr};
+  CU(cudaMalloc(&e.d, sizeof(float) * (size_t)n * n * (n / 2 + 1)));
+  launch_green_fp64(n, L.apm3f, L.apm_range, gs, L.p_order, e.d, g.stream);
+  CU(cudaGetLastError());
+  g.greens.push_back(e);
+  *out = e.d;
+  return CUBE_OK;
+}
+
+static int get_green_host(const float *host, int n, float **out) {
+  const size_t count = (size_t)n * n * (n / 2 + 1);
+  for (auto &e : g.hgreens)
+    if (e.host == host && e.count == count) {
+      *out = e.d;
+      return CUBE_OK;
+    }
+  HostGreen e{host, count, nullptr};
+  CU(cudaMalloc(&e.d, sizeof(float) * count));
+  CU(cudaMemcpy(e.d, host, sizeof(float) * count, cudaMemcpyHostToDevice));
+  g.hgreens.push_back(e);
+  *out = e.d;
+  return CUBE_OK;
+}
+
+// spectral symbol of potential_to_force: D(k) = a sin k + (1-a) sin 2k / 2 with a = real(4) 4/3
+// (parameters.f90:49-50); 0 at k = 0 and at the Nyquist frequency
+static int get_dtab(int n) {
+  CK(grow(g.dtab, sizeof(float) * n));
+  if (g.dtab_n == n) return CUBE_OK;
+  std::vector<float> d(n);
+  const double a = (double)(4.0f / 3.0f), pi = 3.14159265358979323846;
+  for (int w = 0; w < n; w++) {
+    const int m = w < (n + 1) / 2 ? w : w - n;
+    if (m == 0 || (n % 2 == 0 && m == -n / 2)) {
+      d[w] = 0.f;
+      continue;
+    }
+    const double th = 2.0 * pi * (double)m / (double)n;
+    d[w] = (float)(a * sin(th) + (1 - a) * sin(2 * th) / 2);
+  }
+  CU(cudaMemcpy(g.dtab.p, d.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  g.dtab_n = n;
+  return CUBE_OK;
+}
+
+static const int kFftBuckets[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512};
+
+static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, const float *const *gk,
+                   const Dev &d, float mass, float kick, bool want_vmax, size_t &soff) {
+  const Lay &L = g.L;
+  if (L.pm3_mode == CUBE_PM3_PERIODIC) {
+    const int rsf = ratio_sf[m.ires_loc[0] - 1];
+    for (int q = 0; q < L.ns3; q++)
+      if (ratio_sf[m.ires_loc[q] - 1] != rsf) return fail(CUBE_ERR_INVALID);
+    const int n = L.ng * rsf;
+    const int64_t n3 = (int64_t)n * n * n, nk = (int64_t)n * n * (n / 2 + 1);
+    float *G = nullptr;
+    CK(get_green_periodic(n, rsf, &G));
+    CK(get_dtab(n));
+    CK(grow(g.rho, sizeof(float) * n3));
+    CK(grow(g.rhok, sizeof(cufftComplex) * nk));
+    CK(grow(g.fk, sizeof(cufftComplex) * nk * 3));
+    CK(grow(g.force, sizeof(float) * n3 * 3));
+    const double scale = (double)L.rcs / (double)(1.0f / (float)rsf);
+    std::vector<MeshJob> jobs(L.ntile);
+    for (int t = 0; t < L.ntile; t++) {
+      const int tx = t % L.nnt, ty = (t / L.nnt) % L.nnt, tz = t / (L.nnt * L.nnt);
+      MeshJob &J = jobs[t];
+      J.t = t;
+      J.slot = 0;
+      J.range = 0.f;
+      const int tc[3] = {tx, ty, tz};
+      for (int q = 0; q < 3; q++) {
+        J.lo[q] = L.ncb;
+        J.alo[q] = L.ncb;
+        J.off[q] = -(double)tc[q] * L.nt * scale;
+      }
+    }
+    CK(upload(g.jobs, jobs.data(), jobs.size(), soff));
+    PM3Args a{};
+    a.L = &g.L;
+    a.rsf = rsf;
+    a.n = n;
+    a.nslots = 1;
+    a.jobs = (const MeshJob *)g.jobs.p;
+    a.njobs = L.ntile;
+    for (int q = 0; q < 3; q++) a.rdep[q] = a.ract[q] = L.nt;
+    a.wrap = 1;
+    a.shift = 0;
+    a.fphys_lo = 0;
+    a.fphys_n = n;
+    a.scale = scale;
+    a.xp = d.xp;
+    a.rhoc = d.rhoc;
+    a.cell_base = (const int64_t *)g.cell_base.p;
+    a.rho = (float *)g.rho.p;
+    a.rhok = (cufftComplex *)g.rhok.p;
+    a.fk = (cufftComplex *)g.fk.p;
+    a.force = (float *)g.force.p;
+    a.green = G;
+    a.dtab = (const float *)g.dtab.p;
+    a.mass = mass;
+    a.kick = kick;
+    a.vp = d.vp;
+    a.out = (float *)g.out.p;
+    a.want_vmax = want_vmax;
+    cufftHandle fw, bw;
+    CK(get_plan(n, 1, CUFFT_R2C, &fw));
+    CK(get_plan(n, 3, CUFFT_C2R, &bw));
+    CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3, g.stream));
+    launch_pm3_deposit(a, g.stream);
+    CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
+    launch_pm3_kspace(a, g.stream);
+    CF(cufftExecC2R(bw, (cufftComplex *)g.fk.p, (cufftReal *)g.force.p));
+    launch_pm3_f2max(a, g.stream);
+    launch_pm3_gather(a, g.stream);
+    g.launches += 4;
+    CU(cudaGetLastError());
+    return CUBE_OK;
+  }
+  // buffered subtile meshes grouped by level (pm3_fft_cuda.cu:553-591)
+  for (int lev = 2; lev <= 6; lev++) {
+    std::vector<int> locs;
+    for (int q = 0; q < L.ns3; q++)
+      if (m.ires_loc[q] == lev) locs.push_back(q);
+    if (locs.empty()) continue;
+    if (!gk || !gk[lev - 2]) return fail(CUBE_ERR_INVALID);
+    const int rsf = ratio_sf[lev - 1];
+    const int nfp = L.ntt * L.rcs * rsf, nfb = L.rcs * rsf, n = nfp + 2 * nfb;
+    const int64_t n3 = (int64_t)n * n * n, nk = (int64_t)n * n * (n / 2 + 1);
+    float *G = nullptr;
+    CK(get_green_host(gk[lev - 2], n, &G));
+    CK(get_dtab(n));
+    const double scale = (double)L.rcs / (double)(1.0f / (float)rsf);
+    const size_t per_slot = sizeof(float) * (size_t)n3 * 4 + sizeof(cufftComplex) * (size_t)nk * 4;
+    const size_t budget = (size_t)8 << 30;
+    int bmax = (int)std::max<size_t>(1, budget / per_slot);
+    bmax = std::min<int>(bmax, 512);
+    for (size_t j0 = 0; j0 < locs.size(); j0 += bmax) {
+      const int nj = (int)std::min<size_t>(bmax, locs.size() - j0);
+      int nb = nj;
+      for (int b : kFftBuckets)
+        if (b >= nj) {
+          nb = b;
+          break;
+        }
+      CK(grow(g.rho, sizeof(float) * n3 * nb));
+      CK(grow(g.rhok, sizeof(cufftComplex) * nk * nb));
+      CK(grow(g.fk, sizeof(cufftComplex) * nk * 3 * nb));
+      CK(grow(g.force, sizeof(float) * n3 * 3 * nb));
+      std::vector<MeshJob> jobs(nj);
+      for (int j = 0; j < nj; j++) {
+        const int loc = locs[j0 + j];
+        const int nss = L.nns * L.nns * L.nns;
+        const int t = loc / nss, s = loc % nss;
+        const int us[3] = {s % L.nns, (s / L.nns) % L.nns, s / (L.nns * L.nns)};
+        MeshJob &J = jobs[j];
+        J.t = t;
+        J.slot = j;
+        J.range = 0.f;
+        for (int q = 0; q < 3; q++) {
+          J.lo[q] = us[q] * L.ntt + L.ncb - 1;  // nc1 - nloop (kick.f90:429-432)
+          J.alo[q] = us[q] * L.ntt + L.ncb;     // nc1 (kick.f90:503-505)
+          J.off[q] = (double)us[q] * nfp;        // utile_shift * nfp (kick.f90:438)
+        }
+      }
+      CK(upload(g.jobs, jobs.data(), jobs.size(), soff));
+      PM3Args a{};
+      a.L = &g.L;
+      a.rsf = rsf;
+      a.n = n;
+      a.nslots = nb;
+      a.jobs = (const MeshJob *)g.jobs.p;
+      a.njobs = nj;
+      for (int q = 0; q < 3; q++) {
+        a.rdep[q] = L.ntt + 2;
+        a.ract[q] = L.ntt;
+      }
+      a.wrap = 0;
+      a.shift = nfb;
+      a.fphys_lo = nfb;
+      a.fphys_n = nfp;
+      a.scale = scale;
+      a.xp = d.xp;
+      a.rhoc = d.rhoc;
+      a.cell_base = (const int64_t *)g.cell_base.p;
+      a.rho = (float *)g.rho.p;
+      a.rhok = (cufftComplex *)g.rhok.p;
+      a.fk = (cufftComplex *)g.fk.p;
+      a.force = (float *)g.force.p;
+      a.green = G;
+      a.dtab = (const float *)g.dtab.p;
+      a.mass = mass;
+      a.kick = kick;
+      a.vp = d.vp;
+      a.out = (float *)g.out.p;
+      a.want_vmax = want_vmax;
+      cufftHandle fw, bw;
+      CK(get_plan(n, nb, CUFFT_R2C, &fw));
+      CK(get_plan(n, 3 * nb, CUFFT_C2R, &bw));
+      CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3 * nb, g.stream));
+      launch_pm3_deposit(a, g.stream);
+      CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
+      launch_pm3_kspace(a, g.stream);
+      CF(cufftExecC2R(bw, (cufftComplex *)g.fk.p, (cufftReal *)g.force.p));
+      a.nslots = nj;  // f2max over the real jobs only
+      launch_pm3_f2max(a, g.stream);
+      launch_pm3_gather(a, g.stream);
+      g.launches += 4;
+      CU(cudaGetLastError());
+      // the job table is reused by the next batch
+      CU(cudaStreamSynchronize(g.stream));
+      soff = 0;
+    }
+  }
+  return CUBE_OK;
+}
+
+// PP stage: binning, work list, force kernel.  With `pairs` non-null the force
+// kernel only counts accepted pairs and leaves vp untouched.
+static int run_pp(const Meta &m, const Dev &d, float mass, float kick, size_t &soff,
+                  unsigned long long *pairs = nullptr) {
+  const Lay &L = g.L;
+  CK(upload(g.tiles, m.tiles.data(), m.tiles.size(), soff));
+  CK(upload(g.range_loc, m.range_loc.data(), m.range_loc.size(), soff));
+  CK(grow(g.count, sizeof(int32_t) * (size_t)m.ncells));
+  CK(grow(g.cell_start, sizeof(int32_t) * (size_t)(m.ncells + 1)));
+  CK(grow(g.scan_tmp, sizeof(int32_t) * scan_tmp_elems(m.ncells)));
+  CK(grow(g.spos, sizeof(float4) * (size_t)std::max<int64_t>(d.n_used, 1)));
+  const int spill_cap = 2048;
+  CK(grow(g.spill, sizeof(Spill) * spill_cap));
+  CK(grow(g.spill_rank, sizeof(int32_t) * spill_cap));
+  int64_t interior = 0;
+  for (auto &t : m.tiles) interior += (int64_t)L.nt * t.rcp * L.nt * t.rcp * L.nt * t.rcp;
+  const int64_t item_cap = interior + d.n_used / 32 + 16;
+  CK(grow(g.items, sizeof(int4) * (size_t)item_cap));
+  int32_t *ctr = (int32_t *)g.counters.p;  // [0] spill_n [1] head [2] err [64..128) buckets
+  BinArgs b{};
+  b.L = &g.L;
+  b.d_tiles = (const TilePP *)g.tiles.p;
+  b.max_rcp = m.max_rcp;
+  b.ncells = m.ncells;
+  b.xp = d.xp;
+  b.rhoc = d.rhoc;
+  b.cell_base = (const int64_t *)g.cell_base.p;
+  b.count = (int32_t *)g.count.p;
+  b.cell_start = (int32_t *)g.cell_start.p;
+  b.spos = (float4 *)g.spos.p;
+  b.spill = (Spill *)g.spill.p;
+  b.spill_rank = (int32_t *)g.spill_rank.p;
+  b.spill_n = ctr + 0;
+  b.spill_cap = spill_cap;
+  b.scan_tmp = (int32_t *)g.scan_tmp.p;
+  b.err = ctr + 2;
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][2], g.stream));
+  const size_t shm = sizeof(int32_t) * kWarps * m.max_rcp * m.max_rcp * m.max_rcp;
+  if (shm > 48 * 1024) return fail(CUBE_ERR_INVALID);
+  launch_pp_binning(b, g.stream);
+  g.launches += 7;  // count, spill sort, 3 scan passes, scatter, spill placement
+  CU(cudaGetLastError());
+  PPArgs p{};
+  p.L = &g.L;
+  p.d_tiles = (const TilePP *)g.tiles.p;
+  p.h_tiles = m.tiles.data();
+  p.ncells = m.ncells;
+  p.cell_start = (const int32_t *)g.cell_start.p;
+  p.spos = (const float4 *)g.spos.p;
+  p.range_loc = (const float *)g.range_loc.p;
+  p.items = (int4 *)g.items.p;
+  p.bucket = ctr + 64;
+  p.head = ctr + 1;
+  p.item_cap = item_cap;
+  p.vp = d.vp;
+  p.mass2 = mass * mass;
+  p.kick = kick;
+  p.out = (float *)g.out.p;
+  p.want_vmax = 1;
+  p.err = ctr + 2;
+  p.num_sms = g.num_sms;
+  p.pairs = pairs;
+  launch_pp_items(p, g.stream);
+  CU(cudaGetLastError());
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][6], g.stream));
+  launch_pp_force(p, g.stream);
+  g.launches += 3;
+  CU(cudaGetLastError());
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][4], g.stream));
+  return CUBE_OK;
+}
+
+static bool configured() { return g.configured; }
+
+// Whole device pipeline on device inputs; outputs land in g.out (+ err word).
+static int run_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf, const float *apm3,
+                    const float *const *gk, const Dev &d, float mass, float a_mid, float dt, bool do_pm3,
+                    bool do_pp, Meta &m) {
+  if (!configured()) return fail(CUBE_ERR_NOT_CONFIGURED);
+  CK(build_meta(ires, ixyz3, ratio_sf, apm3, m));
+  // the pinned staging area is rewritten below: wait until the previous call's copies out of it ran
+  if (g.stage_pending) {
+    CU(cudaEventSynchronize(g.stage_ev));
+    g.stage_pending = false;
+  }
+  CK(stage((size_t)4 << 20));
+  CK(grow(g.cell_base, sizeof(int64_t) * (size_t)g.L.ntile * g.L.nte * g.L.nte * g.L.nte));
+  CK(grow(g.out, sizeof(float) * 8));
+  CK(grow(g.counters, sizeof(int32_t) * 128));
+  size_t soff = 0;
+  // kick coefficient a_mid*dt/6/pi (kick.f90:529, pp_force_kernel.c:355)
+  const float kick = (float)((double)(a_mid * dt / 6.0f) / 3.14159265358979323846);
+  CU(cudaMemsetAsync(g.out.p, 0, sizeof(float) * 8, g.stream));
+  CU(cudaMemsetAsync(g.counters.p, 0, sizeof(int32_t) * 128, g.stream));
+  if (g.timing) {
+    g.ring_cur = g.ring_next;
+    g.ring_next = (g.ring_next + 1) % Ctx::kRing;
+    g.ring_count = std::min(g.ring_count + 1, Ctx::kRing);
+    g.ring_pm3[g.ring_cur] = do_pm3;
+    g.ring_pp[g.ring_cur] = do_pp;
+    CU(cudaEventRecord(g.ring[g.ring_cur][0], g.stream));
+  }
+  launch_cell_table(g.L, d.rhoc, d.idx, (int64_t *)g.cell_base.p, g.stream);
+  g.launches += 1;
+  CU(cudaGetLastError());
+  if (do_pm3) CK(run_pm3(m, ires, ratio_sf, gk, d, mass, kick, !do_pp, soff));
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][1], g.stream));
+  if (do_pp) CK(run_pp(m, d, mass, kick, soff));
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][5], g.stream));
+  CU(cudaEventRecord(g.stage_ev, g.stream));
+  g.stage_pending = true;
+  // error word next to the outputs
+  CU(cudaMemcpyAsync((char *)g.out.p + 5 * sizeof(float), (char *)g.counters.p + 2 * sizeof(int32_t),
+                     sizeof(int32_t), cudaMemcpyDeviceToDevice, g.stream));
+  return CUBE_OK;
+}
+
+static int finish_times(bool do_pm3, bool do_pp) {
+  if (!g.timing) return CUBE_OK;
+  CU(cudaEventSynchronize(g.ring[g.ring_cur][5]));
+  float a = 0, b = 0, c = 0, t = 0;
+  if (do_pm3) CU(cudaEventElapsedTime(&a, g.ring[g.ring_cur][0], g.ring[g.ring_cur][1]));
+  if (do_pp) {
+    CU(cudaEventElapsedTime(&b, g.ring[g.ring_cur][2], g.ring[g.ring_cur][6]));
+    CU(cudaEventElapsedTime(&c, g.ring[g.ring_cur][6], g.ring[g.ring_cur][4]));
+  }
+  CU(cudaEventElapsedTime(&t, g.ring[g.ring_cur][0], g.ring[g.ring_cur][5]));
+  g.stage_ms[0] = a;
+  g.stage_ms[1] = b;
+  g.stage_ms[2] = c;
+  g.stage_ms[3] = t;
+  return CUBE_OK;
+}
+
+static int check_err_word(int32_t w) {
+  if (!w) return CUBE_OK;
+  if (w & (1 << CUBE_ERR_CAPACITY)) return fail(CUBE_ERR_CAPACITY);
+  return fail(CUBE_ERR_INVALID);
+}
+
+// host-buffer kick: upload, run, download vp and the outputs
+static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf, const float *apm3,
+                     const float *const *gk, const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp,
+                     float *vp, float mass, float a_mid, float dt, bool do_pm3, bool do_pp, float out5[5],
+                     Meta &m) {
+  if (!configured()) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!rhoc || !idx_b_r || !xp || !vp) return fail(CUBE_ERR_INVALID);
+  CK(build_meta(ires, ixyz3, ratio_sf, apm3, m));  // host-side validation before touching the device
+  if (do_pp && !apm3) return fail(CUBE_ERR_INVALID);
+  const Lay &L = g.L;
+  const int64_t nrows = (int64_t)L.ntile * L.nte * L.nte;
+  const int64_t n_used = idx_b_r[nrows - 1];  // pm3_fft_cuda.cu:533-536
+  if (n_used < 0 || n_used >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
+  // the spine must be non-decreasing and consistent with rhoc row sums
+  {
+    int64_t prev = 0;
+    for (int64_t r = 0; r < nrows; r++) {
+      int64_t s = 0;
+      for (int i = 0; i < L.nte; i++) {
+        const int32_t c = rhoc[r * L.nte + i];
+        if (c < 0) return fail(CUBE_ERR_INVALID);
+        s += c;
+      }
+      if (idx_b_r[r] - prev != s) return fail(CUBE_ERR_INVALID);
+      prev = idx_b_r[r];
+    }
+  }
+  CK(ensure_device());
+  CK(grow(g.xp, sizeof(int16_t) * 3 * (size_t)std::max<int64_t>(n_used, 1)));
+  CK(grow(g.vp, sizeof(float) * 3 * (size_t)std::max<int64_t>(n_used, 1)));
+  CK(grow(g.rhoc, sizeof(int32_t) * (size_t)nrows * L.nte));
+  CK(grow(g.idx, sizeof(int64_t) * (size_t)nrows));
+  CU(cudaMemcpyAsync(g.rhoc.p, rhoc, sizeof(int32_t) * nrows * L.nte, cudaMemcpyHostToDevice, g.stream));
+  CU(cudaMemcpyAsync(g.idx.p, idx_b_r, sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, g.stream));
+  if (n_used) {
+    CU(cudaMemcpyAsync(g.xp.p, xp, sizeof(int16_t) * 3 * n_used, cudaMemcpyHostToDevice, g.stream));
+    CU(cudaMemcpyAsync(g.vp.p, vp, sizeof(float) * 3 * n_used, cudaMemcpyHostToDevice, g.stream));
+  }
+  Dev d{(const int16_t *)g.xp.p, (const int32_t *)g.rhoc.p, (const int64_t *)g.idx.p, (float *)g.vp.p, n_used};
+  CK(run_kick(ires, ixyz3, ratio_sf, apm3, gk, d, mass, a_mid, dt, do_pm3, do_pp, m));
+  if (n_used) CU(cudaMemcpyAsync(vp, g.vp.p, sizeof(float) * 3 * n_used, cudaMemcpyDeviceToHost, g.stream));
+  CU(cudaMemcpyAsync(g.h_out, g.out.p, sizeof(float) * 6, cudaMemcpyDeviceToHost, g.stream));
+  CU(cudaStreamSynchronize(g.stream));
+  CK(finish_times(do_pm3, do_pp));
+  int32_t w;
+  memcpy(&w, &g.h_out[5], sizeof(w));
+  CK(check_err_word(w));
+  for (int q = 0; q < 5; q++) out5[q] = g.h_out[q];
+  return CUBE_OK;
+}
+
+}  // namespace cube
+
+using namespace cube;
+
+extern "C" {
+
+int cube_set_layout(const cube_layout *l) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!l) return fail(CUBE_ERR_INVALID);
+  const int rcs = l->ratio_cs;
+  if (l->ng <= 0 || l->nnt <= 0 || l->nns <= 0 || rcs <= 0 || l->ngb <= 0) return fail(CUBE_ERR_INVALID);
+  if (l->ng % rcs || (l->ng / rcs) % l->nnt || ((l->ng / rcs) / l->nnt) % l->nns) return fail(CUBE_ERR_INVALID);
+  if (l->ngb % rcs || l->ngb < rcs) return fail(CUBE_ERR_INVALID);
+  if (l->p_order != 2) return fail(CUBE_ERR_INVALID);
+  if (l->pm3_mode != CUBE_PM3_SUBTILE && l->pm3_mode != CUBE_PM3_PERIODIC) return fail(CUBE_ERR_INVALID);
+  if (!(l->app >= 0.f)) return fail(CUBE_ERR_INVALID);
+  Lay L{};
+  L.ng = l->ng;
+  L.nnt = l->nnt;
+  L.nns = l->nns;
+  L.rcs = rcs;
+  L.ngb = l->ngb;
+  L.nc = L.ng / rcs;
+  L.nt = L.nc / L.nnt;
+  L.ntt = L.nt / L.nns;
+  L.ncb = L.ngb / rcs;
+  L.nte = L.nt + 2 * L.ncb;
+  L.ns3 = (L.nnt * L.nns) * (L.nnt * L.nns) * (L.nnt * L.nns);
+  L.ntile = L.nnt * L.nnt * L.nnt;
+  L.app = l->app;
+  L.pm3_mode = l->pm3_mode;
+  L.apm3f = l->apm3f;
+  L.apm_range = l->apm_range;
+  L.p_order = l->p_order;
+  g.L = L;
+  g.pub = *l;
+  g.configured = true;
+  t_last_error = CUBE_OK;
+  return CUBE_OK;
+}
+
+int cube_get_layout(cube_layout *l) {
+  if (!l) return fail(CUBE_ERR_INVALID);
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  *l = g.pub;
+  return CUBE_OK;
+}
+
+int cube_last_error(void) { return t_last_error; }
+
+const char *cube_error_string(int s) {
+  switch (s) {
+    case CUBE_OK: return "ok";
+    case CUBE_ERR_INVALID: return "invalid argument or subtile metadata";
+    case CUBE_ERR_NOT_CONFIGURED: return "cube_set_layout has not been called";
+    case CUBE_ERR_CUDA: return "CUDA runtime error";
+    case CUBE_ERR_CUFFT: return "cuFFT error";
+    case CUBE_ERR_CAPACITY: return "device capacity check failed";
+    case CUBE_ERR_NO_DEVICE: return "no CUDA device visible";
+    case CUBE_ERR_TIMEOUT: return "bounded device wait timed out";
+    default: return "unknown status";
+  }
+}
+
+int cube_pm3_force(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf,
+                   const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp, const float *const gk[5],
+                   float *vp, float mass, float a_mid, float dt, float *f2max, float vmax[3], double *ptotal) {
+  (void)isort;  // subtiles are independent; order only steered the reference's CPU scheduling
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  float out[5];
+  Meta m;
+  CK(host_kick(ires, ixyz3, ratio_sf, nullptr, gk, rhoc, idx_b_r, xp, vp, mass, a_mid, dt, true, false, out, m));
+  if (f2max) *f2max = out[0];
+  if (vmax) {
+    vmax[0] = out[2];
+    vmax[1] = out[3];
+    vmax[2] = out[4];
+  }
+  if (ptotal) fill_ptotal(m, rhoc, ptotal);
+  return CUBE_OK;
+}
+
+int cube_pp_force(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                  const int32_t *ratio_sf, const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp,
+                  float *vp, float mass, float a_mid, float dt, float *f2max, float vmax[3], double *ptotal,
+                  double *ttotal) {
+  (void)isort;
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!apm3) return fail(CUBE_ERR_INVALID);
+  const bool was = g.timing;
+  g.timing = true;
+  float out[5];
+  Meta m;
+  int s = host_kick(ires, ixyz3, ratio_sf, apm3, nullptr, rhoc, idx_b_r, xp, vp, mass, a_mid, dt, false, true, out,
+                    m);
+  g.timing = was;
+  CK(s);
+  if (f2max) *f2max = out[1];
+  if (vmax) {
+    vmax[0] = out[2];
+    vmax[1] = out[3];
+    vmax[2] = out[4];
+  }
+  if (ptotal) fill_ptotal(m, rhoc, ptotal);
+  if (ttotal) {
+    const Lay &L = g.L;
+    for (int it = 0; it < L.ns3; it++) ttotal[it] = 0.0;
+    const int nss = L.nns * L.nns * L.nns;
+    const double sec = (g.stage_ms[1] + g.stage_ms[2]) * 1e-3 / L.ntile;
+    for (int t = 0; t < L.ntile; t++) ttotal[m.owner[t * nss]] = sec;
+  }
+  return CUBE_OK;
+}
+
+int cube_kick_fine(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                   const int32_t *ratio_sf, const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp,
+                   const float *const gk[5], float *vp, float mass, float a_mid, float dt, float out[5],
+                   double *ptotal) {
+  (void)isort;
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!apm3 || !out) return fail(CUBE_ERR_INVALID);
+  Meta m;
+  CK(host_kick(ires, ixyz3, ratio_sf, apm3, gk, rhoc, idx_b_r, xp, vp, mass, a_mid, dt, true, true, out, m));
+  if (ptotal) fill_ptotal(m, rhoc, ptotal);
+  return CUBE_OK;
+}
+
+int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                          const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r,
+                          const int16_t *d_xp, int64_t n_used, const float *const gk[5], float *d_vp, float mass,
+                          float a_mid, float dt, float *d_out, void *stream) {
+  (void)isort;
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!apm3 || !d_rhoc || !d_idx_b_r || !d_xp || !d_vp || !d_out) return fail(CUBE_ERR_INVALID);
+  if (n_used < 0 || n_used >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  cudaStream_t own = g.stream;
+  if (stream) g.stream = (cudaStream_t)stream;
+  Dev d{d_xp, d_rhoc, d_idx_b_r, d_vp, n_used};
+  Meta m;
+  int s = run_kick(ires, ixyz3, ratio_sf, apm3, gk, d, mass, a_mid, dt, true, true, m);
+  if (s == CUBE_OK) {
+    cudaError_t e = cudaMemcpyAsync(d_out, g.out.p, sizeof(float) * 6, cudaMemcpyDeviceToDevice, g.stream);
+    if (e != cudaSuccess) s = fail(CUBE_ERR_CUDA);
+  }
+  g.stream = own;
+  return s;
+}
+
+void c_pm3_force_kernel(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf,
+                        int32_t *rhoc, int64_t *idx_b_r, int16_t *xp, const float *g2, const float *g4,
+                        const float *g6, const float *g8, const float *g12, float *vp, float mass, float a_mid,
+                        float dt, float *f2max, float vmax[3], double *ptotal) {
+  const float *gk[5] = {g2, g4, g6, g8, g12};
+  cube_pm3_force(isort, ires, ixyz3, ratio_sf, rhoc, idx_b_r, xp, gk, vp, mass, a_mid, dt, f2max, vmax, ptotal);
+}
+
+void c_pp_force_kernel(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                       const int32_t *ratio_sf, int32_t *rhoc, int64_t *idx_b_r, int16_t *xp, float *vp,
+                       float mass, float a_mid, float dt, float *f2max, float vmax[3], double *ptotal,
+                       double *ttotal) {
+  cube_pp_force(isort, ires, ixyz3, apm3, ratio_sf, rhoc, idx_b_r, xp, vp, mass, a_mid, dt, f2max, vmax, ptotal,
+                ttotal);
+}
+
+void c_pm3_fft_finalize(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g.device < 0) return;
+  cudaSetDevice(g.device);
+  cudaStreamSynchronize(g.stream);
+  for (auto &p : g.plans) cufftDestroy(p.h);
+  g.plans.clear();
+  for (auto &e : g.greens) cudaFree(e.d);
+  g.greens.clear();
+  for (auto &e : g.hgreens) cudaFree(e.d);
+  g.hgreens.clear();
+  release(g.rho);
+  release(g.rhok);
+  release(g.fk);
+  release(g.force);
+  release(g.dtab);
+  release(g.jobs);
+  g.dtab_n = -1;
+}
+
+void c_gpu_velocity_finalize(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g.device < 0) return;
+  cudaSetDevice(g.device);
+  cudaStreamSynchronize(g.stream);
+  Buf *bufs[] = {&g.xp, &g.rhoc, &g.idx, &g.vp, &g.cell_base, &g.tiles, &g.count, &g.cell_start, &g.scan_tmp,
+                 &g.spos, &g.spill, &g.spill_rank, &g.counters, &g.items, &g.range_loc, &g.out};
+  for (Buf *b : bufs) release(*b);
+}
+
+int cube_pp_bin_tile(const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf, const int32_t *rhoc,
+                     const int64_t *idx_b_r, const int16_t *xp, int32_t tile, uint32_t *keys, int64_t *ip,
+                     int32_t *cell_start, float *xf, int64_t cap_n, int64_t cap_grid, int64_t *n_out,
+                     int64_t *grid_out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!rhoc || !idx_b_r || !xp) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  const Lay &L = g.L;
+  if (tile < 0 || tile >= L.ntile) return fail(CUBE_ERR_INVALID);
+  Meta m;
+  CK(build_meta(ires, ixyz3, ratio_sf, nullptr, m));
+  const int64_t nrows = (int64_t)L.ntile * L.nte * L.nte;
+  const int64_t n_used = idx_b_r[nrows - 1];
+  if (n_used < 0 || n_used >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
+  CK(stage((size_t)4 << 20));
+  CK(grow(g.xp, sizeof(int16_t) * 3 * (size_t)std::max<int64_t>(n_used, 1)));
+  CK(grow(g.rhoc, sizeof(int32_t) * (size_t)nrows * L.nte));
+  CK(grow(g.idx, sizeof(int64_t) * (size_t)nrows));
+  CK(grow(g.cell_base, sizeof(int64_t) * (size_t)nrows * L.nte));
+  CK(grow(g.counters, sizeof(int32_t) * 128));
+  CU(cudaMemcpyAsync(g.rhoc.p, rhoc, sizeof(int32_t) * nrows * L.nte, cudaMemcpyHostToDevice, g.stream));
+  CU(cudaMemcpyAsync(g.idx.p, idx_b_r, sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, g.stream));
+  if (n_used)
+    CU(cudaMemcpyAsync(g.xp.p, xp, sizeof(int16_t) * 3 * n_used, cudaMemcpyHostToDevice, g.stream));
+  CU(cudaMemsetAsync(g.counters.p, 0, sizeof(int32_t) * 128, g.stream));
+  launch_cell_table(L, (const int32_t *)g.rhoc.p, (const int64_t *)g.idx.p, (int64_t *)g.cell_base.p, g.stream);
+  size_t soff = 0;
+  CK(upload(g.tiles, m.tiles.data(), m.tiles.size(), soff));
+  CK(grow(g.count, sizeof(int32_t) * (size_t)m.ncells));
+  CK(grow(g.cell_start, sizeof(int32_t) * (size_t)(m.ncells + 1)));
+  CK(grow(g.scan_tmp, sizeof(int32_t) * scan_tmp_elems(m.ncells)));
+  CK(grow(g.spos, sizeof(float4) * (size_t)std::max<int64_t>(n_used, 1)));
+  CK(grow(g.spill, sizeof(Spill) * 2048));
+  CK(grow(g.spill_rank, sizeof(int32_t) * 2048));
+  int32_t *ctr = (int32_t *)g.counters.p;
+  BinArgs b{};
+  b.L = &g.L;
+  b.d_tiles = (const TilePP *)g.tiles.p;
+  b.max_rcp = m.max_rcp;
+  b.ncells = m.ncells;
+  b.xp = (const int16_t *)g.xp.p;
+  b.rhoc = (const int32_t *)g.rhoc.p;
+  b.cell_base = (const int64_t *)g.cell_base.p;
+  b.count = (int32_t *)g.count.p;
+  b.cell_start = (int32_t *)g.cell_start.p;
+  b.spos = (float4 *)g.spos.p;
+  b.spill = (Spill *)g.spill.p;
+  b.spill_rank = (int32_t *)g.spill_rank.p;
+  b.spill_n = ctr;
+  b.spill_cap = 2048;
+  b.scan_tmp = (int32_t *)g.scan_tmp.p;
+  b.err = ctr + 2;
+  launch_pp_binning(b, g.stream);
+  CU(cudaGetLastError());
+  const TilePP tp = m.tiles[tile];
+  const int64_t grid = (int64_t)tp.S * tp.S * tp.S;
+  std::vector<int32_t> cs(grid + 1);
+  CU(cudaMemcpyAsync(cs.data(), (int32_t *)g.cell_start.p + tp.cell0, sizeof(int32_t) * (grid + 1),
+                     cudaMemcpyDeviceToHost, g.stream));
+  int32_t err = 0;
+  CU(cudaMemcpyAsync(&err, ctr + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, g.stream));
+  CU(cudaStreamSynchronize(g.stream));
+  CK(check_err_word(err));
+  const int32_t first = cs[0];
+  const int64_t N = cs[grid] - first;
+  if (n_out) *n_out = N;
+  if (grid_out) *grid_out = grid;
+  if (N > cap_n || grid + 1 > cap_grid) return fail(CUBE_ERR_CAPACITY);
+  std::vector<float4> sp(N > 0 ? N : 1);
+  if (N) CU(cudaMemcpy(sp.data(), (float4 *)g.spos.p + first, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+  if (cell_start)
+    for (int64_t c = 0; c <= grid; c++) cell_start[c] = cs[c] - first;
+  if (keys) {
+    int64_t c = 0;
+    for (int64_t q = 0; q < N; q++) {
+      while (cs[c + 1] - first <= q) c++;
+      keys[q] = (uint32_t)c;
+    }
+  }
+  for (int64_t q = 0; q < N; q++) {
+    if (ip) {
+      int32_t v;
+      memcpy(&v, &sp[q].w, sizeof(v));
+      ip[q] = v;
+    }
+    if (xf) {
+      xf[q] = sp[q].x;
+      xf[N + q] = sp[q].y;
+      xf[2 * N + q] = sp[q].z;
+    }
+  }
+  return CUBE_OK;
+}
+
+int cube_pp_pair_count(const int32_t *ires, const int32_t *ixyz3, const float *apm3, const int32_t *ratio_sf,
+                       const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp, int64_t *pairs) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!rhoc || !idx_b_r || !xp || !apm3 || !pairs) return fail(CUBE_ERR_INVALID);
+  Meta m;
+  CK(build_meta(ires, ixyz3, ratio_sf, apm3, m));
+  CK(ensure_device());
+  const Lay &L = g.L;
+  const int64_t nrows = (int64_t)L.ntile * L.nte * L.nte;
+  const int64_t n_used = idx_b_r[nrows - 1];
+  if (n_used < 0 || n_used >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
+  if (g.stage_pending) {
+    CU(cudaEventSynchronize(g.stage_ev));
+    g.stage_pending = false;
+  }
+  CK(stage((size_t)4 << 20));
+  CK(grow(g.xp, sizeof(int16_t) * 3 * (size_t)std::max<int64_t>(n_used, 1)));
+  CK(grow(g.rhoc, sizeof(int32_t) * (size_t)nrows * L.nte));
+  CK(grow(g.idx, sizeof(int64_t) * (size_t)nrows));
+  CK(grow(g.cell_base, sizeof(int64_t) * (size_t)nrows * L.nte));
+  CK(grow(g.counters, sizeof(int32_t) * 128));
+  CK(grow(g.out, sizeof(float) * 8));
+  CU(cudaMemcpyAsync(g.rhoc.p, rhoc, sizeof(int32_t) * nrows * L.nte, cudaMemcpyHostToDevice, g.stream));
+  CU(cudaMemcpyAsync(g.idx.p, idx_b_r, sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, g.stream));
+  if (n_used) CU(cudaMemcpyAsync(g.xp.p, xp, sizeof(int16_t) * 3 * n_used, cudaMemcpyHostToDevice, g.stream));
+  CU(cudaMemsetAsync(g.counters.p, 0, sizeof(int32_t) * 128, g.stream));
+  CU(cudaMemsetAsync(g.out.p, 0, sizeof(float) * 8, g.stream));
+  launch_cell_table(L, (const int32_t *)g.rhoc.p, (const int64_t *)g.idx.p, (int64_t *)g.cell_base.p, g.stream);
+  Dev d{(const int16_t *)g.xp.p, (const int32_t *)g.rhoc.p, (const int64_t *)g.idx.p, nullptr, n_used};
+  size_t soff = 0;
+  unsigned long long *d_pairs = (unsigned long long *)((int32_t *)g.counters.p + 8);
+  CK(run_pp(m, d, 1.0f, 0.0f, soff, d_pairs));
+  unsigned long long h = 0;
+  int32_t err = 0;
+  CU(cudaMemcpyAsync(&h, d_pairs, sizeof(h), cudaMemcpyDeviceToHost, g.stream));
+  CU(cudaMemcpyAsync(&err, (int32_t *)g.counters.p + 2, sizeof(err), cudaMemcpyDeviceToHost, g.stream));
+  CU(cudaStreamSynchronize(g.stream));
+  CK(check_err_word(err));
+  *pairs = (int64_t)h;
+  return CUBE_OK;
+}
+
+int cube_green_table(int32_t n, float apm_soft, float apm_range, float gridsize, float *G) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (n < 2 || !G) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  const size_t count = (size_t)n * n * (n / 2 + 1);
+  float *d = nullptr;
+  CU(cudaMalloc(&d, sizeof(float) * count));
+  launch_green_fp64(n, apm_soft, apm_range, gridsize, 2, d, g.stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(G, d, sizeof(float) * count, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(CUBE_ERR_CUDA);
+  return CUBE_OK;
+}
+
+int cube_force_truth_fp64(const double *pos, int64_t n, double box, double app, const int64_t *targets, int64_t nt,
+                          double alpha, double rcut, int32_t nmax, double *F) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!pos || !targets || !F || n <= 0 || nt < 0 || box <= 0 || rcut > 0.5 * box) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  const int s = ewald_device(pos, n, box, app, targets, nt, alpha, rcut, nmax, F);
+  if (s != CUBE_OK) return fail(s);
+  return CUBE_OK;
+}
+
+int cube_stage_times(float ms[4]) {
+  if (!ms) return fail(CUBE_ERR_INVALID);
+  for (int q = 0; q < 4; q++) ms[q] = g.stage_ms[q];
+  return CUBE_OK;
+}
+
+int cube_timing_read(float *ms, int32_t max_calls, int32_t *n_calls) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!ms || !n_calls || max_calls < 0) return fail(CUBE_ERR_INVALID);
+  const int n = std::min(g.ring_count, (int)max_calls);
+  const int first = (g.ring_next - g.ring_count + Ctx::kRing) % Ctx::kRing;
+  for (int q = 0; q < n; q++) {
+    const int s = (first + q) % Ctx::kRing;
+    cudaEvent_t *e = g.ring[s];
+    CU(cudaEventSynchronize(e[5]));
+    float a = 0, b = 0, c = 0, t = 0;
+    if (g.ring_pm3[s]) CU(cudaEventElapsedTime(&a, e[0], e[1]));
+    if (g.ring_pp[s]) {
+      CU(cudaEventElapsedTime(&b, e[2], e[6]));
+      CU(cudaEventElapsedTime(&c, e[6], e[4]));
+    }
+    CU(cudaEventElapsedTime(&t, e[0], e[5]));
+    ms[4 * q] = a;
+    ms[4 * q + 1] = b;
+    ms[4 * q + 2] = c;
+    ms[4 * q + 3] = t;
+  }
+  *n_calls = n;
+  g.ring_count = 0;
+  return CUBE_OK;
+}
+
+int64_t cube_launch_count(void) { return g.launches; }
+
+int cube_fp32_peak_probe(float *tflops) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!tflops) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  float ms = 0.f;
+  double flops = 0.0;
+  if (fma_probe(g.stream, g.num_sms, &ms, &flops) != cudaSuccess) return fail(CUBE_ERR_CUDA);
+  *tflops = (float)(flops / (ms * 1e-3) / 1e12);
+  return CUBE_OK;
+}
+
+int cube_enable_timing(int on) {
+  g.timing = on != 0;
+  return CUBE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,362 @@
+// Cell-sorted PP binning: a counting sort of every particle of a tile's PP
+// region (the tile plus one coarse cell, pp_force_kernel.c:174-180) by PP cell,
+// bit-exact with the reference's keys, stable order and cell_start
+// (pp_force_kernel.c:196-274).
+//
+// The input is already sorted by coarse cell (CUBE2's storage order), and a PP
+// cell lies inside one coarse cell, so the stable radix sort of the reference
+// reduces to a local counting sort per coarse cell: one warp per coarse cell
+// histograms its particles over its rcp^3 sub-cells (pass 1), a global
+// exclusive scan over all PP cells gives cell_start, and the same warp
+// scatters its particles in storage order (pass 2, ranks via __match_any_sync).
+// The reference computes keys in float (x = (float)(c + (u+0.5)/2^16),
+// floor((float)rcp * x)); the rounding can push a particle into the first PP
+// cell of the next coarse cell (|c| >= 128, or rcp not a power of two).  Such
+// "spilled" particles are collected in a small list, sorted by (key, storage
+// index) and placed ahead of the home particles of their cell, which is where
+// the stable sort puts them: every source of a spill precedes the home cell in
+// storage order.
+#include <cstdio>
+
+#include "common.cuh"
+
+namespace cube {
+
+__global__ void k_cell_table(int64_t nrows, int nte, const int32_t *__restrict__ rhoc,
+                             const int64_t *__restrict__ idx_b_r, int64_t *__restrict__ cell_base) {
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrows) return;
+  const int32_t *row = rhoc + r * nte;
+  int64_t s = idx_b_r[r];
+  for (int i = nte - 1; i >= 0; --i) {
+    s -= row[i];
+    cell_base[r * nte + i] = s;
+  }
+}
+
+void launch_cell_table(const Lay &L, const int32_t *rhoc, const int64_t *idx_b_r, int64_t *cell_base,
+                       cudaStream_t s) {
+  int64_t nrows = (int64_t)L.ntile * L.nte * L.nte;
+  k_cell_table<<<(unsigned)((nrows + 255) / 256), 256, 0, s>>>(nrows, L.nte, rhoc, idx_b_r, cell_base);
+}
+
+struct BinK {
+  int nt, ncb, nte, rcs, R, ntile;
+  int64_t R3;
+  int max_rcp3;
+  const TilePP *tiles;
+  const int16_t *xp;
+  const int32_t *rhoc;
+  const int64_t *cell_base;
+  int32_t *count;
+  const int32_t *cell_start;
+  float4 *spos;
+  Spill *spill;
+  const int32_t *spill_rank;
+  int32_t *spill_n;
+  int spill_cap;
+  int32_t *err;
+};
+
+// number of sorted spill entries with key == g (list sorted by gkey)
+__device__ __forceinline__ int spill_count_of(const Spill *sp, int n, int64_t g) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int m = (lo + hi) >> 1;
+    if (sp[m].gkey < g) lo = m + 1; else hi = m;
+  }
+  int a = lo;
+  hi = n;
+  while (lo < hi) {
+    int m = (lo + hi) >> 1;
+    if (sp[m].gkey <= g) lo = m + 1; else hi = m;
+  }
+  return lo - a;
+}
+
+// Pass 1 (SCATTER = false): per-sub-cell counts, spill collection.
+// Pass 2 (SCATTER = true): stable placement into spos.
+template <bool SCATTER>
+__global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
+  extern __shared__ int32_t sh_hist[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t wid = (int64_t)blockIdx.x * kWarps + warp;
+  if (wid >= (int64_t)p.ntile * p.R3) return;
+  const int t = (int)(wid / p.R3);
+  int64_t rem = wid - (int64_t)t * p.R3;
+  const int cx = (int)(rem % p.R), cy = (int)((rem / p.R) % p.R), cz = (int)(rem / ((int64_t)p.R * p.R));
+  const TilePP tp = p.tiles[t];
+  const int rcp = tp.rcp, S = tp.S, rcp3 = rcp * rcp * rcp;
+  int32_t *hist = sh_hist + warp * p.max_rcp3;
+  // extended-tile C index of this region cell and its tile-local coarse coordinate (may be -1 or nt)
+  const int ci = p.ncb - 1 + cx, cj = p.ncb - 1 + cy, ck = p.ncb - 1 + cz;
+  const int64_t cidx = (((int64_t)t * p.nte + ck) * p.nte + cj) * p.nte + ci;
+  const int np = p.rhoc[cidx];
+  const int64_t base = p.cell_base[cidx];
+  const int lx = cx - 1, ly = cy - 1, lz = cz - 1;
+  const int nspill = SCATTER ? min(*p.spill_n, p.spill_cap) : 0;
+
+  for (int b = lane; b < rcp3; b += 32) hist[b] = 0;
+  __syncwarp();
+
+  for (int l0 = 0; l0 < np; l0 += 32) {
+    const int l = l0 + lane;
+    const bool valid = l < np;
+    bool spilled = false;
+    int b = 0;
+    int64_t gkey = 0;
+    float x = 0.f, y = 0.f, z = 0.f;
+    int64_t ip = base + l;
+    if (valid) {
+      const int16_t *q = p.xp + 3 * ip;
+      // pp_force_kernel.c:213-218: (float)((i-ncb) + ((int16)(xp+ishift)+rshift)*x_resolution)
+      x = __double2float_rn(decode_pos(lx, q[0]));
+      y = __double2float_rn(decode_pos(ly, q[1]));
+      z = __double2float_rn(decode_pos(lz, q[2]));
+      // pp_force_kernel.c:226-228: floor(rcp * (x - utile_shift*ntt)) + rcp, float product
+      int kx = (int)floorf(__fmul_rn((float)rcp, x)) + rcp;
+      int ky = (int)floorf(__fmul_rn((float)rcp, y)) + rcp;
+      int kz = (int)floorf(__fmul_rn((float)rcp, z)) + rcp;
+      // keys beyond the tile grid (float rounding at the outer halo face) are clamped
+      kx = min(max(kx, 0), S - 1);
+      ky = min(max(ky, 0), S - 1);
+      kz = min(max(kz, 0), S - 1);
+      const int rx = kx - rcp * cx, ry = ky - rcp * cy, rz = kz - rcp * cz;
+      spilled = (rx >= rcp) | (ry >= rcp) | (rz >= rcp);
+      if ((rx < 0) | (ry < 0) | (rz < 0)) atomicOr(p.err, 1 << CUBE_ERR_INVALID);
+      b = (rz * rcp + ry) * rcp + rx;
+      gkey = tp.cell0 + ((int64_t)kz * S + ky) * S + kx;
+    }
+    const bool home = valid && !spilled;
+    if (!SCATTER) {
+      if (home) atomicAdd(&hist[b], 1);
+      if (valid && spilled) {
+        int s = atomicAdd(p.spill_n, 1);
+        if (s < p.spill_cap) {
+          Spill e;
+          e.gkey = gkey;
+          e.ip = (int32_t)ip;
+          e.cell = (int32_t)wid;
+          p.spill[s] = e;
+        } else {
+          atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
+        }
+      }
+    } else {
+      const unsigned hm = __ballot_sync(0xffffffffu, home);
+      int hb = 0, rank = 0;
+      unsigned peers = 0;
+      if (home) {
+        peers = __match_any_sync(hm, b);
+        rank = __popc(peers & ((1u << lane) - 1u));
+        hb = hist[b];
+      }
+      __syncwarp();
+      if (home) {
+        int off = 0;
+        if (nspill) off = spill_count_of(p.spill, nspill, gkey);
+        const int64_t pos = (int64_t)p.cell_start[gkey] + off + hb + rank;
+        p.spos[pos] = make_float4(__fmul_rn((float)p.rcs, x), __fmul_rn((float)p.rcs, y),
+                                  __fmul_rn((float)p.rcs, z), __int_as_float((int)ip));
+        if (rank == 0) hist[b] = hb + __popc(peers);
+      }
+      __syncwarp();
+    }
+  }
+  if (!SCATTER) {
+    __syncwarp();
+    for (int b = lane; b < rcp3; b += 32) {
+      const int rx = b % rcp, ry = (b / rcp) % rcp, rz = b / (rcp * rcp);
+      const int64_t g = tp.cell0 + ((int64_t)(rcp * cz + rz) * S + (rcp * cy + ry)) * S + (rcp * cx + rx);
+      p.count[g] = hist[b];
+    }
+  }
+}
+
+// Sort the spill list by (gkey, ip) in one block, add the spills to the cell
+// counts and record each spill's rank inside its cell.
+constexpr int kSpillCap = 2048;
+
+__global__ void __launch_bounds__(1024) k_spill_fix(Spill *sp, int32_t *rank, int32_t *spill_n, int cap,
+                                                   int32_t *count) {
+  __shared__ unsigned long long key[kSpillCap];
+  __shared__ int idx[kSpillCap];
+  const int n = min(*spill_n, cap);
+  if (n == 0) return;
+  int np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+    key[i] = i < n ? (((unsigned long long)sp[i].gkey << 32) | (unsigned)sp[i].ip) : ~0ull;
+    idx[i] = i;
+  }
+  __syncthreads();
+  for (int k = 2; k <= np2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+        int l = i ^ j;
+        if (l > i) {
+          bool up = (i & k) == 0;
+          unsigned long long a = key[i], b = key[l];
+          if ((a > b) == up) {
+            key[i] = b;
+            key[l] = a;
+            int t = idx[i];
+            idx[i] = idx[l];
+            idx[l] = t;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  // kSpillCap / 1024 entries per thread: read all, then write back in sorted order
+  Spill e[kSpillCap / 1024];
+  int m = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) e[m++] = sp[idx[i]];
+  __syncthreads();
+  m = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const Spill v = e[m++];
+    sp[i] = v;
+    int r = 0;
+    while (i - r - 1 >= 0 && (long long)(key[i - r - 1] >> 32) == v.gkey) r++;
+    rank[i] = r;
+    atomicAdd(&count[v.gkey], 1);
+  }
+}
+
+__global__ void k_spill_place(BinK p) {
+  const int n = min(*p.spill_n, p.spill_cap);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const Spill e = p.spill[i];
+    const int t = (int)(e.cell / p.R3);
+    const int64_t rem = e.cell - (int64_t)t * p.R3;
+    const int cx = (int)(rem % p.R), cy = (int)((rem / p.R) % p.R), cz = (int)(rem / ((int64_t)p.R * p.R));
+    const int16_t *q = p.xp + 3 * (int64_t)e.ip;
+    float x = __double2float_rn(decode_pos(cx - 1, q[0]));
+    float y = __double2float_rn(decode_pos(cy - 1, q[1]));
+    float z = __double2float_rn(decode_pos(cz - 1, q[2]));
+    const int64_t pos = (int64_t)p.cell_start[e.gkey] + p.spill_rank[i];
+    p.spos[pos] = make_float4(__fmul_rn((float)p.rcs, x), __fmul_rn((float)p.rcs, y), __fmul_rn((float)p.rcs, z),
+                              __int_as_float(e.ip));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// exclusive scan of int32 counts -> cell_start (n + 1 entries)
+
+constexpr int kScanThreads = 256, kScanPer = 16, kScanTile = kScanThreads * kScanPer;
+
+size_t scan_tmp_elems(int64_t n) { return (size_t)((n + kScanTile - 1) / kScanTile) + 1; }
+
+__device__ __forceinline__ int block_excl_scan(int v, int *total) {
+  __shared__ int ws[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < kScanThreads / 32 ? ws[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kScanThreads / 32) ws[lane] = w;
+  }
+  __syncthreads();
+  int incl = x + (warp ? ws[warp - 1] : 0);
+  *total = ws[kScanThreads / 32 - 1];
+  __syncthreads();
+  return incl - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int32_t *in, int64_t n, int32_t *part) {
+  const int64_t b0 = (int64_t)blockIdx.x * kScanTile;
+  int s = 0;
+  for (int k = 0; k < kScanPer; k++) {
+    int64_t i = b0 + (int64_t)k * kScanThreads + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  int tot;
+  block_excl_scan(s, &tot);
+  if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_top(int32_t *part, int nb) {
+  int carry = 0;
+  for (int c0 = 0; c0 < nb; c0 += kScanThreads) {
+    int i = c0 + threadIdx.x;
+    int v = i < nb ? part[i] : 0;
+    int tot;
+    int ex = block_excl_scan(v, &tot);
+    if (i < nb) part[i] = ex + carry;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) part[nb] = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_down(const int32_t *in, int64_t n, const int32_t *part,
+                                                           int nb, int32_t *out) {
+  const int64_t b0 = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanPer;
+  int v[kScanPer];
+  int s = 0;
+  for (int k = 0; k < kScanPer; k++) {
+    int64_t i = b0 + k;
+    v[k] = i < n ? in[i] : 0;
+    s += v[k];
+  }
+  int tot;
+  int ex = block_excl_scan(s, &tot) + part[blockIdx.x];
+  for (int k = 0; k < kScanPer; k++) {
+    int64_t i = b0 + k;
+    if (i < n) out[i] = ex;
+    ex += v[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = part[nb];
+}
+
+static void scan_exclusive(const int32_t *in, int64_t n, int32_t *out, int32_t *tmp, cudaStream_t s) {
+  const int nb = (int)((n + kScanTile - 1) / kScanTile);
+  k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, n, tmp);
+  k_scan_top<<<1, kScanThreads, 0, s>>>(tmp, nb);
+  k_scan_down<<<nb, kScanThreads, 0, s>>>(in, n, tmp, nb, out);
+}
+
+void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
+  const Lay &L = *a.L;
+  BinK p;
+  p.nt = L.nt;
+  p.ncb = L.ncb;
+  p.nte = L.nte;
+  p.rcs = L.rcs;
+  p.R = L.nt + 2;
+  p.ntile = L.ntile;
+  p.R3 = (int64_t)p.R * p.R * p.R;
+  p.max_rcp3 = a.max_rcp * a.max_rcp * a.max_rcp;
+  p.tiles = a.d_tiles;
+  p.xp = a.xp;
+  p.rhoc = a.rhoc;
+  p.cell_base = a.cell_base;
+  p.count = a.count;
+  p.cell_start = a.cell_start;
+  p.spos = a.spos;
+  p.spill = a.spill;
+  p.spill_rank = a.spill_rank;
+  p.spill_n = a.spill_n;
+  p.spill_cap = a.spill_cap < kSpillCap ? a.spill_cap : kSpillCap;
+  p.err = a.err;
+  const int64_t warps = (int64_t)p.ntile * p.R3;
+  const unsigned blocks = (unsigned)((warps + kWarps - 1) / kWarps);
+  const size_t shm = sizeof(int32_t) * kWarps * p.max_rcp3;
+  cudaMemsetAsync(a.spill_n, 0, sizeof(int32_t), s);
+  k_pp_bin<false><<<blocks, kWarps * 32, shm, s>>>(p);
+  k_spill_fix<<<1, 1024, 0, s>>>(a.spill, a.spill_rank, a.spill_n, p.spill_cap, a.count);
+  scan_exclusive(a.count, a.ncells, a.cell_start, a.scan_tmp, s);
+  k_pp_bin<true><<<blocks, kWarps * 32, shm, s>>>(p);
+  k_spill_place<<<8, 256, 0, s>>>(p);
+}
+
+}  // namespace cube

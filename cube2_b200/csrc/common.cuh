@@ -1,0 +1,168 @@
+// Internal declarations shared by the kernels and the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include "../../include/cube2_b200.h"
+
+namespace cube {
+
+// Run-time layout; the derived sizes mirror parameters.f90:56-78.
+struct Lay {
+  int ng, nnt, nns, rcs, ngb;
+  int nc, nt, ntt, ncb, nte, ns3, ntile;
+  float app;
+  int pm3_mode;
+  float apm3f, apm_range;
+  int p_order;
+};
+
+// Per-parent-tile PP grid (one fine-grid launch per tile, pp_force_kernel.cu:643-661).
+struct TilePP {
+  int rcp;         // PP cells per coarse cell (max ratio_sf over the tile's subtiles)
+  int S;           // PP cells per side of the tile region (nt + 2 coarse cells) = rcp*(nt+2)
+  int64_t cell0;   // first global PP cell index of this tile
+};
+
+// Spilled particle: its PP key lies in a neighbouring coarse cell because the
+// reference's float rounding (pp_force_kernel.c:213-236) pushed it across.
+struct Spill {
+  int64_t gkey;  // global PP cell
+  int32_t ip;    // storage index
+  int32_t cell;  // t * R^3 + (cz*R + cy)*R + cx, region-local coarse cell
+};
+
+// PM3 mesh job (a periodic image tile, or one buffered subtile).
+struct MeshJob {
+  int t;          // parent tile
+  int lo[3];      // first deposit coarse cell (C index into the extended tile)
+  int alo[3];     // first active (gathered) coarse cell
+  double off[3];  // mesh coordinate = (c - ncb + frac) * scale - off
+  int slot;       // batch slot
+  float range;    // unused by PM3 (kept for alignment of the table)
+};
+
+constexpr int kWarps = 8;  // warps per block in warp-per-cell kernels
+
+// ---------------------------------------------------------------------------------------------
+// device helpers
+
+// Fixed-point decode of pp_force_kernel.c:213-218 / kick.f90:292 in double:
+// (c) + (u + 0.5) * 2^-16 with u = (uint16)xp; exact.
+__device__ __forceinline__ double decode_pos(int c, int16_t xp) {
+  return (double)c + ((double)(uint16_t)xp + 0.5) * (1.0 / 65536.0);
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(float *addr, float v) {
+  // non-negative floats order like their bit patterns
+  atomicMax(reinterpret_cast<int *>(addr), __float_as_int(v));
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+  for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ int64_t wrapi(int64_t a, int64_t n) {
+  a %= n;
+  return a < 0 ? a + n : a;
+}
+
+// ---------------------------------------------------------------------------------------------
+// kernel launchers (defined in the .cu files); all enqueue on `s`
+
+// cell_base[t][k][j][i] = idx_b_r[t][k][j] - sum(rhoc[t][k][j][i:])  (pp_force_kernel.c:203-209)
+void launch_cell_table(const Lay &L, const int32_t *rhoc, const int64_t *idx_b_r, int64_t *cell_base,
+                       cudaStream_t s);
+
+// PP binning (counting sort by PP cell, bit-exact with pp_force_kernel.c:196-274)
+struct BinArgs {
+  const Lay *L;
+  const TilePP *d_tiles;  // device table [ntile]
+  int max_rcp;
+  int64_t ncells;         // total PP cells over all tiles
+  const int16_t *xp;
+  const int32_t *rhoc;
+  const int64_t *cell_base;
+  int32_t *count;         // [ncells]
+  int32_t *cell_start;    // [ncells + 1]
+  float4 *spos;           // [n_region] x,y,z (fine units, tile-local), w = ip bits
+  Spill *spill;           // [spill_cap]
+  int32_t *spill_rank;    // [spill_cap]
+  int32_t *spill_n;       // device counter
+  int spill_cap;
+  int32_t *scan_tmp;      // scan scratch
+  int32_t *err;           // device error word
+};
+void launch_pp_binning(const BinArgs &a, cudaStream_t s);
+size_t scan_tmp_elems(int64_t n);
+
+// PP work list + force
+struct PPArgs {
+  const Lay *L;
+  const TilePP *d_tiles;
+  const TilePP *h_tiles;
+  int64_t ncells;
+  const int32_t *cell_start;
+  const float4 *spos;
+  const float *range_loc;   // [ns3] PP range by subtile location
+  int4 *items;              // [item_cap]
+  int32_t *bucket;          // [64]: counts, cursors
+  int32_t *n_items;         // device counter (= total)
+  int32_t *head;            // work-queue head
+  int64_t item_cap;
+  float *vp;                // device vp [n_used][3]
+  float mass2, kick;
+  float *out;               // [5] f2max_pm3, f2max_pp, vmax[3]
+  int want_vmax;
+  int32_t *err;
+  int num_sms;
+  unsigned long long *pairs;  // non-null: count accepted pairs instead of kicking
+};
+void launch_pp_items(const PPArgs &a, cudaStream_t s);
+void launch_pp_force(const PPArgs &a, cudaStream_t s);
+
+// PM3
+struct PM3Args {
+  const Lay *L;
+  int rsf;
+  int n;                 // mesh side
+  int nslots;            // batch size
+  const MeshJob *jobs;   // device [njobs]
+  int njobs;
+  int rdep[3], ract[3];  // deposit / active coarse ranges per job
+  int wrap;              // 1 periodic image mesh, 0 buffered subtile mesh
+  int shift;             // array index = floor(coord) + shift (nfb in buffered mode)
+  int fphys_lo, fphys_n; // f2max region per slot (buffered mode)
+  double scale;          // ratio_cs / gridsize
+  const int16_t *xp;
+  const int32_t *rhoc;
+  const int64_t *cell_base;
+  float *rho;            // [nslots][n^3]
+  cufftComplex *rhok;    // [nslots][n*n*(n/2+1)]
+  cufftComplex *fk;      // [nslots*3][n*n*(n/2+1)]
+  float *force;          // [nslots*3][n^3]
+  const float *green;    // [n*n*(n/2+1)]
+  const float *dtab;     // [n] finite-difference symbol D(k) per signed wavenumber index
+  float mass, kick;
+  float *vp;
+  float *out;
+  int want_vmax;
+};
+void launch_pm3_deposit(const PM3Args &a, cudaStream_t s);
+void launch_pm3_kspace(const PM3Args &a, cudaStream_t s);
+void launch_pm3_f2max(const PM3Args &a, cudaStream_t s);
+void launch_pm3_gather(const PM3Args &a, cudaStream_t s);
+void launch_green_fp64(int n, double apm_soft, double apm_range, double gridsize, int p_order, float *G,
+                       cudaStream_t s);
+
+// FP32 FMA throughput probe (5 launches); returns the time and the FLOPs executed
+cudaError_t fma_probe(cudaStream_t s, int num_sms, float *ms, double *flops);
+
+// FP64 truth
+int ewald_device(const double *pos, int64_t n, double box, double app, const int64_t *targets, int64_t nt,
+                 double alpha, double rcut, int nmax, double *F);
+
+}  // namespace cube

@@ -1,0 +1,327 @@
+// PP short-range pair force over the 27 neighbouring PP cells
+// (pp_force_kernel.c:282-325, pp_force_kernel.cu:192-250) and the kick of
+// the interior particles (pp_force_kernel.c:339-364).
+//
+// Work decomposition: an item is one interior PP cell (or a 32-particle chunk
+// of a crowded one).  The 27 neighbour cells of a cell form 9 contiguous
+// ranges of the cell-sorted array (three cells along x are adjacent in key
+// order).  Items are bucketed by cost (log2 of i-count x candidates) and a
+// persistent kernel hands them out heaviest first through an atomic queue
+// head, so the lognormal occupancy of clustered boxes does not leave a tail.
+//
+// Inside an item one warp splits its 32 lanes into (i-particles) x (groups
+// over the j-candidates): for a cell with 8 particles, 4 lane groups each
+// walk a quarter of the candidates.  Candidates are staged through shared
+// memory by coalesced float4 loads and read back as broadcasts.  Each lane
+// accumulates in FP32 with Kahan compensation per staged tile; the groups'
+// partial sums are merged with warp shuffles (TwoSum), then the owning lane
+// applies af*mass^2, the kick, f2max and vmax.
+#include "common.cuh"
+
+namespace cube {
+
+constexpr int kPPThreads = 256;
+constexpr int kPPWarps = kPPThreads / 32;
+constexpr int kJTile = 128;  // staged candidates per warp
+constexpr int kBuckets = 32;
+
+// basic_functions.f08:95-109 / pp_force_kernel.c:45-74 in FP32, same operation order
+__device__ __forceinline__ float F_ra(float r, float apm) {
+  float ep = 2.0f * r / apm;
+  if (apm == 0.0f || ep > 2.0f) return 1.0f / (r * r);
+  if (ep > 1.0f) {
+    float ep2 = ep * ep, ep3 = ep2 * ep, ep4 = ep3 * ep, ep5 = ep4 * ep, ep6 = ep5 * ep;
+    return (1.0f / 35.0f / (apm * apm)) *
+           (12.0f / ep2 - 224.0f + 896.0f * ep - 840.0f * ep2 + 224.0f * ep3 + 70.0f * ep4 - 48.0f * ep5 +
+            7.0f * ep6);
+  }
+  if (ep > 0.0f) {
+    float ep3 = ep * ep * ep, ep4 = ep3 * ep, ep5 = ep4 * ep, ep6 = ep5 * ep;
+    return (1.0f / 35.0f / (apm * apm)) * (224.0f * ep - 224.0f * ep3 + 70.0f * ep4 + 48.0f * ep5 - 21.0f * ep6);
+  }
+  return 0.0f;
+}
+
+__device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
+  float y = x - c;
+  float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+// (hi, lo) + (hi2, lo2) with an error-free TwoSum of the high parts
+__device__ __forceinline__ void two_sum_merge(float &hi, float &lo, float hi2, float lo2) {
+  float s = hi + hi2;
+  float bp = s - hi;
+  float err = (hi - (s - bp)) + (hi2 - bp);
+  hi = s;
+  lo = lo + lo2 + err;
+}
+
+struct PPK {
+  int nt, ntt, nns, nnt, ntile;
+  const TilePP *tiles;
+  const int32_t *cs;
+  const float4 *spos;
+  const float *range_loc;
+  int4 *items;
+  int32_t *bucket;  // [0,32) counts, [32,64) cursors
+  int32_t *head;
+  int64_t item_cap;
+  float *vp;
+  float mass2, kick, app;
+  float *out;
+  int want_vmax;
+  int32_t *err;
+  int64_t max_cells;  // max interior PP cells per tile (grid sizing)
+  unsigned long long *pairs;  // COUNT mode: accepted ordered pairs
+};
+
+__device__ __forceinline__ int next_pow2(int v) { return v <= 1 ? 1 : 1 << (32 - __clz(v - 1)); }
+
+// cost bucket of a chunk with ni i-particles and nj candidates, heavy = high index
+__device__ __forceinline__ int cost_bucket(int ni, int64_t nj) {
+  int64_t c = nj * next_pow2(ni);
+  if (c < 1) c = 1;
+  int b = 63 - __clzll(c);
+  return b > kBuckets - 1 ? kBuckets - 1 : b;
+}
+
+// Enumerate interior PP cells; pass 0 counts items per bucket, pass 1 emits them.
+template <int PASS>
+__global__ void __launch_bounds__(256) k_pp_items(PPK p) {
+  __shared__ int sc[kBuckets], sbase[kBuckets], soff[kBuckets];
+  if (threadIdx.x < kBuckets) sc[threadIdx.x] = 0;
+  if (PASS == 1 && threadIdx.x == 0) {
+    int acc = 0;
+    for (int b = kBuckets - 1; b >= 0; --b) {
+      soff[b] = acc;
+      acc += p.bucket[b];
+    }
+  }
+  __syncthreads();
+  const int t = blockIdx.y;
+  const TilePP tp = p.tiles[t];
+  const int rcp = tp.rcp, S = tp.S, npg = p.nt * rcp;
+  const int64_t ncell = (int64_t)npg * npg * npg;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int nchunks = 0, ni = 0;
+  int64_t nj = 0, g = 0;
+  if (c < ncell) {
+    const int x = (int)(c % npg) + rcp, y = (int)((c / npg) % npg) + rcp, z = (int)(c / ((int64_t)npg * npg)) + rcp;
+    g = tp.cell0 + ((int64_t)z * S + y) * S + x;
+    ni = p.cs[g + 1] - p.cs[g];
+    if (ni > 0) {
+      for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++) {
+          const int64_t b = g + ((int64_t)dz * S + dy) * S;
+          nj += p.cs[b + 2] - p.cs[b - 1];
+        }
+      nchunks = (ni + 31) >> 5;
+    }
+  }
+  int myrank[4];
+  int mybucket[4];
+  // chunks beyond the first few per thread are rare; handle the first 4 with local ranks,
+  // the rest with direct global atomics
+  for (int k = 0; k < nchunks; k++) {
+    const int nik = min(32, ni - 32 * k);
+    const int b = cost_bucket(nik, nj);
+    if (k < 4) {
+      mybucket[k] = b;
+      myrank[k] = atomicAdd(&sc[b], 1);
+    } else if (PASS == 0) {
+      atomicAdd(&p.bucket[b], 1);
+    } else {
+      const int slot = soff[b] + atomicAdd(&p.bucket[kBuckets + b], 1);
+      if (slot < p.item_cap) p.items[slot] = make_int4((int)g, k, t, 0);
+      else atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kBuckets) {
+    const int n = sc[threadIdx.x];
+    if (PASS == 0) {
+      if (n) atomicAdd(&p.bucket[threadIdx.x], n);
+    } else {
+      sbase[threadIdx.x] = n ? atomicAdd(&p.bucket[kBuckets + threadIdx.x], n) : 0;
+    }
+  }
+  if (PASS == 1) {
+    __syncthreads();
+    for (int k = 0; k < nchunks && k < 4; k++) {
+      const int b = mybucket[k];
+      const int64_t slot = (int64_t)soff[b] + sbase[b] + myrank[k];
+      if (slot < p.item_cap) p.items[slot] = make_int4((int)g, k, t, 0);
+      else atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
+    }
+  }
+}
+
+// COUNT = false: forces and kick.  COUNT = true: only count the accepted ordered
+// pairs 0 < r^2 < rc^2 (the algorithmic work of the kick, for the roofline).
+template <bool COUNT>
+__global__ void __launch_bounds__(kPPThreads) k_pp_force(PPK p) {
+  __shared__ float4 jbuf[kPPWarps][kJTile];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float4 *buf = jbuf[warp];
+  int total = 0;
+  {
+    int v = lane < kBuckets ? p.bucket[lane] : 0;
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    total = min((int64_t)v, p.item_cap);
+  }
+  float f2w = 0.f, vm0 = 0.f, vm1 = 0.f, vm2 = 0.f;
+  unsigned long long npairs = 0;
+  for (;;) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(p.head, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= total) break;
+    const int4 item = p.items[it];
+    const int64_t g = (int64_t)(unsigned)item.x;
+    const TilePP tp = p.tiles[item.z];
+    const int S = tp.S, rcp = tp.rcp;
+    const int64_t loc = g - tp.cell0;
+    const int x = (int)(loc % S), y = (int)((loc / S) % S), z = (int)(loc / ((int64_t)S * S));
+    // subtile of the i-cell -> per-subtile PP range (pp_force_kernel.cu:776-790)
+    const int t = item.z;
+    const int tx = t % p.nnt, ty = (t / p.nnt) % p.nnt, tz = t / (p.nnt * p.nnt);
+    const int sx = (x / rcp - 1) / p.ntt, sy = (y / rcp - 1) / p.ntt, sz = (z / rcp - 1) / p.ntt;
+    const int loc_sub = (((tz * p.nnt + ty) * p.nnt + tx) * p.nns + sz) * p.nns * p.nns + sy * p.nns + sx;
+    const float rc = p.range_loc[loc_sub];
+    const float rc2 = rc * rc;
+
+    const int i0 = p.cs[g] + item.y * 32;
+    const int ni = min(32, p.cs[g + 1] - i0);
+    const int np2 = next_pow2(ni);
+    const int lg = 31 - __clz(np2);
+    const int ngrp = 32 >> lg;
+    const int il = lane & (np2 - 1), grp = lane >> lg;
+    const bool has_i = il < ni;
+    const float4 pi = p.spos[i0 + (has_i ? il : 0)];
+
+    float sx_ = 0.f, cx_ = 0.f, sy_ = 0.f, cy_ = 0.f, sz_ = 0.f, cz_ = 0.f;
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++) {
+        const int64_t b = g + ((int64_t)dz * S + dy) * S;
+        const int js = p.cs[b - 1], je = p.cs[b + 2];
+        for (int jb = js; jb < je; jb += kJTile) {
+          const int nb = min(kJTile, je - jb);
+          __syncwarp();
+          for (int q = lane; q < nb; q += 32) buf[q] = p.spos[jb + q];
+          __syncwarp();
+          float px = 0.f, py = 0.f, pz = 0.f;
+#pragma unroll 4
+          for (int q = grp; q < nb; q += ngrp) {
+            const float4 pj = buf[q];
+            const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
+            const float r2 = dx * dx + dy_ * dy_ + dz_ * dz_;
+            if (COUNT) {
+              npairs += (has_i && r2 > 0.0f && r2 < rc2) ? 1ull : 0ull;
+            } else if (r2 > 0.0f && r2 < rc2) {
+              const float invr = rsqrtf(r2);
+              const float r = r2 * invr;
+              const float s = (F_ra(r, p.app) - F_ra(r, rc)) * invr;
+              px += s * dx;
+              py += s * dy_;
+              pz += s * dz_;
+            }
+          }
+          kahan_add(sx_, cx_, px);
+          kahan_add(sy_, cy_, py);
+          kahan_add(sz_, cz_, pz);
+        }
+      }
+    // merge the lane groups of each i-particle; Kahan c is the negated low part
+    float hx = sx_, lx = -cx_, hy = sy_, ly = -cy_, hz = sz_, lz = -cz_;
+    for (int o = np2; o < 32; o <<= 1) {
+      const float ohx = __shfl_xor_sync(0xffffffffu, hx, o), olx = __shfl_xor_sync(0xffffffffu, lx, o);
+      const float ohy = __shfl_xor_sync(0xffffffffu, hy, o), oly = __shfl_xor_sync(0xffffffffu, ly, o);
+      const float ohz = __shfl_xor_sync(0xffffffffu, hz, o), olz = __shfl_xor_sync(0xffffffffu, lz, o);
+      two_sum_merge(hx, lx, ohx, olx);
+      two_sum_merge(hy, ly, ohy, oly);
+      two_sum_merge(hz, lz, ohz, olz);
+    }
+    if (!COUNT && grp == 0 && has_i) {
+      const float ax = (hx + lx) * p.mass2, ay = (hy + ly) * p.mass2, az = (hz + lz) * p.mass2;
+      f2w = fmaxf(f2w, ax * ax + ay * ay + az * az);
+      const int64_t ip = (int64_t)__float_as_int(pi.w);
+      float *v = p.vp + 3 * ip;
+      const float v0 = v[0] + ax * p.kick, v1 = v[1] + ay * p.kick, v2 = v[2] + az * p.kick;
+      v[0] = v0;
+      v[1] = v1;
+      v[2] = v2;
+      vm0 = fmaxf(vm0, fabsf(v0));
+      vm1 = fmaxf(vm1, fabsf(v1));
+      vm2 = fmaxf(vm2, fabsf(v2));
+    }
+  }
+  if (COUNT) {
+    for (int o = 16; o; o >>= 1) npairs += __shfl_xor_sync(0xffffffffu, npairs, o);
+    if (lane == 0) atomicAdd(p.pairs, npairs);
+    return;
+  }
+  f2w = warp_max(f2w);
+  if (lane == 0) atomic_max_nonneg(&p.out[1], f2w);
+  if (p.want_vmax) {
+    vm0 = warp_max(vm0);
+    vm1 = warp_max(vm1);
+    vm2 = warp_max(vm2);
+    if (lane == 0) {
+      atomic_max_nonneg(&p.out[2], vm0);
+      atomic_max_nonneg(&p.out[3], vm1);
+      atomic_max_nonneg(&p.out[4], vm2);
+    }
+  }
+}
+
+static PPK make_ppk(const PPArgs &a) {
+  const Lay &L = *a.L;
+  PPK p;
+  p.nt = L.nt;
+  p.ntt = L.ntt;
+  p.nns = L.nns;
+  p.nnt = L.nnt;
+  p.ntile = L.ntile;
+  p.tiles = a.d_tiles;
+  p.cs = a.cell_start;
+  p.spos = a.spos;
+  p.range_loc = a.range_loc;
+  p.items = a.items;
+  p.bucket = a.bucket;
+  p.head = a.head;
+  p.item_cap = a.item_cap;
+  p.vp = a.vp;
+  p.mass2 = a.mass2;
+  p.kick = a.kick;
+  p.app = L.app;
+  p.out = a.out;
+  p.want_vmax = a.want_vmax;
+  p.err = a.err;
+  p.pairs = a.pairs;
+  int max_rcp = 1;
+  for (int t = 0; t < L.ntile; t++) max_rcp = a.h_tiles[t].rcp > max_rcp ? a.h_tiles[t].rcp : max_rcp;
+  const int64_t npg = (int64_t)L.nt * max_rcp;
+  p.max_cells = npg * npg * npg;
+  return p;
+}
+
+void launch_pp_items(const PPArgs &a, cudaStream_t s) {
+  PPK p = make_ppk(a);
+  cudaMemsetAsync(a.bucket, 0, sizeof(int32_t) * 2 * kBuckets, s);
+  dim3 grid((unsigned)((p.max_cells + 255) / 256), (unsigned)a.L->ntile);
+  k_pp_items<0><<<grid, 256, 0, s>>>(p);
+  k_pp_items<1><<<grid, 256, 0, s>>>(p);
+}
+
+void launch_pp_force(const PPArgs &a, cudaStream_t s) {
+  PPK p = make_ppk(a);
+  cudaMemsetAsync(a.head, 0, sizeof(int32_t), s);
+  if (a.pairs)
+    k_pp_force<true><<<a.num_sms * 4, kPPThreads, 0, s>>>(p);
+  else
+    k_pp_force<false><<<a.num_sms * 4, kPPThreads, 0, s>>>(p);
+}
+
+}  // namespace cube

@@ -1,0 +1,176 @@
+/*
+ * cube2_b200 -- B200 (sm_100a) fine-scale kick of CUBE2: PM3 fine-mesh force
+ * plus PP short-range pair force, behind the C ABI that CUBE2's Fortran
+ * driver binds in kick.f90:12-46 and finalize.f90:8-13.
+ *
+ * Array conventions are the reference's (C views of Fortran arrays):
+ *   xp       int16  [n_used][3]  fixed-point offset in the coarse cell
+ *   vp       float  [n_used][3]
+ *   rhoc     int32  [nnt][nnt][nnt][nte][nte][nte]   (tz,ty,tx,k,j,i; nte = nt + 2 ncb)
+ *   idx_b_r  int64  [nnt][nnt][nnt][nte][nte]        running count at the end of row (j,k)
+ *   ixyz3    int32  [ns3][6]   sx,sy,sz,tx,ty,tz (1-based), initialize.f90:207-224
+ *   isort    int32  [ns3]      1-based, ires int32 [ns3] levels 2..6
+ *   ratio_sf int32  [7],  apm3 float [7]
+ * n_used = idx_b_r[last] (pm3_fft_cuda.cu:533-536).
+ *
+ * The reference fixes the layout at compile time (parameters.f90); this
+ * library takes it at run time through cube_set_layout(), which the driver
+ * calls once before the first kick.
+ *
+ * Errors never terminate the process.  The reference-named void entry points
+ * record a status readable with cube_last_error(); the cube_* variants
+ * return it.
+ */
+#ifndef CUBE2_B200_H
+#define CUBE2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum cube_status {
+  CUBE_OK = 0,
+  CUBE_ERR_INVALID = 1,        /* bad argument or metadata (the reference aborts: pp_force_kernel.cu:985-986) */
+  CUBE_ERR_NOT_CONFIGURED = 2, /* cube_set_layout() not called */
+  CUBE_ERR_CUDA = 3,           /* CUDA runtime error */
+  CUBE_ERR_CUFFT = 4,          /* cuFFT error */
+  CUBE_ERR_CAPACITY = 5,       /* a device-side capacity check failed */
+  CUBE_ERR_NO_DEVICE = 6,      /* no CUDA device visible */
+  CUBE_ERR_TIMEOUT = 7         /* a bounded device wait gave up */
+};
+
+/* PM3 mesh geometry */
+enum cube_pm3_mode {
+  CUBE_PM3_SUBTILE = 0, /* the reference's per-subtile buffered meshes, Green tables from the caller */
+  CUBE_PM3_PERIODIC = 1 /* one periodic mesh of side ng*ratio_sf over the image, Green table tabulated here */
+};
+
+typedef struct cube_layout {
+  int32_t ng;       /* fine cells per image side          parameters.f90:20 */
+  int32_t nnt;      /* tiles per image side               parameters.f90:24 */
+  int32_t nns;      /* subtiles per tile side             parameters.f90:25 */
+  int32_t ratio_cs; /* fine cells per coarse cell         parameters.f90:22 */
+  int32_t ngb;      /* tile buffer in fine cells          parameters.f90:56 (ncb = ngb/ratio_cs) */
+  float app;        /* PP softening in fine cells         parameters.f90:42 */
+  int32_t pm3_mode; /* enum cube_pm3_mode */
+  float apm3f;      /* PM3 softening in mesh cells, for the tabulated Green table (parameters.f90:38) */
+  float apm_range;  /* PM3 range cut in mesh cells for the tabulated table, 0 = full force */
+  int32_t p_order;  /* assignment order, 2 = TSC (parameters.f90:48); only 2 is supported */
+} cube_layout;
+
+/* Configure the layout (once, before the first kick).  Replaces the
+ * compile-time constants of cuda_parameters_generated.h:4-14. */
+int cube_set_layout(const cube_layout *layout);
+int cube_get_layout(cube_layout *layout);
+
+int cube_last_error(void);
+const char *cube_error_string(int status);
+
+/* ---- reference entry points (drop-in) ---- */
+
+/* PM3 fine-mesh force and kick.  Replaces pm3_fft_cuda.cu:516-620 (bound at
+ * kick.f90:31-45).  Unlike the reference CUDA build, vp is updated here (the
+ * CPU path's semantics, kick.f90:529) instead of being parked in a device
+ * accumulator that only the next c_pp_force_kernel call applies.  f2max,
+ * vmax (max |vp| of the kicked particles) and ptotal (particles per subtile)
+ * are written.  g2..g12 are the Green tables of levels 2..6 (mode
+ * CUBE_PM3_SUBTILE; cached on the device keyed by pointer and size as
+ * pm3_fft_cuda.cu:153-175 does); they are ignored in mode CUBE_PM3_PERIODIC. */
+void c_pm3_force_kernel(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf,
+                        int32_t *rhoc, int64_t *idx_b_r, int16_t *xp, const float *g2, const float *g4,
+                        const float *g6, const float *g8, const float *g12, float *vp, float mass, float a_mid,
+                        float dt, float *f2max, float vmax[3], double *ptotal);
+
+/* PP short-range force and kick.  Replaces pp_force_kernel.cu:960-1050 and the
+ * CPU pp_force_kernel.c:393-445 (bound at kick.f90:13-30).  ptotal: particles
+ * kicked per subtile; ttotal: device seconds of the PP stage, reported on the
+ * first subtile of each tile. */
+void c_pp_force_kernel(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                       const int32_t *ratio_sf, int32_t *rhoc, int64_t *idx_b_r, int16_t *xp, float *vp,
+                       float mass, float a_mid, float dt, float *f2max, float vmax[3], double *ptotal,
+                       double *ttotal);
+
+/* Release PM3 device state (pm3_fft_cuda.cu:621-628, finalize.f90:18-21). */
+void c_pm3_fft_finalize(void);
+/* Release PP / velocity device state (pp_force_kernel.cu:539-547). */
+void c_gpu_velocity_finalize(void);
+
+/* ---- status-returning variants (same arguments) ---- */
+int cube_pm3_force(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf,
+                   const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp, const float *const gk[5],
+                   float *vp, float mass, float a_mid, float dt, float *f2max, float vmax[3], double *ptotal);
+int cube_pp_force(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                  const int32_t *ratio_sf, const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp,
+                  float *vp, float mass, float a_mid, float dt, float *f2max, float vmax[3], double *ptotal,
+                  double *ttotal);
+
+/* Whole fine-scale kick (PM3 then PP) with one upload of xp/rhoc/idx_b_r/vp
+ * and one download of vp.  Equivalent to cube_pm3_force followed by
+ * cube_pp_force (kick.f90:138-236).  out[0] = PM3 f2max, out[1] = PP f2max,
+ * out[2..4] = vmax after the kick.  ptotal may be NULL. */
+int cube_kick_fine(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                   const int32_t *ratio_sf, const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp,
+                   const float *const gk[5], float *vp, float mass, float a_mid, float dt, float out[5],
+                   double *ptotal);
+
+/* Same kick on device-resident arrays; enqueued on `stream` (a cudaStream_t,
+ * NULL = the library's stream) without host synchronisation.  d_out (6 words
+ * of device memory) receives the 5 floats of cube_kick_fine and, in word 5,
+ * an int32 mask of device-side failures (bit CUBE_ERR_CAPACITY or
+ * CUBE_ERR_INVALID; 0 = none) when the stream reaches it.  The small host
+ * tables are read during the call. */
+int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                          const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r,
+                          const int16_t *d_xp, int64_t n_used, const float *const gk[5], float *d_vp, float mass,
+                          float a_mid, float dt, float *d_out, void *stream);
+
+/* ---- inspection (parity checks) ---- */
+
+/* Binning of one parent tile as the PP pass builds it, in the reference's
+ * conventions (pp_force_kernel.c:196-274): key of every sorted particle,
+ * storage index ip (ip_local[values[]]) of every sorted particle, cell_start
+ * (grid_num + 1 entries, tile-local), sorted positions xf [3][N].  Capacities
+ * in elements; *n_out = N, *grid_out = grid_num.  Runs the binning on the
+ * given host inputs. */
+int cube_pp_bin_tile(const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf, const int32_t *rhoc,
+                     const int64_t *idx_b_r, const int16_t *xp, int32_t tile, uint32_t *keys, int64_t *ip,
+                     int32_t *cell_start, float *xf, int64_t cap_n, int64_t cap_grid, int64_t *n_out,
+                     int64_t *grid_out);
+
+/* Number of ordered PP pairs (i interior, 0 < r^2 < range^2) the kick evaluates
+ * for these inputs -- the algorithmic work of pp_force_kernel.c:282-325, counted
+ * by the same binning and work list on the device.  Host inputs as cube_pp_force. */
+int cube_pp_pair_count(const int32_t *ires, const int32_t *ixyz3, const float *apm3, const int32_t *ratio_sf,
+                       const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp, int64_t *pairs);
+
+/* Green table of the periodic mesh (FP64 tabulation on the device, Green.f90:1-80),
+ * copied to host G[n][n][n/2+1]. */
+int cube_green_table(int32_t n, float apm_soft, float apm_range, float gridsize, float *G);
+
+/* FP64 periodic softened direct sum (Ewald split) on the device for nt targets:
+ * pos [N][3] and targets are host arrays, F [nt][3] is written on the host.
+ * Used to state force errors; not part of the kick. */
+int cube_force_truth_fp64(const double *pos, int64_t n, double box, double app, const int64_t *targets, int64_t nt,
+                          double alpha, double rcut, int32_t nmax, double *F);
+
+/* Device time in ms of the last host-API kick's stages: [0] PM3 total,
+ * [1] PP binning + work list, [2] PP force kernel, [3] whole device pipeline
+ * (filled when timing is enabled). */
+int cube_stage_times(float ms[4]);
+int cube_enable_timing(int on);
+/* Stage times of every timed call since the previous read (oldest first, at
+ * most max_calls, 4 floats per call as cube_stage_times); waits for them. */
+int cube_timing_read(float *ms, int32_t max_calls, int32_t *n_calls);
+/* Number of this library's own kernels enqueued so far (cuFFT's not included). */
+int64_t cube_launch_count(void);
+/* FP32 FMA throughput of this device in TFLOP/s, measured by a register-resident
+ * FMA loop (the denominator of the PP kernel's roofline). */
+int cube_fp32_peak_probe(float *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUBE2_B200_H */

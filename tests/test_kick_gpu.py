@@ -1,0 +1,82 @@
+"""The whole fine-scale kick: fused call == PM3 then PP, device API == host API, and the
+force of PM3 + PP against the FP64 direct-summation truth."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+SIXPI = np.float32(6 * np.pi)
+
+
+def _tables(L):
+    from cube2_b200.layout import RATIO_SF, apm3_table, ixyz3_table
+    return (np.arange(1, L.ns3 + 1, dtype=np.int32), np.full(L.ns3, 2, np.int32), ixyz3_table(L), apm3_table(4.0),
+            RATIO_SF)
+
+
+def test_kick_fine_equals_pm3_then_pp(gpu):
+    from cube2_b200.kick import FineKick
+    img, _ = load_golden("t32_edge")
+    L = img.layout
+    fk = FineKick(L)
+    isort, ires, ix, apm3, rs = _tables(L)
+    v1, f2a, _, _ = fk.c_pm3_force_kernel(img, isort, ires, ix, rs, 1.0, SIXPI, 1.0)
+    v2, f2b, vmax, _, _ = fk.c_pp_force_kernel(img, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0, vp=v1.copy())
+    v3, out = fk.kick_fine(img, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0)
+    np.testing.assert_array_equal(v3, v2)
+    assert out[0] == f2a and out[1] == f2b
+    np.testing.assert_array_equal(out[2:], vmax)
+
+
+def test_device_api_equals_host_api(gpu):
+    import torch
+    from cube2_b200.kick import FineKick
+    img, _ = load_golden("t32")
+    L = img.layout
+    fk = FineKick(L)
+    isort, ires, ix, apm3, rs = _tables(L)
+    vh, out_h = fk.kick_fine(img, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0)
+    dev = torch.device("cuda:0")
+    d_rhoc = torch.from_numpy(img.rhoc.reshape(-1).copy()).to(dev)
+    d_idx = torch.from_numpy(img.idx_b_r.reshape(-1).copy()).to(dev)
+    d_xp = torch.from_numpy(img.xp.reshape(-1).copy()).to(dev)
+    d_vp = torch.from_numpy(img.vp.reshape(-1).copy()).to(dev)
+    d_out = torch.zeros(8, dtype=torch.float32, device=dev)
+    s = torch.cuda.current_stream()
+    fk.kick_fine_device(d_rhoc, d_idx, d_xp, img.n_used, d_vp, d_out, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0,
+                        stream=s)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d_vp.cpu().numpy().reshape(-1, 3), vh)
+    o = d_out.cpu().numpy()
+    np.testing.assert_array_equal(o[:5], out_h)
+    assert o[5:6].view(np.int32)[0] == 0
+
+
+def test_kick_vs_fp64_truth_zeldovich(gpu):
+    """64^3 Zel'dovich lattice, PM3 128^3 + PP cutoff 2 cells: rms force error < 1% vs FP64 Ewald,
+    and the device FP64 truth agrees with the CPU one."""
+    from cube2_b200 import ic
+    from cube2_b200.kick import FineKick, force_truth_fp64
+    from cube2_b200.layout import Layout, build_image, encode_positions
+    from oracle import oracle as O
+    from oracle.layouts import LAYOUTS
+    L = Layout(**LAYOUTS["cfg0"])
+    pos, vel, _ = ic.zeldovich_lattice(64, 0.5, 1000)
+    img = build_image(pos, vel, L)
+    fk = FineKick(L)
+    isort, ires, ix, apm3, rs = _tables(L)
+    zero = np.zeros_like(img.vp)
+    v, _ = fk.kick_fine(img, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0, vp=zero.copy())
+    kick = float(np.float32(SIXPI) / np.float32(6.0)) / np.pi
+    cc, u = encode_positions(pos, 4, 16)
+    posq = (cc + (u.astype(np.float64) + 0.5) / 65536.0) * 4.0
+    act = np.nonzero(img.active)[0]
+    samp = np.random.default_rng(1).choice(act, 1000, replace=False)
+    Fd = force_truth_fp64(posq, 64.0, 0.1, img.pid[samp])
+    Fc = O.ewald(posq, 64.0, 0.1, img.pid[samp][:100])
+    assert np.max(np.abs(Fd[:100] - Fc)) / np.sqrt(np.mean(Fc ** 2)) < 1e-9
+    F = v[samp].astype(np.float64) / kick
+    rel = np.sqrt(np.sum((F - Fd) ** 2) / np.sum(Fd ** 2))
+    assert rel < 0.01, rel
