@@ -134,7 +134,10 @@ def run_ours(args, rank, world, local_rank):
     vp0 = torch.from_numpy(img.vp.reshape(-1).copy()).to(dev)
     d_vp = vp0.clone()
     d_out = torch.zeros(8, dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated stream: the kernels and the timing events must share it
+    stream = torch.cuda.Stream(dev)
+
+    torch.cuda.synchronize()
 
     def kick():
         fk.kick_fine_device(d_rhoc, d_idx, d_xp, img.n_used, d_vp, d_out, isort, ires, ix, apm3, rs, 1.0, a_mid,

@@ -71,8 +71,13 @@ struct Ctx {
   bool timing = false;
   float stage_ms[4] = {0, 0, 0, 0};
   long long launches = 0;  // kernels of this library enqueued so far
-  cudaEvent_t stage_ev = nullptr;  // recorded after the last staged upload of a call
-  bool stage_pending = false;
+  // Pinned staging areas for the small per-call tables, used round robin so the
+  // host can enqueue the next kick while earlier ones still copy out of theirs.
+  static constexpr int kStage = 4;
+  void *stage_buf[kStage] = {};
+  cudaEvent_t stage_evs[kStage] = {};
+  bool stage_used[kStage] = {};
+  int stage_slot = 0;
 };
 
 static Ctx g;
@@ -156,18 +161,36 @@ static int ensure_device() {
   CU(cudaMallocHost(&g.h_out, sizeof(float) * 8));
   for (auto &slot : g.ring)
     for (auto &e : slot) CU(cudaEventCreate(&e));
-  CU(cudaEventCreateWithFlags(&g.stage_ev, cudaEventDisableTiming));
+  for (auto &e : g.stage_evs) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   return CUBE_OK;
 }
 
-static int stage(size_t bytes) {
-  if (bytes <= g.h_stage_cap) return CUBE_OK;
-  if (g.h_stage) {
-    CU(cudaStreamSynchronize(g.stream));
-    CU(cudaFreeHost(g.h_stage));
+// Make every staging area hold `bytes` and select the next one, waiting until
+// the call that last used it has finished copying out of it.
+static int stage_begin(size_t bytes) {
+  if (bytes > g.h_stage_cap) {
+    CU(cudaDeviceSynchronize());
+    for (auto &b : g.stage_buf)
+      if (b) CU(cudaFreeHost(b));
+    g.h_stage_cap = std::max(bytes, (size_t)1 << 20);
+    for (auto &b : g.stage_buf) CU(cudaMallocHost(&b, g.h_stage_cap));
+    for (auto &u : g.stage_used) u = false;
   }
-  g.h_stage_cap = std::max(bytes, (size_t)1 << 20);
-  CU(cudaMallocHost(&g.h_stage, g.h_stage_cap));
+  const int s = g.stage_slot;
+  if (g.stage_used[s]) {
+    CU(cudaEventSynchronize(g.stage_evs[s]));
+    g.stage_used[s] = false;
+  }
+  g.h_stage = g.stage_buf[s];
+  return CUBE_OK;
+}
+
+// Mark the current staging area busy until the stream passes this point.
+static int stage_end() {
+  const int s = g.stage_slot;
+  CU(cudaEventRecord(g.stage_evs[s], g.stream));
+  g.stage_used[s] = true;
+  g.stage_slot = (s + 1) % Ctx::kStage;
   return CUBE_OK;
 }
 
@@ -594,12 +617,7 @@ static int run_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *ra
                     bool do_pp, Meta &m) {
   if (!configured()) return fail(CUBE_ERR_NOT_CONFIGURED);
   CK(build_meta(ires, ixyz3, ratio_sf, apm3, m));
-  // the pinned staging area is rewritten below: wait until the previous call's copies out of it ran
-  if (g.stage_pending) {
-    CU(cudaEventSynchronize(g.stage_ev));
-    g.stage_pending = false;
-  }
-  CK(stage((size_t)4 << 20));
+  CK(stage_begin((size_t)4 << 20));
   CK(grow(g.cell_base, sizeof(int64_t) * (size_t)g.L.ntile * g.L.nte * g.L.nte * g.L.nte));
   CK(grow(g.out, sizeof(float) * 8));
   CK(grow(g.counters, sizeof(int32_t) * 128));
@@ -623,8 +641,7 @@ static int run_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *ra
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][1], g.stream));
   if (do_pp) CK(run_pp(m, d, mass, kick, soff));
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][5], g.stream));
-  CU(cudaEventRecord(g.stage_ev, g.stream));
-  g.stage_pending = true;
+  CK(stage_end());
   // error word next to the outputs
   CU(cudaMemcpyAsync((char *)g.out.p + 5 * sizeof(float), (char *)g.counters.p + 2 * sizeof(int32_t),
                      sizeof(int32_t), cudaMemcpyDeviceToDevice, g.stream));
@@ -923,7 +940,7 @@ int cube_pp_bin_tile(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   const int64_t nrows = (int64_t)L.ntile * L.nte * L.nte;
   const int64_t n_used = idx_b_r[nrows - 1];
   if (n_used < 0 || n_used >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
-  CK(stage((size_t)4 << 20));
+  CK(stage_begin((size_t)4 << 20));
   CK(grow(g.xp, sizeof(int16_t) * 3 * (size_t)std::max<int64_t>(n_used, 1)));
   CK(grow(g.rhoc, sizeof(int32_t) * (size_t)nrows * L.nte));
   CK(grow(g.idx, sizeof(int64_t) * (size_t)nrows));
@@ -963,6 +980,7 @@ int cube_pp_bin_tile(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   b.err = ctr + 2;
   launch_pp_binning(b, g.stream);
   CU(cudaGetLastError());
+  CK(stage_end());
   const TilePP tp = m.tiles[tile];
   const int64_t grid = (int64_t)tp.S * tp.S * tp.S;
   std::vector<int32_t> cs(grid + 1);
@@ -1016,11 +1034,7 @@ int cube_pp_pair_count(const int32_t *ires, const int32_t *ixyz3, const float *a
   const int64_t nrows = (int64_t)L.ntile * L.nte * L.nte;
   const int64_t n_used = idx_b_r[nrows - 1];
   if (n_used < 0 || n_used >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
-  if (g.stage_pending) {
-    CU(cudaEventSynchronize(g.stage_ev));
-    g.stage_pending = false;
-  }
-  CK(stage((size_t)4 << 20));
+  CK(stage_begin((size_t)4 << 20));
   CK(grow(g.xp, sizeof(int16_t) * 3 * (size_t)std::max<int64_t>(n_used, 1)));
   CK(grow(g.rhoc, sizeof(int32_t) * (size_t)nrows * L.nte));
   CK(grow(g.idx, sizeof(int64_t) * (size_t)nrows));
@@ -1037,6 +1051,7 @@ int cube_pp_pair_count(const int32_t *ires, const int32_t *ixyz3, const float *a
   size_t soff = 0;
   unsigned long long *d_pairs = (unsigned long long *)((int32_t *)g.counters.p + 8);
   CK(run_pp(m, d, 1.0f, 0.0f, soff, d_pairs));
+  CK(stage_end());
   unsigned long long h = 0;
   int32_t err = 0;
   CU(cudaMemcpyAsync(&h, d_pairs, sizeof(h), cudaMemcpyDeviceToHost, g.stream));

@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
   for (int l0 = 0; l0 < np; l0 += 32) {
     const int l = l0 + lane;
     const bool valid = l < np;
-    bool spilled = false;
+    bool spilled = false, bad = false;
     int b = 0;
     int64_t gkey = 0;
     float x = 0.f, y = 0.f, z = 0.f;
@@ -123,14 +123,16 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
       kz = min(max(kz, 0), S - 1);
       const int rx = kx - rcp * cx, ry = ky - rcp * cy, rz = kz - rcp * cz;
       spilled = (rx >= rcp) | (ry >= rcp) | (rz >= rcp);
-      if ((rx < 0) | (ry < 0) | (rz < 0)) atomicOr(p.err, 1 << CUBE_ERR_INVALID);
+      // a key below its own coarse cell cannot come from the float path; reject it
+      bad = (rx < 0) | (ry < 0) | (rz < 0) | (rx > rcp) | (ry > rcp) | (rz > rcp);
+      if (bad) atomicOr(p.err, 1 << CUBE_ERR_INVALID);
       b = (rz * rcp + ry) * rcp + rx;
       gkey = tp.cell0 + ((int64_t)kz * S + ky) * S + kx;
     }
-    const bool home = valid && !spilled;
+    const bool home = valid && !spilled && !bad;
     if (!SCATTER) {
       if (home) atomicAdd(&hist[b], 1);
-      if (valid && spilled) {
+      if (valid && spilled && !bad) {
         int s = atomicAdd(p.spill_n, 1);
         if (s < p.spill_cap) {
           Spill e;

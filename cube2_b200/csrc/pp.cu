@@ -77,11 +77,10 @@ struct PPK {
   unsigned long long *pairs;  // COUNT mode: accepted ordered pairs
 };
 
-__device__ __forceinline__ int next_pow2(int v) { return v <= 1 ? 1 : 1 << (32 - __clz(v - 1)); }
-
-// cost bucket of a chunk with ni i-particles and nj candidates, heavy = high index
+// cost bucket of a chunk with ni i-particles and nj candidates, heavy = high index:
+// the warp walks the candidates in floor(32/ni) lane groups
 __device__ __forceinline__ int cost_bucket(int ni, int64_t nj) {
-  int64_t c = nj * next_pow2(ni);
+  int64_t c = nj / (32 / max(ni, 1));
   if (c < 1) c = 1;
   int b = 63 - __clzll(c);
   return b > kBuckets - 1 ? kBuckets - 1 : b;
@@ -161,7 +160,7 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
 // COUNT = false: forces and kick.  COUNT = true: only count the accepted ordered
 // pairs 0 < r^2 < rc^2 (the algorithmic work of the kick, for the roofline).
 template <bool COUNT>
-__global__ void __launch_bounds__(kPPThreads) k_pp_force(PPK p) {
+__global__ void __launch_bounds__(kPPThreads, 3) k_pp_force(PPK p) {
   __shared__ float4 jbuf[kPPWarps][kJTile];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float4 *buf = jbuf[warp];
@@ -194,12 +193,22 @@ __global__ void __launch_bounds__(kPPThreads) k_pp_force(PPK p) {
 
     const int i0 = p.cs[g] + item.y * 32;
     const int ni = min(32, p.cs[g + 1] - i0);
-    const int np2 = next_pow2(ni);
-    const int lg = 31 - __clz(np2);
-    const int ngrp = 32 >> lg;
-    const int il = lane & (np2 - 1), grp = lane >> lg;
-    const bool has_i = il < ni;
-    const float4 pi = p.spos[i0 + (has_i ? il : 0)];
+    // lanes = ngrp groups of ni lanes; group `grp` walks every ngrp-th candidate
+    const int ngrp = 32 / ni;
+    const int il = lane % ni, grp = lane / ni;
+    const bool has_i = grp < ngrp;  // the 32 mod ni leftover lanes idle
+    const float4 pi = p.spos[i0 + il];
+
+    // F_ra(r,app) - F_ra(r,rc) (basic_functions.f08:95-109) with per-cell constants and no
+    // division: for r > app it equals A/r^2 - sum_k c_k ep^k, ep = 2r/rc, where
+    //   outer (ep > 1): A = 32/35 (the 12/ep^2 term folded in), c = [-224,896,-840,224,70,-48,7]/(35 rc^2)
+    //   inner:          A = 1,                                  c = [0,224,0,-224,70,48,-21]/(35 rc^2)
+    const float k35 = 1.0f / (35.0f * rc2);
+    const float cep = 2.0f / rc;
+    const float app2 = p.app * p.app;
+    const float o0 = -224.f * k35, o1 = 896.f * k35, o2 = -840.f * k35, o3 = 224.f * k35, o4 = 70.f * k35,
+                o5 = -48.f * k35, o6 = 7.f * k35;
+    const float n1 = 224.f * k35, n3 = -224.f * k35, n4 = 70.f * k35, n5 = 48.f * k35, n6 = -21.f * k35;
 
     float sx_ = 0.f, cx_ = 0.f, sy_ = 0.f, cy_ = 0.f, sz_ = 0.f, cz_ = 0.f;
     for (int dz = -1; dz <= 1; dz++)
@@ -213,19 +222,34 @@ __global__ void __launch_bounds__(kPPThreads) k_pp_force(PPK p) {
           __syncwarp();
           float px = 0.f, py = 0.f, pz = 0.f;
 #pragma unroll 4
-          for (int q = grp; q < nb; q += ngrp) {
+          for (int q = has_i ? grp : nb; q < nb; q += ngrp) {
             const float4 pj = buf[q];
             const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
             const float r2 = dx * dx + dy_ * dy_ + dz_ * dz_;
+            const bool ok = (r2 > 0.0f) & (r2 < rc2);
             if (COUNT) {
-              npairs += (has_i && r2 > 0.0f && r2 < rc2) ? 1ull : 0ull;
-            } else if (r2 > 0.0f && r2 < rc2) {
+              npairs += ok ? 1ull : 0ull;
+            } else {
               const float invr = rsqrtf(r2);
-              const float r = r2 * invr;
-              const float s = (F_ra(r, p.app) - F_ra(r, rc)) * invr;
-              px += s * dx;
-              py += s * dy_;
-              pz += s * dz_;
+              const float ir2 = invr * invr;
+              const float ep = r2 * invr * cep;
+              const bool outer = ep > 1.0f;
+              float q6 = outer ? o6 : n6;
+              q6 = fmaf(q6, ep, outer ? o5 : n5);
+              q6 = fmaf(q6, ep, outer ? o4 : n4);
+              q6 = fmaf(q6, ep, outer ? o3 : n3);
+              q6 = fmaf(q6, ep, outer ? o2 : 0.0f);
+              q6 = fmaf(q6, ep, outer ? o1 : n1);
+              q6 = fmaf(q6, ep, outer ? o0 : 0.0f);
+              float fpp = fmaf(outer ? (32.0f / 35.0f) : 1.0f, ir2, -q6);
+              if (ok && r2 <= app2) {  // inside the softening length: the exact S2 law (rare)
+                const float r = r2 * invr;
+                fpp = F_ra(r, p.app) - F_ra(r, rc);
+              }
+              const float s = ok ? fpp * invr : 0.0f;
+              px = fmaf(s, dx, px);
+              py = fmaf(s, dy_, py);
+              pz = fmaf(s, dz_, pz);
             }
           }
           kahan_add(sx_, cx_, px);
@@ -233,15 +257,19 @@ __global__ void __launch_bounds__(kPPThreads) k_pp_force(PPK p) {
           kahan_add(sz_, cz_, pz);
         }
       }
-    // merge the lane groups of each i-particle; Kahan c is the negated low part
+    // merge the lane groups of each i-particle (tree over groups, stride s*ni lanes);
+    // Kahan c is the negated low part
     float hx = sx_, lx = -cx_, hy = sy_, ly = -cy_, hz = sz_, lz = -cz_;
-    for (int o = np2; o < 32; o <<= 1) {
-      const float ohx = __shfl_xor_sync(0xffffffffu, hx, o), olx = __shfl_xor_sync(0xffffffffu, lx, o);
-      const float ohy = __shfl_xor_sync(0xffffffffu, hy, o), oly = __shfl_xor_sync(0xffffffffu, ly, o);
-      const float ohz = __shfl_xor_sync(0xffffffffu, hz, o), olz = __shfl_xor_sync(0xffffffffu, lz, o);
-      two_sum_merge(hx, lx, ohx, olx);
-      two_sum_merge(hy, ly, ohy, oly);
-      two_sum_merge(hz, lz, ohz, olz);
+    for (int s = 1; s < ngrp; s <<= 1) {
+      const int delta = s * ni;
+      const float ohx = __shfl_down_sync(0xffffffffu, hx, delta), olx = __shfl_down_sync(0xffffffffu, lx, delta);
+      const float ohy = __shfl_down_sync(0xffffffffu, hy, delta), oly = __shfl_down_sync(0xffffffffu, ly, delta);
+      const float ohz = __shfl_down_sync(0xffffffffu, hz, delta), olz = __shfl_down_sync(0xffffffffu, lz, delta);
+      if ((grp % (2 * s)) == 0 && grp + s < ngrp) {
+        two_sum_merge(hx, lx, ohx, olx);
+        two_sum_merge(hy, ly, ohy, oly);
+        two_sum_merge(hz, lz, ohz, olz);
+      }
     }
     if (!COUNT && grp == 0 && has_i) {
       const float ax = (hx + lx) * p.mass2, ay = (hy + ly) * p.mass2, az = (hz + lz) * p.mass2;

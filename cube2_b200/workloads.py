@@ -28,6 +28,9 @@ WORKLOADS = {
                         rms=0.5, seed=1000, rsf=2, apm3f=4.0),
     "clustered256": dict(layout=dict(ng=256, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1), kind="lognormal", n=256,
                          sigma=1.5, seed=2000, rsf=2, apm3f=4.0),
+    # profiling size: same statistics, 192^3 box (~7M particles), 384^3 mesh (> L2 per array)
+    "clustered192": dict(layout=dict(ng=192, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1), kind="lognormal", n=192,
+                         sigma=1.5, seed=2000, rsf=2, apm3f=4.0),
 }
 
 

@@ -25,9 +25,11 @@ def test_kick_fine_equals_pm3_then_pp(gpu):
     v1, f2a, _, _ = fk.c_pm3_force_kernel(img, isort, ires, ix, rs, 1.0, SIXPI, 1.0)
     v2, f2b, vmax, _, _ = fk.c_pp_force_kernel(img, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0, vp=v1.copy())
     v3, out = fk.kick_fine(img, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0)
-    np.testing.assert_array_equal(v3, v2)
-    assert out[0] == f2a and out[1] == f2b
-    np.testing.assert_array_equal(out[2:], vmax)
+    # the PM3 deposit accumulates with float atomics: runs agree to rounding, not bit for bit
+    d2, d3 = (v2 - img.vp).astype(np.float64), (v3 - img.vp).astype(np.float64)
+    assert np.sqrt(np.sum((d3 - d2) ** 2) / np.sum(d2 ** 2)) < 1e-6
+    assert abs(out[0] - f2a) <= 1e-5 * f2a and abs(out[1] - f2b) <= 1e-6 * f2b
+    np.testing.assert_allclose(out[2:], vmax, rtol=1e-5)
 
 
 def test_device_api_equals_host_api(gpu):
@@ -44,13 +46,15 @@ def test_device_api_equals_host_api(gpu):
     d_xp = torch.from_numpy(img.xp.reshape(-1).copy()).to(dev)
     d_vp = torch.from_numpy(img.vp.reshape(-1).copy()).to(dev)
     d_out = torch.zeros(8, dtype=torch.float32, device=dev)
-    s = torch.cuda.current_stream()
+    s = torch.cuda.Stream(dev)
     fk.kick_fine_device(d_rhoc, d_idx, d_xp, img.n_used, d_vp, d_out, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0,
                         stream=s)
     torch.cuda.synchronize()
-    np.testing.assert_array_equal(d_vp.cpu().numpy().reshape(-1, 3), vh)
+    vd = d_vp.cpu().numpy().reshape(-1, 3)
+    d_h, d_d = (vh - img.vp).astype(np.float64), (vd - img.vp).astype(np.float64)
+    assert np.sqrt(np.sum((d_d - d_h) ** 2) / np.sum(d_h ** 2)) < 1e-6
     o = d_out.cpu().numpy()
-    np.testing.assert_array_equal(o[:5], out_h)
+    np.testing.assert_allclose(o[:5], out_h, rtol=1e-5)
     assert o[5:6].view(np.int32)[0] == 0
 
 
