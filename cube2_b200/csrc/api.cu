@@ -575,7 +575,7 @@ static int run_pp(const Meta &m, const Dev &d, float mass, float kick, size_t &s
   b.err = ctr + 2;
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][2], g.stream));
   const size_t shm = sizeof(int32_t) * kWarps * m.max_rcp * m.max_rcp * m.max_rcp;
-  if (shm > 48 * 1024) return fail(CUBE_ERR_INVALID);
+  if (shm > 200 * 1024) return fail(CUBE_ERR_INVALID);  // rcp^3 sub-cell histograms per warp
   launch_pp_binning(b, g.stream);
   g.launches += 7;  // count, spill sort, 3 scan passes, scatter, spill placement
   CU(cudaGetLastError());

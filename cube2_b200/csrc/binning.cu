@@ -353,6 +353,10 @@ void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
   const int64_t warps = (int64_t)p.ntile * p.R3;
   const unsigned blocks = (unsigned)((warps + kWarps - 1) / kWarps);
   const size_t shm = sizeof(int32_t) * kWarps * p.max_rcp3;
+  if (shm > 48 * 1024) {  // fine levels (ratio_sf up to 12 or 16) need more than the default window
+    cudaFuncSetAttribute(k_pp_bin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    cudaFuncSetAttribute(k_pp_bin<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  }
   cudaMemsetAsync(a.spill_n, 0, sizeof(int32_t), s);
   k_pp_bin<false><<<blocks, kWarps * 32, shm, s>>>(p);
   k_spill_fix<<<1, 1024, 0, s>>>(a.spill, a.spill_rank, a.spill_n, p.spill_cap, a.count);

@@ -1,29 +1,39 @@
-// PP short-range pair force over the 27 neighbouring PP cells
-// (pp_force_kernel.c:282-325, pp_force_kernel.cu:192-250) and the kick of
-// the interior particles (pp_force_kernel.c:339-364).
+// PP short-range pair force over the neighbouring PP cells
+// (pp_force_kernel.c:282-325, pp_force_kernel.cu:192-250) and the kick of the
+// interior particles (pp_force_kernel.c:339-364).
 //
-// Work decomposition: an item is one interior PP cell (or a 32-particle chunk
-// of a crowded one).  The 27 neighbour cells of a cell form 9 contiguous
-// ranges of the cell-sorted array (three cells along x are adjacent in key
-// order).  Items are bucketed by cost (log2 of i-count x candidates) and a
+// Work decomposition.  An item is one interior PP cell, or a 32-particle chunk
+// of a crowded one.  A particle of range rc needs the cells within
+// R = ceil(rc * rcp / ratio_cs) of its own (pp_force_kernel.cu:205); the rows
+// (dy, dz) of that stencil whose nearest point is farther than rc are skipped,
+// and the cells of a row are one contiguous range of the cell-sorted array.
+// Items are bucketed by cost (log2 of candidates per lane group) and a
 // persistent kernel hands them out heaviest first through an atomic queue
 // head, so the lognormal occupancy of clustered boxes does not leave a tail.
 //
-// Inside an item one warp splits its 32 lanes into (i-particles) x (groups
-// over the j-candidates): for a cell with 8 particles, 4 lane groups each
-// walk a quarter of the candidates.  Candidates are staged through shared
-// memory by coalesced float4 loads and read back as broadcasts.  Each lane
-// accumulates in FP32 with Kahan compensation per staged tile; the groups'
-// partial sums are merged with warp shuffles (TwoSum), then the owning lane
-// applies af*mass^2, the kick, f2max and vmax.
+// Inside an item one warp splits its 32 lanes into floor(32/ni) groups of ni
+// lanes; lane (group g, particle i) walks every ngrp-th candidate.  Candidates
+// are staged per warp in shared memory (coalesced float4 loads, broadcast
+// reads).  Only about 15% of the stencil candidates lie inside the cutoff, so
+// evaluating the pair law for every candidate would spend most issue slots on
+// rejected pairs: instead each lane pushes its accepted (dx, dy, dz, r^2)
+// into its own shared-memory queue, and when any lane's queue is full the
+// warp drains all queues in lock-step rounds.  The pair law is evaluated
+// without divisions or branches (one rsqrt and a degree-6 Horner polynomial
+// with per-lane coefficient selection).  Each lane keeps Kahan-compensated
+// sums updated once per drain; the groups of a particle are merged with warp
+// shuffles (TwoSum), and the owning lane applies af*mass^2, the kick, f2max
+// and vmax.
 #include "common.cuh"
 
 namespace cube {
 
 constexpr int kPPThreads = 256;
 constexpr int kPPWarps = kPPThreads / 32;
-constexpr int kJTile = 128;  // staged candidates per warp
+constexpr int kJTile = 64;    // staged candidates per warp
+constexpr int kQ = 16;        // accepted-pair queue entries per lane
 constexpr int kBuckets = 32;
+constexpr size_t kPPSmem = sizeof(float4) * kPPWarps * (kJTile + kQ * 32);
 
 // basic_functions.f08:95-109 / pp_force_kernel.c:45-74 in FP32, same operation order
 __device__ __forceinline__ float F_ra(float r, float apm) {
@@ -42,6 +52,45 @@ __device__ __forceinline__ float F_ra(float r, float apm) {
   return 0.0f;
 }
 
+// F_ra(r,app) - F_ra(r,rc) for 0 < r < rc, as a function of r^2, with per-cell constants and
+// no division: for r > app it equals A/r^2 - sum_k c_k ep^k with ep = 2r/rc, where
+//   outer (ep > 1): A = 32/35 (the 12/ep^2 term folded in), c = [-224,896,-840,224,70,-48,7]/(35 rc^2)
+//   inner:          A = 1,                                  c = [0,224,0,-224,70,48,-21]/(35 rc^2)
+// Returns the scale s such that the pair force is s * (dx, dy, dz).
+struct PairLaw {
+  float cep, app2, app, rc;
+  float o0, o1, o2, o3, o4, o5, o6, n1, n3, n4, n5, n6;
+  __device__ __forceinline__ void init(float rc_, float app_) {
+    rc = rc_;
+    app = app_;
+    const float k35 = 1.0f / (35.0f * rc_ * rc_);
+    cep = 2.0f / rc_;
+    app2 = app_ * app_;
+    o0 = -224.f * k35, o1 = 896.f * k35, o2 = -840.f * k35, o3 = 224.f * k35, o4 = 70.f * k35, o5 = -48.f * k35,
+    o6 = 7.f * k35;
+    n1 = 224.f * k35, n3 = -224.f * k35, n4 = 70.f * k35, n5 = 48.f * k35, n6 = -21.f * k35;
+  }
+  __device__ __forceinline__ float scale(float r2) const {
+    const float invr = rsqrtf(r2);
+    const float ir2 = invr * invr;
+    const float ep = r2 * invr * cep;
+    const bool outer = ep > 1.0f;
+    float q = outer ? o6 : n6;
+    q = fmaf(q, ep, outer ? o5 : n5);
+    q = fmaf(q, ep, outer ? o4 : n4);
+    q = fmaf(q, ep, outer ? o3 : n3);
+    q = fmaf(q, ep, outer ? o2 : 0.0f);
+    q = fmaf(q, ep, outer ? o1 : n1);
+    q = fmaf(q, ep, outer ? o0 : 0.0f);
+    float fpp = fmaf(outer ? (32.0f / 35.0f) : 1.0f, ir2, -q);
+    if (r2 <= app2) {  // inside the softening length: the exact S2 law (rare)
+      const float r = r2 * invr;
+      fpp = F_ra(r, app) - F_ra(r, rc);
+    }
+    return fpp * invr;
+  }
+};
+
 __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   float y = x - c;
   float t = s + y;
@@ -59,7 +108,7 @@ __device__ __forceinline__ void two_sum_merge(float &hi, float &lo, float hi2, f
 }
 
 struct PPK {
-  int nt, ntt, nns, nnt, ntile;
+  int nt, ntt, nns, nnt, ntile, rcs;
   const TilePP *tiles;
   const int32_t *cs;
   const float4 *spos;
@@ -73,9 +122,25 @@ struct PPK {
   float *out;
   int want_vmax;
   int32_t *err;
-  int64_t max_cells;  // max interior PP cells per tile (grid sizing)
+  int64_t max_cells;          // max interior PP cells per tile (grid sizing)
   unsigned long long *pairs;  // COUNT mode: accepted ordered pairs
 };
+
+// PP range of the particles of interior cell (x, y, z) of tile t (per subtile, pp_force_kernel.cu:776-790)
+__device__ __forceinline__ float cell_range(const PPK &p, int t, int x, int y, int z, int rcp) {
+  const int tx = t % p.nnt, ty = (t / p.nnt) % p.nnt, tz = t / (p.nnt * p.nnt);
+  const int sx = (x / rcp - 1) / p.ntt, sy = (y / rcp - 1) / p.ntt, sz = (z / rcp - 1) / p.ntt;
+  return p.range_loc[(((tz * p.nnt + ty) * p.nnt + tx) * p.nns + sz) * p.nns * p.nns + sy * p.nns + sx];
+}
+
+// stencil radius in cells and the row test: row (dy, dz) can hold a particle within rc
+__device__ __forceinline__ int stencil_radius(float rc, int rcp, int rcs) {
+  return (int)ceilf(rc * (float)rcp / (float)rcs);
+}
+__device__ __forceinline__ bool row_needed(int dy, int dz, float h, float rc2) {
+  const float ay = (float)max(abs(dy) - 1, 0) * h, az = (float)max(abs(dz) - 1, 0) * h;
+  return ay * ay + az * az < rc2;
+}
 
 // cost bucket of a chunk with ni i-particles and nj candidates, heavy = high index:
 // the warp walks the candidates in floor(32/ni) lane groups
@@ -111,10 +176,16 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
     g = tp.cell0 + ((int64_t)z * S + y) * S + x;
     ni = p.cs[g + 1] - p.cs[g];
     if (ni > 0) {
-      for (int dz = -1; dz <= 1; dz++)
-        for (int dy = -1; dy <= 1; dy++) {
+      const float rc = cell_range(p, t, x, y, z, rcp);
+      const int R = stencil_radius(rc, rcp, p.rcs);
+      if (R > rcp) atomicOr(p.err, 1 << CUBE_ERR_INVALID);  // beyond the one coarse-cell halo
+      const float h = (float)p.rcs / (float)rcp;
+      const int Rc = min(R, rcp);
+      for (int dz = -Rc; dz <= Rc; dz++)
+        for (int dy = -Rc; dy <= Rc; dy++) {
+          if (!row_needed(dy, dz, h, rc * rc)) continue;
           const int64_t b = g + ((int64_t)dz * S + dy) * S;
-          nj += p.cs[b + 2] - p.cs[b - 1];
+          nj += p.cs[b + Rc + 1] - p.cs[b - Rc];
         }
       nchunks = (ni + 31) >> 5;
     }
@@ -160,10 +231,11 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
 // COUNT = false: forces and kick.  COUNT = true: only count the accepted ordered
 // pairs 0 < r^2 < rc^2 (the algorithmic work of the kick, for the roofline).
 template <bool COUNT>
-__global__ void __launch_bounds__(kPPThreads, 3) k_pp_force(PPK p) {
-  __shared__ float4 jbuf[kPPWarps][kJTile];
+__global__ void __launch_bounds__(kPPThreads, 2) k_pp_force(PPK p) {
+  extern __shared__ float4 pp_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float4 *buf = jbuf[warp];
+  float4 *buf = pp_smem + warp * (kJTile + kQ * 32);
+  float4 *queue = buf + kJTile;  // queue[k * 32 + lane]: entry k of this lane
   int total = 0;
   {
     int v = lane < kBuckets ? p.bucket[lane] : 0;
@@ -179,17 +251,17 @@ __global__ void __launch_bounds__(kPPThreads, 3) k_pp_force(PPK p) {
     if (it >= total) break;
     const int4 item = p.items[it];
     const int64_t g = (int64_t)(unsigned)item.x;
-    const TilePP tp = p.tiles[item.z];
+    const int t = item.z;
+    const TilePP tp = p.tiles[t];
     const int S = tp.S, rcp = tp.rcp;
     const int64_t loc = g - tp.cell0;
     const int x = (int)(loc % S), y = (int)((loc / S) % S), z = (int)(loc / ((int64_t)S * S));
-    // subtile of the i-cell -> per-subtile PP range (pp_force_kernel.cu:776-790)
-    const int t = item.z;
-    const int tx = t % p.nnt, ty = (t / p.nnt) % p.nnt, tz = t / (p.nnt * p.nnt);
-    const int sx = (x / rcp - 1) / p.ntt, sy = (y / rcp - 1) / p.ntt, sz = (z / rcp - 1) / p.ntt;
-    const int loc_sub = (((tz * p.nnt + ty) * p.nnt + tx) * p.nns + sz) * p.nns * p.nns + sy * p.nns + sx;
-    const float rc = p.range_loc[loc_sub];
+    const float rc = cell_range(p, t, x, y, z, rcp);
     const float rc2 = rc * rc;
+    const int R = min(stencil_radius(rc, rcp, p.rcs), rcp);
+    const float h = (float)p.rcs / (float)rcp;
+    PairLaw law;
+    law.init(rc, p.app);
 
     const int i0 = p.cs[g] + item.y * 32;
     const int ni = min(32, p.cs[g + 1] - i0);
@@ -199,64 +271,52 @@ __global__ void __launch_bounds__(kPPThreads, 3) k_pp_force(PPK p) {
     const bool has_i = grp < ngrp;  // the 32 mod ni leftover lanes idle
     const float4 pi = p.spos[i0 + il];
 
-    // F_ra(r,app) - F_ra(r,rc) (basic_functions.f08:95-109) with per-cell constants and no
-    // division: for r > app it equals A/r^2 - sum_k c_k ep^k, ep = 2r/rc, where
-    //   outer (ep > 1): A = 32/35 (the 12/ep^2 term folded in), c = [-224,896,-840,224,70,-48,7]/(35 rc^2)
-    //   inner:          A = 1,                                  c = [0,224,0,-224,70,48,-21]/(35 rc^2)
-    const float k35 = 1.0f / (35.0f * rc2);
-    const float cep = 2.0f / rc;
-    const float app2 = p.app * p.app;
-    const float o0 = -224.f * k35, o1 = 896.f * k35, o2 = -840.f * k35, o3 = 224.f * k35, o4 = 70.f * k35,
-                o5 = -48.f * k35, o6 = 7.f * k35;
-    const float n1 = 224.f * k35, n3 = -224.f * k35, n4 = 70.f * k35, n5 = 48.f * k35, n6 = -21.f * k35;
-
     float sx_ = 0.f, cx_ = 0.f, sy_ = 0.f, cy_ = 0.f, sz_ = 0.f, cz_ = 0.f;
-    for (int dz = -1; dz <= 1; dz++)
-      for (int dy = -1; dy <= 1; dy++) {
+    int cnt = 0;  // entries in this lane's queue
+    auto drain = [&]() {
+      const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+      float px = 0.f, py = 0.f, pz = 0.f;
+      for (int r = 0; r < rounds; r++) {
+        const float4 e = queue[r * 32 + lane];
+        if (r < cnt) {
+          const float s = law.scale(e.w);
+          px = fmaf(s, e.x, px);
+          py = fmaf(s, e.y, py);
+          pz = fmaf(s, e.z, pz);
+        }
+      }
+      kahan_add(sx_, cx_, px);
+      kahan_add(sy_, cy_, py);
+      kahan_add(sz_, cz_, pz);
+      cnt = 0;
+    };
+    for (int dz = -R; dz <= R; dz++)
+      for (int dy = -R; dy <= R; dy++) {
+        if (!row_needed(dy, dz, h, rc2)) continue;
         const int64_t b = g + ((int64_t)dz * S + dy) * S;
-        const int js = p.cs[b - 1], je = p.cs[b + 2];
+        const int js = p.cs[b - R], je = p.cs[b + R + 1];
         for (int jb = js; jb < je; jb += kJTile) {
           const int nb = min(kJTile, je - jb);
           __syncwarp();
           for (int q = lane; q < nb; q += 32) buf[q] = p.spos[jb + q];
           __syncwarp();
-          float px = 0.f, py = 0.f, pz = 0.f;
-#pragma unroll 4
-          for (int q = has_i ? grp : nb; q < nb; q += ngrp) {
-            const float4 pj = buf[q];
+          const int nsteps = (nb + ngrp - 1) / ngrp;
+          for (int k = 0; k < nsteps; k++) {
+            const int q = grp + k * ngrp;
+            const float4 pj = buf[q < nb ? q : nb - 1];
             const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
             const float r2 = dx * dx + dy_ * dy_ + dz_ * dz_;
-            const bool ok = (r2 > 0.0f) & (r2 < rc2);
+            const bool ok = has_i && (q < nb) && (r2 > 0.0f) && (r2 < rc2);
             if (COUNT) {
               npairs += ok ? 1ull : 0ull;
             } else {
-              const float invr = rsqrtf(r2);
-              const float ir2 = invr * invr;
-              const float ep = r2 * invr * cep;
-              const bool outer = ep > 1.0f;
-              float q6 = outer ? o6 : n6;
-              q6 = fmaf(q6, ep, outer ? o5 : n5);
-              q6 = fmaf(q6, ep, outer ? o4 : n4);
-              q6 = fmaf(q6, ep, outer ? o3 : n3);
-              q6 = fmaf(q6, ep, outer ? o2 : 0.0f);
-              q6 = fmaf(q6, ep, outer ? o1 : n1);
-              q6 = fmaf(q6, ep, outer ? o0 : 0.0f);
-              float fpp = fmaf(outer ? (32.0f / 35.0f) : 1.0f, ir2, -q6);
-              if (ok && r2 <= app2) {  // inside the softening length: the exact S2 law (rare)
-                const float r = r2 * invr;
-                fpp = F_ra(r, p.app) - F_ra(r, rc);
-              }
-              const float s = ok ? fpp * invr : 0.0f;
-              px = fmaf(s, dx, px);
-              py = fmaf(s, dy_, py);
-              pz = fmaf(s, dz_, pz);
+              if (ok) queue[cnt++ * 32 + lane] = make_float4(dx, dy_, dz_, r2);
+              if (__any_sync(0xffffffffu, cnt == kQ)) drain();
             }
           }
-          kahan_add(sx_, cx_, px);
-          kahan_add(sy_, cy_, py);
-          kahan_add(sz_, cz_, pz);
         }
       }
+    if (!COUNT) drain();
     // merge the lane groups of each i-particle (tree over groups, stride s*ni lanes);
     // Kahan c is the negated low part
     float hx = sx_, lx = -cx_, hy = sy_, ly = -cy_, hz = sz_, lz = -cz_;
@@ -312,6 +372,7 @@ static PPK make_ppk(const PPArgs &a) {
   p.nns = L.nns;
   p.nnt = L.nnt;
   p.ntile = L.ntile;
+  p.rcs = L.rcs;
   p.tiles = a.d_tiles;
   p.cs = a.cell_start;
   p.spos = a.spos;
@@ -343,13 +404,30 @@ void launch_pp_items(const PPArgs &a, cudaStream_t s) {
   k_pp_items<1><<<grid, 256, 0, s>>>(p);
 }
 
+// one persistent block per resident slot: blocks beyond the resident count would
+// only start once the queue is empty
+static int resident_blocks(const void *fn, int num_sms) {
+  static int cached[2] = {0, 0};
+  const int which = fn == (const void *)k_pp_force<true> ? 1 : 0;
+  if (!cached[which]) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPPSmem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPPThreads, kPPSmem);
+    cached[which] = per_sm > 0 ? per_sm : 1;
+  }
+  return cached[which] * num_sms;
+}
+
 void launch_pp_force(const PPArgs &a, cudaStream_t s) {
   PPK p = make_ppk(a);
   cudaMemsetAsync(a.head, 0, sizeof(int32_t), s);
-  if (a.pairs)
-    k_pp_force<true><<<a.num_sms * 4, kPPThreads, 0, s>>>(p);
-  else
-    k_pp_force<false><<<a.num_sms * 4, kPPThreads, 0, s>>>(p);
+  if (a.pairs) {
+    const void *fn = (const void *)k_pp_force<true>;
+    k_pp_force<true><<<resident_blocks(fn, a.num_sms), kPPThreads, kPPSmem, s>>>(p);
+  } else {
+    const void *fn = (const void *)k_pp_force<false>;
+    k_pp_force<false><<<resident_blocks(fn, a.num_sms), kPPThreads, kPPSmem, s>>>(p);
+  }
 }
 
 }  // namespace cube

@@ -96,6 +96,41 @@ def test_pp_repeatable(gpu):
     np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("levels", [(2, 3), (3, 4), (2, 6)])
+def test_pp_mixed_levels_in_one_tile(gpu, levels):
+    """Subtiles of one parent tile at different levels: the tile's PP grid takes the finest
+    ratio_sf, and every particle keeps the range of its own subtile, so a particle of the
+    coarser level searches R = ceil(rc*rcp/ratio_cs) > 1 cells (pp_force_kernel.cu:205)."""
+    from cube2_b200 import ic
+    from cube2_b200.kick import FineKick
+    from cube2_b200.layout import RATIO_SF, Layout, apm3_table, build_image, encode_positions, ixyz3_table
+    from oracle.pp_direct import pp_forces
+    L = Layout(ng=32, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1)
+    pos, vel = ic.uniform_random(12000, 32.0, 31)
+    img = build_image(pos, vel, L)
+    ix = ixyz3_table(L)
+    ires = np.array([levels[(k % 3) == 0] for k in range(L.ns3)], np.int32)
+    apm3 = apm3_table(3.5)
+    vp, _, _, _, _ = FineKick(L).c_pp_force_kernel(img, np.arange(1, L.ns3 + 1, dtype=np.int32), ires, ix, apm3,
+                                                   RATIO_SF, 1.0, SIXPI, 1.0, vp=np.zeros_like(img.vp))
+    # range of each physical particle from its subtile
+    cc, u = encode_positions(pos, 4, 8)
+    posq = (cc + (u.astype(np.float64) + 0.5) / 65536.0) * 4.0
+    tx, ty, tz = cc[:, 0] // L.nt, cc[:, 1] // L.nt, cc[:, 2] // L.nt
+    sx, sy, sz = (cc[:, 0] % L.nt) // L.ntt, (cc[:, 1] % L.nt) // L.ntt, (cc[:, 2] % L.nt) // L.ntt
+    loc = (((tz * 2 + ty) * 2 + tx) * 2 + sz) * 4 + sy * 2 + sx
+    it_of_loc = np.zeros(L.ns3, np.int64)
+    for it, r in enumerate(ix):
+        it_of_loc[(((r[5] - 1) * 2 + r[4] - 1) * 2 + r[3] - 1) * 8 + (r[2] - 1) * 4 + (r[1] - 1) * 2 + r[0] - 1] = it
+    ranges = apm3[ires[it_of_loc[loc]] - 1].astype(np.float64)
+    F = pp_forces(posq, 32.0, 0.1, ranges)
+    kick = float(np.float32(SIXPI) / np.float32(6.0)) / np.pi
+    mine = np.zeros_like(F)
+    act = img.active
+    mine[img.pid[act]] = vp[act].astype(np.float64) / kick
+    assert _rel_rms(mine, F) < TOL
+
+
 def test_pair_count_matches_kdtree(gpu):
     """The algorithmic work counter: ordered pairs 0 < r < 2 in the periodic box (scipy cKDTree)."""
     from scipy.spatial import cKDTree
