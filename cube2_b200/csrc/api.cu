@@ -217,7 +217,13 @@ static int get_plan(int n, int batch, cufftType type, cufftHandle *out) {
     }
   Plan p{n, batch, type, 0};
   int dims[3] = {n, n, n};
-  CF(cufftPlanMany(&p.h, 3, dims, nullptr, 1, 0, nullptr, 1, 0, type, batch));
+  if (type == CUFFT_C2R) {
+    // the three force components of one mesh, written interleaved: out[4*point + component]
+    int iemb[3] = {n, n, n / 2 + 1}, oemb[3] = {n, n, n};
+    CF(cufftPlanMany(&p.h, 3, dims, iemb, 1, n * n * (n / 2 + 1), oemb, 4, 1, type, batch));
+  } else {
+    CF(cufftPlanMany(&p.h, 3, dims, nullptr, 1, 0, nullptr, 1, 0, type, batch));
+  }
   CF(cufftSetStream(p.h, g.stream));
   g.plans.push_back(p);
   *out = p.h;
@@ -381,7 +387,7 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     CK(grow(g.rho, sizeof(float) * n3));
     CK(grow(g.rhok, sizeof(cufftComplex) * nk));
     CK(grow(g.fk, sizeof(cufftComplex) * nk * 3));
-    CK(grow(g.force, sizeof(float) * n3 * 3));
+    CK(grow(g.force, sizeof(float) * n3 * 4));  // interleaved (Fx, Fy, Fz, -)
     const double scale = (double)L.rcs / (double)(1.0f / (float)rsf);
     std::vector<MeshJob> jobs(L.ntile);
     for (int t = 0; t < L.ntile; t++) {
@@ -468,7 +474,7 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       CK(grow(g.rho, sizeof(float) * n3 * nb));
       CK(grow(g.rhok, sizeof(cufftComplex) * nk * nb));
       CK(grow(g.fk, sizeof(cufftComplex) * nk * 3 * nb));
-      CK(grow(g.force, sizeof(float) * n3 * 3 * nb));
+      CK(grow(g.force, sizeof(float) * n3 * 4 * nb));
       std::vector<MeshJob> jobs(nj);
       for (int j = 0; j < nj; j++) {
         const int loc = locs[j0 + j];
@@ -518,12 +524,13 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       a.want_vmax = want_vmax;
       cufftHandle fw, bw;
       CK(get_plan(n, nb, CUFFT_R2C, &fw));
-      CK(get_plan(n, 3 * nb, CUFFT_C2R, &bw));
+      CK(get_plan(n, 3, CUFFT_C2R, &bw));
       CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3 * nb, g.stream));
       launch_pm3_deposit(a, g.stream);
       CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
       launch_pm3_kspace(a, g.stream);
-      CF(cufftExecC2R(bw, (cufftComplex *)g.fk.p, (cufftReal *)g.force.p));
+      for (int sl = 0; sl < nj; sl++)  // interleaved output: one 3-component transform per mesh
+        CF(cufftExecC2R(bw, (cufftComplex *)g.fk.p + (size_t)sl * 3 * nk, (cufftReal *)g.force.p + (size_t)sl * 4 * n3));
       a.nslots = nj;  // f2max over the real jobs only
       launch_pm3_f2max(a, g.stream);
       launch_pm3_gather(a, g.stream);
@@ -574,8 +581,8 @@ static int run_pp(const Meta &m, const Dev &d, float mass, float kick, size_t &s
   b.scan_tmp = (int32_t *)g.scan_tmp.p;
   b.err = ctr + 2;
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][2], g.stream));
-  const size_t shm = sizeof(int32_t) * kWarps * m.max_rcp * m.max_rcp * m.max_rcp;
-  if (shm > 200 * 1024) return fail(CUBE_ERR_INVALID);  // rcp^3 sub-cell histograms per warp
+  if (bin_smem_bytes(m.max_rcp) > 200 * 1024) return fail(CUBE_ERR_INVALID);  // rcp^3 histograms per warp
+  b.spatial = 1;
   launch_pp_binning(b, g.stream);
   g.launches += 7;  // count, spill sort, 3 scan passes, scatter, spill placement
   CU(cudaGetLastError());
@@ -925,8 +932,8 @@ void c_gpu_velocity_finalize(void) {
 }
 
 int cube_pp_bin_tile(const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf, const int32_t *rhoc,
-                     const int64_t *idx_b_r, const int16_t *xp, int32_t tile, uint32_t *keys, int64_t *ip,
-                     int32_t *cell_start, float *xf, int64_t cap_n, int64_t cap_grid, int64_t *n_out,
+                     const int64_t *idx_b_r, const int16_t *xp, int32_t tile, int32_t spatial, uint32_t *keys,
+                     int64_t *ip, int32_t *cell_start, float *xf, int64_t cap_n, int64_t cap_grid, int64_t *n_out,
                      int64_t *grid_out) {
   std::lock_guard<std::mutex> lk(g_mu);
   t_last_error = CUBE_OK;
@@ -978,6 +985,8 @@ int cube_pp_bin_tile(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   b.spill_cap = 2048;
   b.scan_tmp = (int32_t *)g.scan_tmp.p;
   b.err = ctr + 2;
+  b.spatial = spatial ? 1 : 0;
+  if (bin_smem_bytes(m.max_rcp) > 200 * 1024) return fail(CUBE_ERR_INVALID);
   launch_pp_binning(b, g.stream);
   CU(cudaGetLastError());
   CK(stage_end());

@@ -16,6 +16,13 @@
 // index) and placed ahead of the home particles of their cell, which is where
 // the stable sort puts them: every source of a spill precedes the home cell in
 // storage order.
+//
+// Spatial order (used by the kick, not by the parity view): with rcp dividing
+// 8, pass 2 can instead order the particles inside each PP cell by the Morton
+// index of their 1/8-coarse-cell sub-cell (then storage order).  Keys and
+// cell_start are unchanged; 32-particle chunks of a crowded cell then occupy
+// a compact sub-volume, which lets the PP kernel prune candidates against the
+// chunk's bounding box.
 #include <cstdio>
 
 #include "common.cuh"
@@ -44,6 +51,8 @@ struct BinK {
   int nt, ncb, nte, rcs, R, ntile;
   int64_t R3;
   int max_rcp3;
+  int hist_words;  // shared ints per warp
+  int spatial;     // order inside a PP cell by Morton sub-cell (rcp must divide 8)
   const TilePP *tiles;
   const int16_t *xp;
   const int32_t *rhoc;
@@ -74,6 +83,12 @@ __device__ __forceinline__ int spill_count_of(const Spill *sp, int n, int64_t g)
   return lo - a;
 }
 
+// Morton interleave of up to 2 bits per axis
+__device__ __forceinline__ int morton2(int x, int y, int z) {
+  auto sp = [](int v) { return (v & 1) | ((v & 2) << 2); };
+  return sp(x) | (sp(y) << 1) | (sp(z) << 2);
+}
+
 // Pass 1 (SCATTER = false): per-sub-cell counts, spill collection.
 // Pass 2 (SCATTER = true): stable placement into spos.
 template <bool SCATTER>
@@ -87,7 +102,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
   const int cx = (int)(rem % p.R), cy = (int)((rem / p.R) % p.R), cz = (int)(rem / ((int64_t)p.R * p.R));
   const TilePP tp = p.tiles[t];
   const int rcp = tp.rcp, S = tp.S, rcp3 = rcp * rcp * rcp;
-  int32_t *hist = sh_hist + warp * p.max_rcp3;
+  int32_t *hist = sh_hist + warp * p.hist_words;
   // extended-tile C index of this region cell and its tile-local coarse coordinate (may be -1 or nt)
   const int ci = p.ncb - 1 + cx, cj = p.ncb - 1 + cy, ck = p.ncb - 1 + cz;
   const int64_t cidx = (((int64_t)t * p.nte + ck) * p.nte + cj) * p.nte + ci;
@@ -95,39 +110,89 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
   const int64_t base = p.cell_base[cidx];
   const int lx = cx - 1, ly = cy - 1, lz = cz - 1;
   const int nspill = SCATTER ? min(*p.spill_n, p.spill_cap) : 0;
+  // spatial order: bins = (PP sub-cell b, Morton index of the 1/8-coarse-cell sub-cell inside b)
+  const bool spatial = SCATTER && p.spatial && (rcp == 2 || rcp == 4);
+  const int fs = spatial ? 8 / rcp : 1, s3 = fs * fs * fs;
+  const int nbins = rcp3 * s3;
+  int32_t *pre = hist + nbins;  // exclusive prefix of the bins (spatial order only)
 
-  for (int b = lane; b < rcp3; b += 32) hist[b] = 0;
+  // key, spill flag and bin of particle l of this coarse cell (pp_force_kernel.c:213-236)
+  auto classify = [&](int l, float &x, float &y, float &z, bool &spilled, bool &bad, int &b, int &bin,
+                      int64_t &gkey) {
+    const int16_t *q = p.xp + 3 * (base + l);
+    // pp_force_kernel.c:213-218: (float)((i-ncb) + ((int16)(xp+ishift)+rshift)*x_resolution)
+    x = __double2float_rn(decode_pos(lx, q[0]));
+    y = __double2float_rn(decode_pos(ly, q[1]));
+    z = __double2float_rn(decode_pos(lz, q[2]));
+    // pp_force_kernel.c:226-228: floor(rcp * (x - utile_shift*ntt)) + rcp, float product
+    int kx = (int)floorf(__fmul_rn((float)rcp, x)) + rcp;
+    int ky = (int)floorf(__fmul_rn((float)rcp, y)) + rcp;
+    int kz = (int)floorf(__fmul_rn((float)rcp, z)) + rcp;
+    // keys beyond the tile grid (float rounding at the outer halo face) are clamped
+    kx = min(max(kx, 0), S - 1);
+    ky = min(max(ky, 0), S - 1);
+    kz = min(max(kz, 0), S - 1);
+    const int rx = kx - rcp * cx, ry = ky - rcp * cy, rz = kz - rcp * cz;
+    spilled = (rx >= rcp) | (ry >= rcp) | (rz >= rcp);
+    // a key below its own coarse cell cannot come from the float path; reject it
+    bad = (rx < 0) | (ry < 0) | (rz < 0) | (rx > rcp) | (ry > rcp) | (rz > rcp);
+    b = (rz * rcp + ry) * rcp + rx;
+    gkey = tp.cell0 + ((int64_t)kz * S + ky) * S + kx;
+    bin = b;
+    if (spatial && !spilled && !bad) {
+      // 1/8-coarse-cell sub-cell of the same float position, relative to the PP sub-cell
+      const int fx = min(max((int)floorf(__fmul_rn(8.f, x)) - 8 * lx, 0), 7);
+      const int fy = min(max((int)floorf(__fmul_rn(8.f, y)) - 8 * ly, 0), 7);
+      const int fz = min(max((int)floorf(__fmul_rn(8.f, z)) - 8 * lz, 0), 7);
+      bin = b * s3 + morton2(fx % fs, fy % fs, fz % fs);
+    }
+  };
+
+  for (int q = lane; q < nbins; q += 32) hist[q] = 0;
   __syncwarp();
+
+  if (spatial) {
+    // histogram of the bins, then an exclusive prefix per PP sub-cell
+    for (int l0 = 0; l0 < np; l0 += 32) {
+      const int l = l0 + lane;
+      if (l < np) {
+        float x, y, z;
+        bool spilled, bad;
+        int b, bin;
+        int64_t gkey;
+        classify(l, x, y, z, spilled, bad, b, bin, gkey);
+        if (!spilled && !bad) atomicAdd(&hist[bin], 1);
+      }
+    }
+    __syncwarp();
+    for (int b = 0; b < rcp3; b++) {  // s3 <= 64 bins per PP sub-cell: two per lane
+      const int q0 = b * s3 + 2 * lane;
+      const int v0 = 2 * lane < s3 ? hist[q0] : 0, v1 = 2 * lane + 1 < s3 ? hist[q0 + 1] : 0;
+      int incl = v0 + v1;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+      }
+      const int ex = incl - v0 - v1;
+      if (2 * lane < s3) pre[q0] = ex;
+      if (2 * lane + 1 < s3) pre[q0 + 1] = ex + v0;
+    }
+    __syncwarp();
+    for (int q = lane; q < nbins; q += 32) hist[q] = 0;
+    __syncwarp();
+  }
 
   for (int l0 = 0; l0 < np; l0 += 32) {
     const int l = l0 + lane;
     const bool valid = l < np;
     bool spilled = false, bad = false;
-    int b = 0;
+    int b = 0, bin = 0;
     int64_t gkey = 0;
     float x = 0.f, y = 0.f, z = 0.f;
-    int64_t ip = base + l;
+    const int64_t ip = base + l;
     if (valid) {
-      const int16_t *q = p.xp + 3 * ip;
-      // pp_force_kernel.c:213-218: (float)((i-ncb) + ((int16)(xp+ishift)+rshift)*x_resolution)
-      x = __double2float_rn(decode_pos(lx, q[0]));
-      y = __double2float_rn(decode_pos(ly, q[1]));
-      z = __double2float_rn(decode_pos(lz, q[2]));
-      // pp_force_kernel.c:226-228: floor(rcp * (x - utile_shift*ntt)) + rcp, float product
-      int kx = (int)floorf(__fmul_rn((float)rcp, x)) + rcp;
-      int ky = (int)floorf(__fmul_rn((float)rcp, y)) + rcp;
-      int kz = (int)floorf(__fmul_rn((float)rcp, z)) + rcp;
-      // keys beyond the tile grid (float rounding at the outer halo face) are clamped
-      kx = min(max(kx, 0), S - 1);
-      ky = min(max(ky, 0), S - 1);
-      kz = min(max(kz, 0), S - 1);
-      const int rx = kx - rcp * cx, ry = ky - rcp * cy, rz = kz - rcp * cz;
-      spilled = (rx >= rcp) | (ry >= rcp) | (rz >= rcp);
-      // a key below its own coarse cell cannot come from the float path; reject it
-      bad = (rx < 0) | (ry < 0) | (rz < 0) | (rx > rcp) | (ry > rcp) | (rz > rcp);
+      classify(l, x, y, z, spilled, bad, b, bin, gkey);
       if (bad) atomicOr(p.err, 1 << CUBE_ERR_INVALID);
-      b = (rz * rcp + ry) * rcp + rx;
-      gkey = tp.cell0 + ((int64_t)kz * S + ky) * S + kx;
     }
     const bool home = valid && !spilled && !bad;
     if (!SCATTER) {
@@ -149,9 +214,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
       int hb = 0, rank = 0;
       unsigned peers = 0;
       if (home) {
-        peers = __match_any_sync(hm, b);
+        peers = __match_any_sync(hm, bin);
         rank = __popc(peers & ((1u << lane) - 1u));
-        hb = hist[b];
+        hb = hist[bin] + (spatial ? pre[bin] : 0);
       }
       __syncwarp();
       if (home) {
@@ -160,7 +225,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
         const int64_t pos = (int64_t)p.cell_start[gkey] + off + hb + rank;
         p.spos[pos] = make_float4(__fmul_rn((float)p.rcs, x), __fmul_rn((float)p.rcs, y),
                                   __fmul_rn((float)p.rcs, z), __int_as_float((int)ip));
-        if (rank == 0) hist[b] = hb + __popc(peers);
+        if (rank == 0) hist[bin] += __popc(peers);
       }
       __syncwarp();
     }
@@ -338,6 +403,9 @@ void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
   p.ntile = L.ntile;
   p.R3 = (int64_t)p.R * p.R * p.R;
   p.max_rcp3 = a.max_rcp * a.max_rcp * a.max_rcp;
+  p.spatial = a.spatial;
+  // histogram words per warp: rcp^3 PP sub-cells, at least 2 x 512 bins for the spatial order
+  p.hist_words = p.max_rcp3 < 1024 ? 1024 : p.max_rcp3;
   p.tiles = a.d_tiles;
   p.xp = a.xp;
   p.rhoc = a.rhoc;
@@ -352,7 +420,7 @@ void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
   p.err = a.err;
   const int64_t warps = (int64_t)p.ntile * p.R3;
   const unsigned blocks = (unsigned)((warps + kWarps - 1) / kWarps);
-  const size_t shm = sizeof(int32_t) * kWarps * p.max_rcp3;
+  const size_t shm = sizeof(int32_t) * kWarps * p.hist_words;
   if (shm > 48 * 1024) {  // fine levels (ratio_sf up to 12 or 16) need more than the default window
     cudaFuncSetAttribute(k_pp_bin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     cudaFuncSetAttribute(k_pp_bin<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -363,6 +431,11 @@ void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
   scan_exclusive(a.count, a.ncells, a.cell_start, a.scan_tmp, s);
   k_pp_bin<true><<<blocks, kWarps * 32, shm, s>>>(p);
   k_spill_place<<<8, 256, 0, s>>>(p);
+}
+
+size_t bin_smem_bytes(int max_rcp) {
+  const int r3 = max_rcp * max_rcp * max_rcp;
+  return sizeof(int32_t) * kWarps * (r3 < 1024 ? 1024 : r3);
 }
 
 }  // namespace cube

@@ -95,8 +95,10 @@ struct BinArgs {
   int spill_cap;
   int32_t *scan_tmp;      // scan scratch
   int32_t *err;           // device error word
+  int spatial;            // 1: order inside each PP cell by Morton sub-cell (kick); 0: reference order
 };
 void launch_pp_binning(const BinArgs &a, cudaStream_t s);
+size_t bin_smem_bytes(int max_rcp);
 size_t scan_tmp_elems(int64_t n);
 
 // PP work list + force

@@ -2,18 +2,21 @@
 //
 // Pipeline per batch of meshes:
 //   deposit  TSC weights of every particle of the job's coarse cells into the
-//            mesh (kick.f90:420-468); one warp per coarse cell, shared-memory
-//            free first version with global float atomics;
+//            mesh (kick.f90:420-468); one warp per coarse cell, float atomics
+//            (the cost follows the particles, not the mesh, which matters for
+//            clustered boxes where most mesh bricks are nearly empty);
 //   R2C      cuFFT;
 //   k-space  one kernel multiplies by the Green table and by the spectral
 //            symbol of the 4-point difference, i*D(k) with
 //            D = a sin k + (1-a) sin 2k / 2, a = 4/3 -- the exact Fourier image
 //            of potential_to_force (kick.f90:545-568) on the FFT mesh -- and
 //            writes the three force spectra;
-//   C2R      cuFFT, batched over the 3 components;
-//   f2max    max |F|^2 over the physical mesh points (kick.f90:494);
-//   gather   TSC gather of the force at each active particle and the kick
-//            vp += dv * a_mid*dt/(6 pi) (kick.f90:497-540).
+//   C2R      cuFFT, batched over the 3 components and written interleaved
+//            (output stride 4): force[point] = (Fx, Fy, Fz, unused);
+//   f2max    max |F|^2 over the physical mesh points (kick.f90:494), one
+//            16-byte load per point;
+//   gather   TSC gather of the force at each active particle (27 16-byte loads)
+//            and the kick vp += dv * a_mid*dt/(6 pi) (kick.f90:497-540).
 #include <cmath>
 
 #include "common.cuh"
@@ -34,7 +37,7 @@ struct PM3K {
   float *rho;
   const cufftComplex *rhok;
   cufftComplex *fk;
-  const float *force;
+  const float4 *force;  // [slot][n^3] interleaved (Fx, Fy, Fz, -)
   const float *green;
   const float *dtab;
   float gscale;  // mass / n^3
@@ -129,10 +132,8 @@ __global__ void k_f2max(PM3K p) {
     const int64_t r = e - slot * nph;
     const int64_t x = r % p.fphys_n + p.fphys_lo, y = (r / p.fphys_n) % p.fphys_n + p.fphys_lo,
                   z = r / ((int64_t)p.fphys_n * p.fphys_n) + p.fphys_lo;
-    const int64_t q = (z * n + y) * n + x;
-    const float *F = p.force + (int64_t)slot * 3 * p.n3;
-    const float a = F[q], b = F[p.n3 + q], c = F[2 * p.n3 + q];
-    m = fmaxf(m, a * a + b * b + c * c);
+    const float4 f = __ldg(p.force + (int64_t)slot * p.n3 + (z * n + y) * n + x);
+    m = fmaxf(m, f.x * f.x + f.y * f.y + f.z * f.z);
   }
   m = warp_max(m);
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&p.out[0], m);
@@ -153,8 +154,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_gather(PM3K p) {
     const int64_t cidx = (((int64_t)J.t * p.nte + ck) * p.nte + cj) * p.nte + ci;
     const int np = p.rhoc[cidx];
     const int64_t base = p.cell_base[cidx];
-    const float *F = p.force + (int64_t)J.slot * 3 * p.n3;
-    const int64_t n = p.n, n3 = p.n3;
+    const float4 *F = p.force + (int64_t)J.slot * p.n3;
+    const int64_t n = p.n;
     for (int l = lane; l < np; l += 32) {
       const int64_t ip = base + l;
       const int16_t *q = p.xp + 3 * ip;
@@ -172,11 +173,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_gather(PM3K p) {
 #pragma unroll
           for (int a = 0; a < 3; a++) {
             const int64_t X = p.wrap ? wrapi(ix + a - 1, n) : ix + a - 1;
-            const int64_t m = (Z * n + Y) * n + X;
+            const float4 f = __ldg(F + (Z * n + Y) * n + X);
             const float w = (wx[a] * wy[b]) * wz[c];
-            d0 += F[m] * w;
-            d1 += F[n3 + m] * w;
-            d2 += F[2 * n3 + m] * w;
+            d0 += f.x * w;
+            d1 += f.y * w;
+            d2 += f.z * w;
           }
         }
       }
@@ -200,244 +201,6 @@ __global__ void __launch_bounds__(kWarps * 32) k_gather(PM3K p) {
       atomic_max_nonneg(&p.out[4], vm2);
     }
   }
-}
-
-// ---------------------------------------------------------------------------------------------
-// Brick-tiled deposit and gather.  A brick is BC^3 coarse cells of one job; its
-// particles touch mesh points [m0 - 1, m0 + BC*cm] per axis (cm = mesh cells per
-// coarse cell), held in a shared-memory tile that is 8 points wider in x so that
-// every float4 group of a mesh row is 16-byte aligned.  The deposit accumulates
-// with shared-memory atomics and flushes non-zero float4 groups with vector
-// global atomics; the gather loads the three force tiles with float4 loads and
-// reads the 27 TSC points from shared memory.
-
-struct TileGeom {
-  int cm, bc;         // mesh cells per coarse cell, coarse cells per brick side
-  int tx, ty;         // tile extent (x; y = z)
-  int nb[3];          // bricks per job per axis
-};
-
-__device__ __forceinline__ void brick_of(const PM3K &p, const TileGeom &tg, const int *rd, const int *lo0,
-                                         const MeshJob &J, int64_t b, int lo[3], int hi[3], int64_t m0[3]) {
-  const int bx = (int)(b % tg.nb[0]), by = (int)((b / tg.nb[0]) % tg.nb[1]),
-            bz = (int)(b / ((int64_t)tg.nb[0] * tg.nb[1]));
-  const int bb[3] = {bx, by, bz};
-  for (int d = 0; d < 3; d++) {
-    lo[d] = lo0[d] + bb[d] * tg.bc;
-    hi[d] = min(lo[d] + tg.bc, lo0[d] + rd[d]);
-    m0[d] = (int64_t)(lo[d] - p.ncb) * tg.cm - (int64_t)llrint(J.off[d]) + p.shift;
-  }
-}
-
-__global__ void __launch_bounds__(256) k_deposit_tile(PM3K p, TileGeom tg) {
-  extern __shared__ float tile[];
-  const int64_t per_job = (int64_t)tg.nb[0] * tg.nb[1] * tg.nb[2];
-  const int j = (int)(blockIdx.x / per_job);
-  const int64_t b = blockIdx.x - (int64_t)j * per_job;
-  const MeshJob J = p.jobs[j];
-  int lo[3], hi[3];
-  int64_t m0[3];
-  brick_of(p, tg, p.rdep, J.lo, J, b, lo, hi, m0);
-  const int tx = tg.tx, ty = tg.ty, tsz = tx * ty * ty;
-  for (int q = threadIdx.x; q < tsz; q += blockDim.x) tile[q] = 0.f;
-  __syncthreads();
-  const int64_t ox = m0[0] - 4, oy = m0[1] - 1, oz = m0[2] - 1;
-  float *R = p.rho + (int64_t)J.slot * p.n3;
-  const int64_t n = p.n;
-  for (int ck = lo[2]; ck < hi[2]; ck++)
-    for (int cj = lo[1]; cj < hi[1]; cj++)
-      for (int ci = lo[0]; ci < hi[0]; ci++) {
-        const int64_t cidx = (((int64_t)J.t * p.nte + ck) * p.nte + cj) * p.nte + ci;
-        const int np = p.rhoc[cidx];
-        const int64_t base = p.cell_base[cidx];
-        for (int l = threadIdx.x; l < np; l += blockDim.x) {
-          const int16_t *q = p.xp + 3 * (base + l);
-          float wx[3], wy[3], wz[3];
-          const int64_t ix = tsc(decode_pos(ci - p.ncb, q[0]) * p.scale - J.off[0], wx) + p.shift;
-          const int64_t iy = tsc(decode_pos(cj - p.ncb, q[1]) * p.scale - J.off[1], wy) + p.shift;
-          const int64_t iz = tsc(decode_pos(ck - p.ncb, q[2]) * p.scale - J.off[2], wz) + p.shift;
-          // tile-local corner of the 3x3x3 stencil
-          const int lx0 = (int)(ix - ox) - 1, ly0 = (int)(iy - oy) - 1, lz0 = (int)(iz - oz) - 1;
-          if (lx0 >= 0 && lx0 + 2 < tx && ly0 >= 0 && ly0 + 2 < ty && lz0 >= 0 && lz0 + 2 < ty) {
-            float *t0 = tile + (lz0 * ty + ly0) * tx + lx0;
-#pragma unroll
-            for (int c = 0; c < 3; c++)
-#pragma unroll
-              for (int bq = 0; bq < 3; bq++)
-#pragma unroll
-                for (int a = 0; a < 3; a++) atomicAdd(t0 + (c * ty + bq) * tx + a, (wx[a] * wy[bq]) * wz[c]);
-          } else {  // outside the tile (not reached for exact mesh scales): straight to global
-            for (int c = 0; c < 3; c++)
-              for (int bq = 0; bq < 3; bq++)
-                for (int a = 0; a < 3; a++) {
-                  int64_t X = ix + a - 1, Y = iy + bq - 1, Z = iz + c - 1;
-                  if (p.wrap) {
-                    X = wrapi(X, n);
-                    Y = wrapi(Y, n);
-                    Z = wrapi(Z, n);
-                  } else if (X < 0 || X >= n || Y < 0 || Y >= n || Z < 0 || Z >= n) {
-                    continue;
-                  }
-                  atomicAdd(R + (Z * n + Y) * n + X, (wx[a] * wy[bq]) * wz[c]);
-                }
-          }
-        }
-      }
-  __syncthreads();
-  const int g4 = tx / 4, ngroups = g4 * ty * ty;
-  const float4 *t4 = reinterpret_cast<const float4 *>(tile);
-  for (int q = threadIdx.x; q < ngroups; q += blockDim.x) {
-    const float4 v = t4[q];
-    if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
-    const int gx = q % g4, gy = (q / g4) % ty, gz = q / (g4 * ty);
-    int64_t X = ox + 4 * gx, Y = oy + gy, Z = oz + gz;
-    if (p.wrap) {
-      X = wrapi(X, n);
-      Y = wrapi(Y, n);
-      Z = wrapi(Z, n);
-    } else if (X < 0 || X >= n || Y < 0 || Y >= n || Z < 0 || Z >= n) {
-      continue;
-    }
-    atomicAdd(reinterpret_cast<float4 *>(R + (Z * n + Y) * n + X), v);
-  }
-}
-
-__global__ void __launch_bounds__(256) k_gather_tile(PM3K p, TileGeom tg) {
-  extern __shared__ float ftile[];
-  const int64_t per_job = (int64_t)tg.nb[0] * tg.nb[1] * tg.nb[2];
-  const int j = (int)(blockIdx.x / per_job);
-  const int64_t b = blockIdx.x - (int64_t)j * per_job;
-  const MeshJob J = p.jobs[j];
-  int lo[3], hi[3];
-  int64_t m0[3];
-  brick_of(p, tg, p.ract, J.alo, J, b, lo, hi, m0);
-  const int tx = tg.tx, ty = tg.ty, tsz = tx * ty * ty;
-  const int64_t ox = m0[0] - 4, oy = m0[1] - 1, oz = m0[2] - 1;
-  const int64_t n = p.n, n3 = p.n3;
-  const float *F = p.force + (int64_t)J.slot * 3 * n3;
-  const int g4 = tx / 4, ngroups = g4 * ty * ty;
-  float4 *t4 = reinterpret_cast<float4 *>(ftile);
-  for (int q = threadIdx.x; q < 3 * ngroups; q += blockDim.x) {
-    const int c = q / ngroups, r = q - c * ngroups;
-    const int gx = r % g4, gy = (r / g4) % ty, gz = r / (g4 * ty);
-    int64_t X = ox + 4 * gx, Y = oy + gy, Z = oz + gz;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    bool in = true;
-    if (p.wrap) {
-      X = wrapi(X, n);
-      Y = wrapi(Y, n);
-      Z = wrapi(Z, n);
-    } else {
-      in = X >= 0 && X < n && Y >= 0 && Y < n && Z >= 0 && Z < n;
-    }
-    if (in) v = __ldg(reinterpret_cast<const float4 *>(F + c * n3 + (Z * n + Y) * n + X));
-    t4[q] = v;
-  }
-  __syncthreads();
-  float vm0 = 0.f, vm1 = 0.f, vm2 = 0.f;
-  for (int ck = lo[2]; ck < hi[2]; ck++)
-    for (int cj = lo[1]; cj < hi[1]; cj++)
-      for (int ci = lo[0]; ci < hi[0]; ci++) {
-        const int64_t cidx = (((int64_t)J.t * p.nte + ck) * p.nte + cj) * p.nte + ci;
-        const int np = p.rhoc[cidx];
-        const int64_t base = p.cell_base[cidx];
-        for (int l = threadIdx.x; l < np; l += blockDim.x) {
-          const int64_t ip = base + l;
-          const int16_t *q = p.xp + 3 * ip;
-          float wx[3], wy[3], wz[3];
-          const int64_t ix = tsc(decode_pos(ci - p.ncb, q[0]) * p.scale - J.off[0], wx) + p.shift;
-          const int64_t iy = tsc(decode_pos(cj - p.ncb, q[1]) * p.scale - J.off[1], wy) + p.shift;
-          const int64_t iz = tsc(decode_pos(ck - p.ncb, q[2]) * p.scale - J.off[2], wz) + p.shift;
-          float d0 = 0.f, d1 = 0.f, d2 = 0.f;
-          const int lx0 = (int)(ix - ox) - 1, ly0 = (int)(iy - oy) - 1, lz0 = (int)(iz - oz) - 1;
-          if (lx0 >= 0 && lx0 + 2 < tx && ly0 >= 0 && ly0 + 2 < ty && lz0 >= 0 && lz0 + 2 < ty) {
-            const float *t0 = ftile + (lz0 * ty + ly0) * tx + lx0;
-#pragma unroll
-            for (int c = 0; c < 3; c++)
-#pragma unroll
-              for (int bq = 0; bq < 3; bq++)
-#pragma unroll
-                for (int a = 0; a < 3; a++) {
-                  const float w = (wx[a] * wy[bq]) * wz[c];
-                  const int o = (c * ty + bq) * tx + a;
-                  d0 += t0[o] * w;
-                  d1 += t0[tsz + o] * w;
-                  d2 += t0[2 * tsz + o] * w;
-                }
-          } else {  // outside the tile (not reached for exact mesh scales)
-            for (int c = 0; c < 3; c++)
-              for (int bq = 0; bq < 3; bq++)
-                for (int a = 0; a < 3; a++) {
-                  const float w = (wx[a] * wy[bq]) * wz[c];
-                  const int64_t X = p.wrap ? wrapi(ix + a - 1, n) : ix + a - 1;
-                  const int64_t Y = p.wrap ? wrapi(iy + bq - 1, n) : iy + bq - 1;
-                  const int64_t Z = p.wrap ? wrapi(iz + c - 1, n) : iz + c - 1;
-                  const int64_t m = (Z * n + Y) * n + X;
-                  d0 += F[m] * w;
-                  d1 += F[n3 + m] * w;
-                  d2 += F[2 * n3 + m] * w;
-                }
-          }
-          float *v = p.vp + 3 * ip;
-          const float v0 = v[0] + d0 * p.kick, v1 = v[1] + d1 * p.kick, v2 = v[2] + d2 * p.kick;
-          v[0] = v0;
-          v[1] = v1;
-          v[2] = v2;
-          vm0 = fmaxf(vm0, fabsf(v0));
-          vm1 = fmaxf(vm1, fabsf(v1));
-          vm2 = fmaxf(vm2, fabsf(v2));
-        }
-      }
-  if (p.want_vmax) {
-    vm0 = warp_max(vm0);
-    vm1 = warp_max(vm1);
-    vm2 = warp_max(vm2);
-    if ((threadIdx.x & 31) == 0) {
-      atomic_max_nonneg(&p.out[2], vm0);
-      atomic_max_nonneg(&p.out[3], vm1);
-      atomic_max_nonneg(&p.out[4], vm2);
-    }
-  }
-}
-
-// f2max with float4 loads along x (the physical region starts and ends on multiples of 4)
-__global__ void k_f2max_v4(PM3K p) {
-  float m = 0.f;
-  const int64_t g4 = p.fphys_n / 4;
-  const int64_t nph = g4 * p.fphys_n * p.fphys_n;
-  const int64_t total = nph * p.nslots;
-  const int64_t n = p.n;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int slot = (int)(e / nph);
-    const int64_t r = e - slot * nph;
-    const int64_t x = 4 * (r % g4) + p.fphys_lo, y = (r / g4) % p.fphys_n + p.fphys_lo,
-                  z = r / (g4 * p.fphys_n) + p.fphys_lo;
-    const int64_t q = (z * n + y) * n + x;
-    const float *F = p.force + (int64_t)slot * 3 * p.n3;
-    const float4 a = __ldg(reinterpret_cast<const float4 *>(F + q));
-    const float4 b = __ldg(reinterpret_cast<const float4 *>(F + p.n3 + q));
-    const float4 c = __ldg(reinterpret_cast<const float4 *>(F + 2 * p.n3 + q));
-    m = fmaxf(m, fmaxf(fmaxf(a.x * a.x + b.x * b.x + c.x * c.x, a.y * a.y + b.y * b.y + c.y * c.y),
-                       fmaxf(a.z * a.z + b.z * b.z + c.z * c.z, a.w * a.w + b.w * b.w + c.w * c.w)));
-  }
-  m = warp_max(m);
-  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&p.out[0], m);
-}
-
-// brick tiling applies when the mesh scale is an exact integer number of mesh
-// cells per coarse cell and the tile fits the shared-memory budget
-static bool tile_geom(const PM3Args &a, const int *rd, TileGeom &tg, size_t per_comp_limit) {
-  const double cmd = a.scale;
-  const int cm = (int)llrint(cmd);
-  if ((double)cm != cmd || a.n % 4) return false;
-  tg.cm = cm;
-  tg.bc = cm >= 16 ? 1 : 16 / cm;
-  tg.tx = tg.bc * cm + 8;
-  tg.ty = tg.bc * cm + 2;
-  if (sizeof(float) * (size_t)tg.tx * tg.ty * tg.ty > per_comp_limit) return false;
-  for (int d = 0; d < 3; d++) tg.nb[d] = (rd[d] + tg.bc - 1) / tg.bc;
-  return true;
 }
 
 static PM3K make_k(const PM3Args &a) {
@@ -464,7 +227,7 @@ static PM3K make_k(const PM3Args &a) {
   p.rho = a.rho;
   p.rhok = a.rhok;
   p.fk = a.fk;
-  p.force = a.force;
+  p.force = reinterpret_cast<const float4 *>(a.force);
   p.green = a.green;
   p.dtab = a.dtab;
   p.gscale = (float)((double)a.mass / ((double)a.n * a.n * a.n));
@@ -478,18 +241,8 @@ static PM3K make_k(const PM3Args &a) {
   return p;
 }
 
-constexpr size_t kTileBytes = 72 * 1024;  // per force component / deposit tile
-
 void launch_pm3_deposit(const PM3Args &a, cudaStream_t s) {
   PM3K p = make_k(a);
-  TileGeom tg;
-  if (tile_geom(a, a.rdep, tg, kTileBytes)) {
-    const size_t shm = sizeof(float) * (size_t)tg.tx * tg.ty * tg.ty;
-    cudaFuncSetAttribute(k_deposit_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-    const int64_t blocks = (int64_t)tg.nb[0] * tg.nb[1] * tg.nb[2] * a.njobs;
-    k_deposit_tile<<<(unsigned)blocks, 256, shm, s>>>(p, tg);
-    return;
-  }
   const int64_t warps = (int64_t)a.rdep[0] * a.rdep[1] * a.rdep[2] * a.njobs;
   k_deposit<<<(unsigned)((warps + kWarps - 1) / kWarps), kWarps * 32, 0, s>>>(p);
 }
@@ -501,22 +254,11 @@ void launch_pm3_kspace(const PM3Args &a, cudaStream_t s) {
 
 void launch_pm3_f2max(const PM3Args &a, cudaStream_t s) {
   PM3K p = make_k(a);
-  if (a.fphys_lo % 4 == 0 && a.fphys_n % 4 == 0 && a.n % 4 == 0)
-    k_f2max_v4<<<148 * 8, 256, 0, s>>>(p);
-  else
-    k_f2max<<<148 * 8, 256, 0, s>>>(p);
+  k_f2max<<<148 * 8, 256, 0, s>>>(p);
 }
 
 void launch_pm3_gather(const PM3Args &a, cudaStream_t s) {
   PM3K p = make_k(a);
-  TileGeom tg;
-  if (tile_geom(a, a.ract, tg, kTileBytes)) {
-    const size_t shm = 3 * sizeof(float) * (size_t)tg.tx * tg.ty * tg.ty;
-    cudaFuncSetAttribute(k_gather_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-    const int64_t blocks = (int64_t)tg.nb[0] * tg.nb[1] * tg.nb[2] * a.njobs;
-    k_gather_tile<<<(unsigned)blocks, 256, shm, s>>>(p, tg);
-    return;
-  }
   const int64_t warps = (int64_t)a.ract[0] * a.ract[1] * a.ract[2] * a.njobs;
   k_gather<<<(unsigned)((warps + kWarps - 1) / kWarps), kWarps * 32, 0, s>>>(p);
 }

@@ -30,10 +30,9 @@ namespace cube {
 
 constexpr int kPPThreads = 256;
 constexpr int kPPWarps = kPPThreads / 32;
-constexpr int kJTile = 64;    // staged candidates per warp
-constexpr int kQ = 16;        // accepted-pair queue entries per lane
+constexpr int kJTile = 128;  // staged candidates per warp
 constexpr int kBuckets = 32;
-constexpr size_t kPPSmem = sizeof(float4) * kPPWarps * (kJTile + kQ * 32);
+constexpr size_t kPPSmem = sizeof(float4) * kPPWarps * kJTile;
 
 // basic_functions.f08:95-109 / pp_force_kernel.c:45-74 in FP32, same operation order
 __device__ __forceinline__ float F_ra(float r, float apm) {
@@ -90,6 +89,11 @@ struct PairLaw {
     return fpp * invr;
   }
 };
+
+__device__ __forceinline__ float warp_min(float v) {
+  for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
 
 __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   float y = x - c;
@@ -231,11 +235,10 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
 // COUNT = false: forces and kick.  COUNT = true: only count the accepted ordered
 // pairs 0 < r^2 < rc^2 (the algorithmic work of the kick, for the roofline).
 template <bool COUNT>
-__global__ void __launch_bounds__(kPPThreads, 2) k_pp_force(PPK p) {
+__global__ void __launch_bounds__(kPPThreads, 3) k_pp_force(PPK p) {
   extern __shared__ float4 pp_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float4 *buf = pp_smem + warp * (kJTile + kQ * 32);
-  float4 *queue = buf + kJTile;  // queue[k * 32 + lane]: entry k of this lane
+  float4 *buf = pp_smem + warp * kJTile;
   int total = 0;
   {
     int v = lane < kBuckets ? p.bucket[lane] : 0;
@@ -271,52 +274,63 @@ __global__ void __launch_bounds__(kPPThreads, 2) k_pp_force(PPK p) {
     const bool has_i = grp < ngrp;  // the 32 mod ni leftover lanes idle
     const float4 pi = p.spos[i0 + il];
 
+    // bounding box of the item's particles: candidates farther than rc from it are dropped
+    // while staging, so the pair loop below only sees possibly-interacting candidates
+    const float blx = warp_min(pi.x), bhx = warp_max(pi.x), bly = warp_min(pi.y), bhy = warp_max(pi.y),
+                blz = warp_min(pi.z), bhz = warp_max(pi.z);
     float sx_ = 0.f, cx_ = 0.f, sy_ = 0.f, cy_ = 0.f, sz_ = 0.f, cz_ = 0.f;
-    int cnt = 0;  // entries in this lane's queue
-    auto drain = [&]() {
-      const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    int nbuf = 0;  // staged candidates (warp-uniform)
+    auto flush = [&]() {
+      __syncwarp();
       float px = 0.f, py = 0.f, pz = 0.f;
-      for (int r = 0; r < rounds; r++) {
-        const float4 e = queue[r * 32 + lane];
-        if (r < cnt) {
-          const float s = law.scale(e.w);
-          px = fmaf(s, e.x, px);
-          py = fmaf(s, e.y, py);
-          pz = fmaf(s, e.z, pz);
+#pragma unroll 4
+      for (int q = has_i ? grp : nbuf; q < nbuf; q += ngrp) {
+        const float4 pj = buf[q];
+        const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
+        const float r2 = dx * dx + dy_ * dy_ + dz_ * dz_;
+        const bool ok = (r2 > 0.0f) & (r2 < rc2);
+        if (COUNT) {
+          npairs += ok ? 1ull : 0ull;
+        } else {
+          // evaluated for every candidate and masked: a divergent accept branch would
+          // run on nearly every iteration of a 32-lane warp anyway
+          const float s = ok ? law.scale(r2) : 0.0f;
+          px = fmaf(s, dx, px);
+          py = fmaf(s, dy_, py);
+          pz = fmaf(s, dz_, pz);
         }
       }
-      kahan_add(sx_, cx_, px);
-      kahan_add(sy_, cy_, py);
-      kahan_add(sz_, cz_, pz);
-      cnt = 0;
+      if (!COUNT) {
+        kahan_add(sx_, cx_, px);
+        kahan_add(sy_, cy_, py);
+        kahan_add(sz_, cz_, pz);
+      }
+      nbuf = 0;
+      __syncwarp();
     };
     for (int dz = -R; dz <= R; dz++)
       for (int dy = -R; dy <= R; dy++) {
         if (!row_needed(dy, dz, h, rc2)) continue;
         const int64_t b = g + ((int64_t)dz * S + dy) * S;
         const int js = p.cs[b - R], je = p.cs[b + R + 1];
-        for (int jb = js; jb < je; jb += kJTile) {
-          const int nb = min(kJTile, je - jb);
-          __syncwarp();
-          for (int q = lane; q < nb; q += 32) buf[q] = p.spos[jb + q];
-          __syncwarp();
-          const int nsteps = (nb + ngrp - 1) / ngrp;
-          for (int k = 0; k < nsteps; k++) {
-            const int q = grp + k * ngrp;
-            const float4 pj = buf[q < nb ? q : nb - 1];
-            const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
-            const float r2 = dx * dx + dy_ * dy_ + dz_ * dz_;
-            const bool ok = has_i && (q < nb) && (r2 > 0.0f) && (r2 < rc2);
-            if (COUNT) {
-              npairs += ok ? 1ull : 0ull;
-            } else {
-              if (ok) queue[cnt++ * 32 + lane] = make_float4(dx, dy_, dz_, r2);
-              if (__any_sync(0xffffffffu, cnt == kQ)) drain();
-            }
+        for (int jb = js; jb < je; jb += 32) {
+          const int q = jb + lane;
+          bool keep = q < je;
+          float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (keep) {
+            pj = p.spos[q];
+            const float ex = fmaxf(fmaxf(blx - pj.x, pj.x - bhx), 0.f);
+            const float ey = fmaxf(fmaxf(bly - pj.y, pj.y - bhy), 0.f);
+            const float ez = fmaxf(fmaxf(blz - pj.z, pj.z - bhz), 0.f);
+            keep = ex * ex + ey * ey + ez * ez < rc2;
           }
+          const unsigned m = __ballot_sync(0xffffffffu, keep);
+          if (keep) buf[nbuf + __popc(m & ((1u << lane) - 1u))] = pj;
+          nbuf += __popc(m);
+          if (nbuf > kJTile - 32) flush();
         }
       }
-    if (!COUNT) drain();
+    if (nbuf) flush();
     // merge the lane groups of each i-particle (tree over groups, stride s*ni lanes);
     // Kahan c is the negated low part
     float hx = sx_, lx = -cx_, hy = sy_, ly = -cy_, hz = sz_, lz = -cz_;

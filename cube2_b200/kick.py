@@ -183,8 +183,10 @@ class FineKick:
         del keep
 
     # -- inspection ------------------------------------------------------------------------------
-    def pp_bin_tile(self, img: Image, tile: int, ires, ixyz3, ratio_sf):
-        """Binning of one parent tile: dict(keys, ip, cell_start, xf[3][N])."""
+    def pp_bin_tile(self, img: Image, tile: int, ires, ixyz3, ratio_sf, spatial: bool = False):
+        """Binning of one parent tile: dict(keys, ip, cell_start, xf[3][N]).
+
+        spatial=False: the reference's order inside each PP cell; True: the kick's order."""
         L = self.layout
         rcp = int(max(np.asarray(ratio_sf)[np.asarray(ires) - 1]))
         S = rcp * (L.nt + 2)
@@ -198,7 +200,8 @@ class FineKick:
         g_out = np.zeros(1, np.int64)
         ires, ixyz3, ratio_sf = _c32(ires), _c32(ixyz3), _c32(ratio_sf)
         st = lib().cube_pp_bin_tile(_p(ires), _p(ixyz3), _p(ratio_sf), _p(img.rhoc), _p(img.idx_b_r), _p(img.xp),
-                                    ctypes.c_int32(tile), _p(keys), _p(ip), _p(cs), _p(xf),
+                                    ctypes.c_int32(tile), ctypes.c_int32(1 if spatial else 0), _p(keys), _p(ip),
+                                    _p(cs), _p(xf),
                                     ctypes.c_int64(max(cap, 1)), ctypes.c_int64(grid + 1), _p(n_out), _p(g_out))
         _check(st, "cube_pp_bin_tile")
         N = int(n_out[0])

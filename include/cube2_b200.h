@@ -134,10 +134,12 @@ int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32
  * storage index ip (ip_local[values[]]) of every sorted particle, cell_start
  * (grid_num + 1 entries, tile-local), sorted positions xf [3][N].  Capacities
  * in elements; *n_out = N, *grid_out = grid_num.  Runs the binning on the
- * given host inputs. */
+ * given host inputs.  spatial = 0 gives the reference's order inside each PP
+ * cell (stable by storage slot); spatial = 1 gives the order the kick uses
+ * (Morton sub-cell, then storage slot), with the same keys and cell_start. */
 int cube_pp_bin_tile(const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf, const int32_t *rhoc,
-                     const int64_t *idx_b_r, const int16_t *xp, int32_t tile, uint32_t *keys, int64_t *ip,
-                     int32_t *cell_start, float *xf, int64_t cap_n, int64_t cap_grid, int64_t *n_out,
+                     const int64_t *idx_b_r, const int16_t *xp, int32_t tile, int32_t spatial, uint32_t *keys,
+                     int64_t *ip, int32_t *cell_start, float *xf, int64_t cap_n, int64_t cap_grid, int64_t *n_out,
                      int64_t *grid_out);
 
 /* Number of ordered PP pairs (i interior, 0 < r^2 < range^2) the kick evaluates

@@ -31,6 +31,32 @@ def test_binning_matches_reference_golden(gpu, case):
                       z[f"t{t}_ip_local"])
 
 
+@pytest.mark.parametrize("case", CASES)
+def test_kick_order_is_a_within_cell_permutation(gpu, case):
+    """The kick's spatial order keeps the reference keys and cell_start bit for bit and only
+    permutes particles inside each PP cell (Morton sub-cell, then storage slot)."""
+    from cube2_b200.kick import FineKick
+    from cube2_b200.layout import RATIO_SF, ixyz3_table
+    img, z = load_golden(case)
+    L = img.layout
+    fk = FineKick(L)
+    ires = np.full(L.ns3, 2, np.int32)
+    ix = ixyz3_table(L)
+    for t in range(L.nnt ** 3):
+        ref = fk.pp_bin_tile(img, t, ires, ix, RATIO_SF, spatial=False)
+        sp = fk.pp_bin_tile(img, t, ires, ix, RATIO_SF, spatial=True)
+        np.testing.assert_array_equal(sp["keys"], z[f"t{t}_keys"])
+        np.testing.assert_array_equal(sp["cell_start"], z[f"t{t}_cell_start"])
+        cs = sp["cell_start"]
+        for c in np.nonzero(np.diff(cs))[0]:
+            a, b = cs[c], cs[c + 1]
+            assert sorted(sp["ip"][a:b]) == sorted(ref["ip"][a:b])
+            # positions travel with their particles
+            order_s = np.argsort(sp["ip"][a:b])
+            order_r = np.argsort(ref["ip"][a:b])
+            np.testing.assert_array_equal(sp["xf"][:, a:b][:, order_s], ref["xf"][:, a:b][:, order_r])
+
+
 def test_binning_zeldovich_box_matches_reference(gpu):
     """64^3 Zel'dovich lattice (one periodic tile) against the compiled reference, live."""
     from cube2_b200 import ic
