@@ -217,13 +217,7 @@ static int get_plan(int n, int batch, cufftType type, cufftHandle *out) {
     }
   Plan p{n, batch, type, 0};
   int dims[3] = {n, n, n};
-  if (type == CUFFT_C2R) {
-    // the three force components of one mesh, written interleaved: out[4*point + component]
-    int iemb[3] = {n, n, n / 2 + 1}, oemb[3] = {n, n, n};
-    CF(cufftPlanMany(&p.h, 3, dims, iemb, 1, n * n * (n / 2 + 1), oemb, 4, 1, type, batch));
-  } else {
-    CF(cufftPlanMany(&p.h, 3, dims, nullptr, 1, 0, nullptr, 1, 0, type, batch));
-  }
+  CF(cufftPlanMany(&p.h, 3, dims, nullptr, 1, 0, nullptr, 1, 0, type, batch));
   CF(cufftSetStream(p.h, g.stream));
   g.plans.push_back(p);
   *out = p.h;
@@ -387,7 +381,7 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     CK(grow(g.rho, sizeof(float) * n3));
     CK(grow(g.rhok, sizeof(cufftComplex) * nk));
     CK(grow(g.fk, sizeof(cufftComplex) * nk * 3));
-    CK(grow(g.force, sizeof(float) * n3 * 4));  // interleaved (Fx, Fy, Fz, -)
+    CK(grow(g.force, sizeof(float) * n3 * 3));
     const double scale = (double)L.rcs / (double)(1.0f / (float)rsf);
     std::vector<MeshJob> jobs(L.ntile);
     for (int t = 0; t < L.ntile; t++) {
@@ -474,7 +468,7 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       CK(grow(g.rho, sizeof(float) * n3 * nb));
       CK(grow(g.rhok, sizeof(cufftComplex) * nk * nb));
       CK(grow(g.fk, sizeof(cufftComplex) * nk * 3 * nb));
-      CK(grow(g.force, sizeof(float) * n3 * 4 * nb));
+      CK(grow(g.force, sizeof(float) * n3 * 3 * nb));
       std::vector<MeshJob> jobs(nj);
       for (int j = 0; j < nj; j++) {
         const int loc = locs[j0 + j];
@@ -524,13 +518,12 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       a.want_vmax = want_vmax;
       cufftHandle fw, bw;
       CK(get_plan(n, nb, CUFFT_R2C, &fw));
-      CK(get_plan(n, 3, CUFFT_C2R, &bw));
+      CK(get_plan(n, 3 * nb, CUFFT_C2R, &bw));
       CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3 * nb, g.stream));
       launch_pm3_deposit(a, g.stream);
       CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
       launch_pm3_kspace(a, g.stream);
-      for (int sl = 0; sl < nj; sl++)  // interleaved output: one 3-component transform per mesh
-        CF(cufftExecC2R(bw, (cufftComplex *)g.fk.p + (size_t)sl * 3 * nk, (cufftReal *)g.force.p + (size_t)sl * 4 * n3));
+      CF(cufftExecC2R(bw, (cufftComplex *)g.fk.p, (cufftReal *)g.force.p));
       a.nslots = nj;  // f2max over the real jobs only
       launch_pm3_f2max(a, g.stream);
       launch_pm3_gather(a, g.stream);

@@ -11,12 +11,13 @@
 //            D = a sin k + (1-a) sin 2k / 2, a = 4/3 -- the exact Fourier image
 //            of potential_to_force (kick.f90:545-568) on the FFT mesh -- and
 //            writes the three force spectra;
-//   C2R      cuFFT, batched over the 3 components and written interleaved
-//            (output stride 4): force[point] = (Fx, Fy, Fz, unused);
-//   f2max    max |F|^2 over the physical mesh points (kick.f90:494), one
-//            16-byte load per point;
-//   gather   TSC gather of the force at each active particle (27 16-byte loads)
-//            and the kick vp += dv * a_mid*dt/(6 pi) (kick.f90:497-540).
+//   C2R      cuFFT, batched over the 3 components (three separate arrays: a
+//            stride-4 interleaved output measured slower for both cuFFT and
+//            the gather);
+//   f2max    max |F|^2 over the physical mesh points (kick.f90:494), float4
+//            loads along x;
+//   gather   TSC gather of the force at each active particle and the kick
+//            vp += dv * a_mid*dt/(6 pi) (kick.f90:497-540).
 #include <cmath>
 
 #include "common.cuh"
@@ -37,7 +38,7 @@ struct PM3K {
   float *rho;
   const cufftComplex *rhok;
   cufftComplex *fk;
-  const float4 *force;  // [slot][n^3] interleaved (Fx, Fy, Fz, -)
+  const float *force;  // [slot][3][n^3]
   const float *green;
   const float *dtab;
   float gscale;  // mass / n^3
@@ -132,8 +133,35 @@ __global__ void k_f2max(PM3K p) {
     const int64_t r = e - slot * nph;
     const int64_t x = r % p.fphys_n + p.fphys_lo, y = (r / p.fphys_n) % p.fphys_n + p.fphys_lo,
                   z = r / ((int64_t)p.fphys_n * p.fphys_n) + p.fphys_lo;
-    const float4 f = __ldg(p.force + (int64_t)slot * p.n3 + (z * n + y) * n + x);
-    m = fmaxf(m, f.x * f.x + f.y * f.y + f.z * f.z);
+    const int64_t q = (z * n + y) * n + x;
+    const float *F = p.force + (int64_t)slot * 3 * p.n3;
+    const float a = F[q], b = F[p.n3 + q], c = F[2 * p.n3 + q];
+    m = fmaxf(m, a * a + b * b + c * c);
+  }
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&p.out[0], m);
+}
+
+// f2max with float4 loads along x (the physical region starts and ends on multiples of 4)
+__global__ void k_f2max_v4(PM3K p) {
+  float m = 0.f;
+  const int64_t g4 = p.fphys_n / 4;
+  const int64_t nph = g4 * p.fphys_n * p.fphys_n;
+  const int64_t total = nph * p.nslots;
+  const int64_t n = p.n;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int slot = (int)(e / nph);
+    const int64_t r = e - slot * nph;
+    const int64_t x = 4 * (r % g4) + p.fphys_lo, y = (r / g4) % p.fphys_n + p.fphys_lo,
+                  z = r / (g4 * p.fphys_n) + p.fphys_lo;
+    const int64_t q = (z * n + y) * n + x;
+    const float *F = p.force + (int64_t)slot * 3 * p.n3;
+    const float4 a = __ldg(reinterpret_cast<const float4 *>(F + q));
+    const float4 b = __ldg(reinterpret_cast<const float4 *>(F + p.n3 + q));
+    const float4 c = __ldg(reinterpret_cast<const float4 *>(F + 2 * p.n3 + q));
+    m = fmaxf(m, fmaxf(fmaxf(a.x * a.x + b.x * b.x + c.x * c.x, a.y * a.y + b.y * b.y + c.y * c.y),
+                       fmaxf(a.z * a.z + b.z * b.z + c.z * c.z, a.w * a.w + b.w * b.w + c.w * c.w)));
   }
   m = warp_max(m);
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&p.out[0], m);
@@ -154,8 +182,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_gather(PM3K p) {
     const int64_t cidx = (((int64_t)J.t * p.nte + ck) * p.nte + cj) * p.nte + ci;
     const int np = p.rhoc[cidx];
     const int64_t base = p.cell_base[cidx];
-    const float4 *F = p.force + (int64_t)J.slot * p.n3;
-    const int64_t n = p.n;
+    const float *F = p.force + (int64_t)J.slot * 3 * p.n3;
+    const int64_t n = p.n, n3 = p.n3;
     for (int l = lane; l < np; l += 32) {
       const int64_t ip = base + l;
       const int16_t *q = p.xp + 3 * ip;
@@ -173,11 +201,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_gather(PM3K p) {
 #pragma unroll
           for (int a = 0; a < 3; a++) {
             const int64_t X = p.wrap ? wrapi(ix + a - 1, n) : ix + a - 1;
-            const float4 f = __ldg(F + (Z * n + Y) * n + X);
+            const int64_t m = (Z * n + Y) * n + X;
             const float w = (wx[a] * wy[b]) * wz[c];
-            d0 += f.x * w;
-            d1 += f.y * w;
-            d2 += f.z * w;
+            d0 += F[m] * w;
+            d1 += F[n3 + m] * w;
+            d2 += F[2 * n3 + m] * w;
           }
         }
       }
@@ -227,7 +255,7 @@ static PM3K make_k(const PM3Args &a) {
   p.rho = a.rho;
   p.rhok = a.rhok;
   p.fk = a.fk;
-  p.force = reinterpret_cast<const float4 *>(a.force);
+  p.force = a.force;
   p.green = a.green;
   p.dtab = a.dtab;
   p.gscale = (float)((double)a.mass / ((double)a.n * a.n * a.n));
@@ -254,7 +282,10 @@ void launch_pm3_kspace(const PM3Args &a, cudaStream_t s) {
 
 void launch_pm3_f2max(const PM3Args &a, cudaStream_t s) {
   PM3K p = make_k(a);
-  k_f2max<<<148 * 8, 256, 0, s>>>(p);
+  if (a.fphys_lo % 4 == 0 && a.fphys_n % 4 == 0 && a.n % 4 == 0)
+    k_f2max_v4<<<148 * 8, 256, 0, s>>>(p);
+  else
+    k_f2max<<<148 * 8, 256, 0, s>>>(p);
 }
 
 void launch_pm3_gather(const PM3Args &a, cudaStream_t s) {
