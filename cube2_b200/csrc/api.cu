@@ -1023,6 +1023,21 @@ int cube_pp_bin_tile(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   return CUBE_OK;
 }
 
+int cube_pp_force_noalloc(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                          const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r,
+                          const int16_t *d_xp, int64_t n_used, float *d_vp, float mass, float a_mid, float dt,
+                          float *d_out, void *stream) {
+  (void)isort;
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  // no context set-up here: the current device and the caller's stream are used as they are
+  const int s = pp_force_noalloc(g.L, ires, ixyz3, apm3, ratio_sf, d_rhoc, d_idx_b_r, d_xp, n_used, d_vp, mass,
+                                 a_mid, dt, d_out, (cudaStream_t)stream);
+  if (s != CUBE_OK) return fail(s);
+  return CUBE_OK;
+}
+
 int cube_pp_pair_count(const int32_t *ires, const int32_t *ixyz3, const float *apm3, const int32_t *ratio_sf,
                        const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp, int64_t *pairs) {
   std::lock_guard<std::mutex> lk(g_mu);

@@ -160,6 +160,12 @@ void launch_pm3_gather(const PM3Args &a, cudaStream_t s);
 void launch_green_fp64(int n, double apm_soft, double apm_range, double gridsize, int p_order, float *G,
                        cudaStream_t s);
 
+// PP kick with all scratch in a static device array (noalloc.cu)
+int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                     const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp,
+                     int64_t n_used, float *d_vp, float mass, float a_mid, float dt, float *d_out, cudaStream_t s);
+size_t noalloc_scratch_bytes();
+
 // FP32 FMA throughput probe (5 launches); returns the time and the FLOPs executed
 cudaError_t fma_probe(cudaStream_t s, int num_sms, float *ms, double *flops);
 

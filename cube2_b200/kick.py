@@ -52,7 +52,7 @@ EXPORTS = ("cube_set_layout", "cube_get_layout", "cube_last_error", "cube_error_
            "c_pp_force_kernel", "c_pm3_fft_finalize", "c_gpu_velocity_finalize", "cube_pm3_force", "cube_pp_force",
            "cube_kick_fine", "cube_kick_fine_device", "cube_pp_bin_tile", "cube_pp_pair_count", "cube_green_table",
            "cube_force_truth_fp64", "cube_stage_times", "cube_enable_timing", "cube_timing_read",
-           "cube_launch_count", "cube_fp32_peak_probe")
+           "cube_launch_count", "cube_fp32_peak_probe", "cube_pp_force_noalloc")
 
 
 def lib() -> ctypes.CDLL:

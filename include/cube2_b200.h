@@ -127,6 +127,35 @@ int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32
                           const int16_t *d_xp, int64_t n_used, const float *const gk[5], float *d_vp, float mass,
                           float a_mid, float dt, float *d_out, void *stream);
 
+/* ---- allocation-free PP kick ---- */
+
+/* Largest input cube_pp_force_noalloc accepts: stored particles (n_used) and
+ * PP cells over all tiles (also the bound on coarse cells over all extended
+ * tiles).  The scratch for this size is one static device array of about
+ * 17 MB that every GPU loading the library holds until the process exits. */
+#define CUBE_NOALLOC_MAX_PARTICLES 524288
+#define CUBE_NOALLOC_MAX_CELLS 262144
+
+/* The PP kick of cube_pp_force on device-resident arrays, for callers that
+ * cannot let a library allocate device memory (their allocator owns every
+ * byte, or an allocation-free execution policy is in force).  It calls no
+ * cudaMalloc, cudaFree or other allocating routine: the caller passes the
+ * inputs (d_rhoc, d_idx_b_r, d_xp) and outputs (d_vp is kicked in place;
+ * d_out, 6 words of device memory, receives PP f2max in word 1, vmax in words
+ * 2..4 and a device failure mask in word 5), and all scratch lives in a
+ * file-scope device array.  Enqueued on `stream` (NULL = the default stream)
+ * on the current device, without host synchronisation.
+ * The first call on each device looks up the array's device address, so make
+ * that first call before any stream capture.  Every call shares the array and
+ * it keeps the previous call's contents (counters are reset by each call):
+ * calls that overlap on the GPU race on it.  Returns CUBE_ERR_CAPACITY beyond
+ * CUBE_NOALLOC_MAX_PARTICLES / CUBE_NOALLOC_MAX_CELLS, 64 tiles or 4096
+ * subtiles.  This entry point has no counterpart in the reference. */
+int cube_pp_force_noalloc(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                          const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r,
+                          const int16_t *d_xp, int64_t n_used, float *d_vp, float mass, float a_mid, float dt,
+                          float *d_out, void *stream);
+
 /* ---- inspection (parity checks) ---- */
 
 /* Binning of one parent tile as the PP pass builds it, in the reference's
