@@ -553,7 +553,7 @@ static int run_pp(const Meta &m, const Dev &d, float mass, float kick, size_t &s
   CK(grow(g.spill_rank, sizeof(int32_t) * spill_cap));
   int64_t interior = 0;
   for (auto &t : m.tiles) interior += (int64_t)L.nt * t.rcp * L.nt * t.rcp * L.nt * t.rcp;
-  const int64_t item_cap = interior + d.n_used / 32 + 16;
+  const int64_t item_cap = interior + d.n_used / kPPChunk + 16;
   CK(grow(g.items, sizeof(int4) * (size_t)item_cap));
   int32_t *ctr = (int32_t *)g.counters.p;  // [0] spill_n [1] head [2] err [64..128) buckets
   BinArgs b{};

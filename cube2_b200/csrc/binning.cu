@@ -20,9 +20,9 @@
 // Spatial order (used by the kick, not by the parity view): with rcp dividing
 // 8, pass 2 can instead order the particles inside each PP cell by the Morton
 // index of their 1/8-coarse-cell sub-cell (then storage order).  Keys and
-// cell_start are unchanged; 32-particle chunks of a crowded cell then occupy
-// a compact sub-volume, which lets the PP kernel prune candidates against the
-// chunk's bounding box.
+// cell_start are unchanged; the PP work items (chunks of a crowded cell) then
+// occupy a compact sub-volume, which lets the PP kernel prune candidates
+// against the chunk's bounding box.
 #include <cstdio>
 
 #include "common.cuh"

@@ -45,6 +45,7 @@ struct MeshJob {
 };
 
 constexpr int kWarps = 8;  // warps per block in warp-per-cell kernels
+constexpr int kPPChunk = 8;  // i-particles per PP work item (a crowded PP cell is split into chunks)
 
 // ---------------------------------------------------------------------------------------------
 // device helpers

@@ -38,7 +38,7 @@ constexpr size_t kOffStart = kOffCount + na_align(sizeof(int32_t) * kNaCells);  
 constexpr size_t kOffScan = kOffStart + na_align(sizeof(int32_t) * (kNaCells + 1));    // int32 scan scratch
 constexpr size_t kOffSpos = kOffScan + na_align(sizeof(int32_t) * (kNaCells / 4096 + 2));
 constexpr size_t kOffItems = kOffSpos + na_align(sizeof(float4) * kNaParticles);       // int4 work list
-constexpr size_t kItemCap = kNaCells + kNaParticles / 32 + 16;
+constexpr size_t kItemCap = kNaCells + kNaParticles / kPPChunk + 16;
 constexpr size_t kOffSpill = kOffItems + na_align(sizeof(int4) * kItemCap);
 constexpr size_t kOffSpillRank = kOffSpill + na_align(sizeof(Spill) * kNaSpill);
 constexpr size_t kOffTiles = kOffSpillRank + na_align(sizeof(int32_t) * kNaSpill);
@@ -98,7 +98,7 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
     max_rcp = rcp > max_rcp ? rcp : max_rcp;
   }
   if (ncells > kNaCells) return CUBE_ERR_CAPACITY;
-  if (interior + n_used / 32 + 16 > (int64_t)kItemCap) return CUBE_ERR_CAPACITY;
+  if (interior + n_used / kPPChunk + 16 > (int64_t)kItemCap) return CUBE_ERR_CAPACITY;
   if (bin_smem_bytes(max_rcp) > 200 * 1024) return CUBE_ERR_INVALID;
 
   // device address of the scratch on the current device (once per device)

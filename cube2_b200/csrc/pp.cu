@@ -2,37 +2,46 @@
 // (pp_force_kernel.c:282-325, pp_force_kernel.cu:192-250) and the kick of the
 // interior particles (pp_force_kernel.c:339-364).
 //
-// Work decomposition.  An item is one interior PP cell, or a 32-particle chunk
-// of a crowded one.  A particle of range rc needs the cells within
-// R = ceil(rc * rcp / ratio_cs) of its own (pp_force_kernel.cu:205); the rows
-// (dy, dz) of that stencil whose nearest point is farther than rc are skipped,
-// and the cells of a row are one contiguous range of the cell-sorted array.
-// Items are bucketed by cost (log2 of candidates per lane group) and a
-// persistent kernel hands them out heaviest first through an atomic queue
-// head, so the lognormal occupancy of clustered boxes does not leave a tail.
+// Work decomposition.  An item is one interior PP cell, or a kPPChunk-particle
+// chunk of a crowded one (the kick's binning orders a cell's particles by
+// Morton sub-cell, so a chunk occupies a compact sub-volume).  A particle of
+// range rc needs the cells within R = ceil(rc * rcp / ratio_cs) of its own
+// (pp_force_kernel.cu:205); the rows (dy, dz) of that stencil whose nearest
+// point is farther than rc are skipped, and the cells of a row are one
+// contiguous range of the cell-sorted array.  Items are bucketed by cost
+// (log2 of candidates per lane group) and a persistent kernel hands them out
+// heaviest first through an atomic queue head, so the lognormal occupancy of
+// clustered boxes does not leave a tail.
 //
 // Inside an item one warp splits its 32 lanes into floor(32/ni) groups of ni
-// lanes; lane (group g, particle i) walks every ngrp-th candidate.  Candidates
-// are staged per warp in shared memory (coalesced float4 loads, broadcast
-// reads).  Only about 15% of the stencil candidates lie inside the cutoff, so
-// evaluating the pair law for every candidate would spend most issue slots on
-// rejected pairs: instead each lane pushes its accepted (dx, dy, dz, r^2)
-// into its own shared-memory queue, and when any lane's queue is full the
-// warp drains all queues in lock-step rounds.  The pair law is evaluated
-// without divisions or branches (one rsqrt and a degree-6 Horner polynomial
-// with per-lane coefficient selection).  Each lane keeps Kahan-compensated
-// sums updated once per drain; the groups of a particle are merged with warp
-// shuffles (TwoSum), and the owning lane applies af*mass^2, the kick, f2max
-// and vmax.
+// lanes; lane (group g, particle i) walks every ngrp-th staged candidate.  The
+// needed rows are laid end to end in a per-warp row table, so every staging
+// step loads 32 candidates (prefetched one step ahead) however short the rows
+// are.  A candidate is staged in shared memory only if it lies within rc of
+// the bounding box of the item's particles, which removes most of the stencil
+// volume before the pair law runs.  The pair law is evaluated without
+// divisions or selects: the inner piece of the S2 law differs from the outer
+// one by (1 - ep)^6 (12 + 72 ep + 28 ep^2) / ep^2, so one Horner polynomial in
+// r plus max(1 - ep, 0)^6 times a quadratic covers both.  Each lane keeps
+// Kahan-compensated sums updated once per flush of the staging buffer; the
+// groups of a particle are merged with warp shuffles (TwoSum), and the owning
+// lane applies af*mass^2, the kick, f2max and vmax.
 #include "common.cuh"
 
 namespace cube {
 
 constexpr int kPPThreads = 256;
 constexpr int kPPWarps = kPPThreads / 32;
-constexpr int kJTile = 128;  // staged candidates per warp
+constexpr int kJTile = 128;   // staged candidates per warp (+32 sentinel slots)
+constexpr int kMaxRows = 96;  // stencil rows per row table (a multiple of 32)
 constexpr int kBuckets = 32;
-constexpr size_t kPPSmem = sizeof(float4) * kPPWarps * kJTile;
+#ifndef PP_UNROLL
+#define PP_UNROLL 2  // unroll factor of the pair-evaluation loop
+#endif
+constexpr int kPairUnroll = PP_UNROLL;
+static_assert(kJTile / (32 / kPPChunk) <= 32, "a flush has at most 32 rounds (one bit each)");
+constexpr size_t kPPSmemWarp = sizeof(float4) * (kJTile + 32) + sizeof(int2) * kMaxRows;
+constexpr size_t kPPSmem = kPPSmemWarp * kPPWarps;
 
 // basic_functions.f08:95-109 / pp_force_kernel.c:45-74 in FP32, same operation order
 __device__ __forceinline__ float F_ra(float r, float apm) {
@@ -51,49 +60,73 @@ __device__ __forceinline__ float F_ra(float r, float apm) {
   return 0.0f;
 }
 
-// F_ra(r,app) - F_ra(r,rc) for 0 < r < rc, as a function of r^2, with per-cell constants and
-// no division: for r > app it equals A/r^2 - sum_k c_k ep^k with ep = 2r/rc, where
-//   outer (ep > 1): A = 32/35 (the 12/ep^2 term folded in), c = [-224,896,-840,224,70,-48,7]/(35 rc^2)
-//   inner:          A = 1,                                  c = [0,224,0,-224,70,48,-21]/(35 rc^2)
-// Returns the scale s such that the pair force is s * (dx, dy, dz).
+// s(r^2) = (F_ra(r,app) - F_ra(r,rc)) / r for 0 <= r < rc, so that the pair force is s * (dx, dy, dz).
+// With ep = 2r/rc and k = 1/(35 rc^2), for r > app:
+//   outer (ep > 1): 1/r^2 - F_ra(r,rc) = (32/35)/r^2 - k P(ep),  P = -224 + 896ep - 840ep^2 + 224ep^3
+//                                                                     + 70ep^4 - 48ep^5 + 7ep^6
+//   inner (ep <= 1): the outer form plus k (1-ep)^6 (12 + 72ep + 28ep^2) / ep^2
+//                    = (1/r^2) (1-ep)^6 (3/35 + 18/35 ep + 7/35 ep^2)
+// (expanding the product gives back the inner polynomial 224ep - 224ep^3 + 70ep^4 + 48ep^5 - 21ep^6).
+// The polynomial coefficients are literals (instruction immediates), so a law costs two registers
+// per item (2/rc and 1/(35 rc^2)).  Inside the softening length (rare, soft()) the reference's own
+// expression is evaluated.
 struct PairLaw {
-  float cep, app2, app, rc;
-  float o0, o1, o2, o3, o4, o5, o6, n1, n3, n4, n5, n6;
+  float cep, k35, app2, app, rc;
   __device__ __forceinline__ void init(float rc_, float app_) {
     rc = rc_;
     app = app_;
-    const float k35 = 1.0f / (35.0f * rc_ * rc_);
-    cep = 2.0f / rc_;
     app2 = app_ * app_;
-    o0 = -224.f * k35, o1 = 896.f * k35, o2 = -840.f * k35, o3 = 224.f * k35, o4 = 70.f * k35, o5 = -48.f * k35,
-    o6 = 7.f * k35;
-    n1 = 224.f * k35, n3 = -224.f * k35, n4 = 70.f * k35, n5 = 48.f * k35, n6 = -21.f * k35;
+    k35 = 1.0f / (35.0f * rc_ * rc_);
+    cep = 2.0f / rc_;
   }
   __device__ __forceinline__ float scale(float r2) const {
     const float invr = rsqrtf(r2);
     const float ir2 = invr * invr;
     const float ep = r2 * invr * cep;
-    const bool outer = ep > 1.0f;
-    float q = outer ? o6 : n6;
-    q = fmaf(q, ep, outer ? o5 : n5);
-    q = fmaf(q, ep, outer ? o4 : n4);
-    q = fmaf(q, ep, outer ? o3 : n3);
-    q = fmaf(q, ep, outer ? o2 : 0.0f);
-    q = fmaf(q, ep, outer ? o1 : n1);
-    q = fmaf(q, ep, outer ? o0 : 0.0f);
-    float fpp = fmaf(outer ? (32.0f / 35.0f) : 1.0f, ir2, -q);
-    if (r2 <= app2) {  // inside the softening length: the exact S2 law (rare)
-      const float r = r2 * invr;
-      fpp = F_ra(r, app) - F_ra(r, rc);
-    }
-    return fpp * invr;
+    float q = fmaf(7.0f, ep, -48.0f);
+    q = fmaf(q, ep, 70.0f);
+    q = fmaf(q, ep, 224.0f);
+    q = fmaf(q, ep, -840.0f);
+    q = fmaf(q, ep, 896.0f);
+    q = fmaf(q, ep, -224.0f);
+    const float u = fmaxf(1.0f - ep, 0.0f);
+    const float u2 = u * u;
+    const float u6 = u2 * u2 * u2;
+    const float w = fmaf(fmaf(7.0f / 35.0f, ep, 18.0f / 35.0f), ep, 3.0f / 35.0f);
+    const float br = fmaf(u6, w, 32.0f / 35.0f);
+    return fmaf(br, ir2, -q * k35) * invr;
+  }
+  // 0 < r <= app: the reference's expression
+  __device__ __forceinline__ float soft(float r2) const {
+    const float invr = rsqrtf(r2);
+    const float r = r2 * invr;
+    return (F_ra(r, app) - F_ra(r, rc)) * invr;
   }
 };
 
-__device__ __forceinline__ float warp_min(float v) {
-  for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
+// order-preserving map between floats and ints, for the integer warp reductions (redux.sync)
+__device__ __forceinline__ int float_key(float f) {
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
 }
+__device__ __forceinline__ float key_float(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff); }
+__device__ __forceinline__ float warp_min_redux(float v) {
+  return key_float(__reduce_min_sync(0xffffffffu, float_key(v)));
+}
+__device__ __forceinline__ float warp_max_redux(float v) {
+  return key_float(__reduce_max_sync(0xffffffffu, float_key(v)));
+}
+
+// n / d for 0 <= n < 2^11 and 1 <= d <= 64 by a multiply with ceil(2^20 / d): the error
+// n * (ceil(2^20/d) - 2^20/d) / 2^20 < 2^-9 stays below the 1/d gap to the next integer
+struct DivTable {
+  int m[65];
+  constexpr DivTable() : m() {
+    for (int d = 1; d <= 64; d++) m[d] = ((1 << 20) + d - 1) / d;
+  }
+};
+__constant__ DivTable c_div = DivTable();
+__device__ __forceinline__ int div_small(int n, int d) { return (n * c_div.m[d]) >> 20; }
 
 __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   float y = x - c;
@@ -117,7 +150,7 @@ struct PPK {
   const int32_t *cs;
   const float4 *spos;
   const float *range_loc;
-  int4 *items;
+  int4 *items;      // (global cell, chunk, tile, PP range bits)
   int32_t *bucket;  // [0,32) counts, [32,64) cursors
   int32_t *head;
   int64_t item_cap;
@@ -155,7 +188,10 @@ __device__ __forceinline__ int cost_bucket(int ni, int64_t nj) {
   return b > kBuckets - 1 ? kBuckets - 1 : b;
 }
 
-// Enumerate interior PP cells; pass 0 counts items per bucket, pass 1 emits them.
+// Enumerate the chunks of the interior PP cells; pass 0 counts items per bucket,
+// pass 1 writes them, heaviest bucket first.  A cell's full chunks share one
+// bucket and its remainder chunk has another, so a thread reserves its slots
+// with at most two shared-memory atomics.
 template <int PASS>
 __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
   __shared__ int sc[kBuckets], sbase[kBuckets], soff[kBuckets];
@@ -173,45 +209,34 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
   const int rcp = tp.rcp, S = tp.S, npg = p.nt * rcp;
   const int64_t ncell = (int64_t)npg * npg * npg;
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int nchunks = 0, ni = 0;
-  int64_t nj = 0, g = 0;
+  int nfull = 0, bfull = 0, brem = -1, rcbits = 0;
+  int64_t g = 0;
   if (c < ncell) {
     const int x = (int)(c % npg) + rcp, y = (int)((c / npg) % npg) + rcp, z = (int)(c / ((int64_t)npg * npg)) + rcp;
     g = tp.cell0 + ((int64_t)z * S + y) * S + x;
-    ni = p.cs[g + 1] - p.cs[g];
+    const int ni = p.cs[g + 1] - p.cs[g];
     if (ni > 0) {
       const float rc = cell_range(p, t, x, y, z, rcp);
+      rcbits = __float_as_int(rc);
       const int R = stencil_radius(rc, rcp, p.rcs);
       if (R > rcp) atomicOr(p.err, 1 << CUBE_ERR_INVALID);  // beyond the one coarse-cell halo
       const float h = (float)p.rcs / (float)rcp;
       const int Rc = min(R, rcp);
+      int64_t nj = 0;
       for (int dz = -Rc; dz <= Rc; dz++)
         for (int dy = -Rc; dy <= Rc; dy++) {
           if (!row_needed(dy, dz, h, rc * rc)) continue;
           const int64_t b = g + ((int64_t)dz * S + dy) * S;
           nj += p.cs[b + Rc + 1] - p.cs[b - Rc];
         }
-      nchunks = (ni + 31) >> 5;
+      nfull = ni / kPPChunk;
+      bfull = cost_bucket(kPPChunk, nj);
+      if (ni % kPPChunk) brem = cost_bucket(ni % kPPChunk, nj);
     }
   }
-  int myrank[4];
-  int mybucket[4];
-  // chunks beyond the first few per thread are rare; handle the first 4 with local ranks,
-  // the rest with direct global atomics
-  for (int k = 0; k < nchunks; k++) {
-    const int nik = min(32, ni - 32 * k);
-    const int b = cost_bucket(nik, nj);
-    if (k < 4) {
-      mybucket[k] = b;
-      myrank[k] = atomicAdd(&sc[b], 1);
-    } else if (PASS == 0) {
-      atomicAdd(&p.bucket[b], 1);
-    } else {
-      const int slot = soff[b] + atomicAdd(&p.bucket[kBuckets + b], 1);
-      if (slot < p.item_cap) p.items[slot] = make_int4((int)g, k, t, 0);
-      else atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
-    }
-  }
+  int rfull = 0, rrem = 0;
+  if (nfull) rfull = atomicAdd(&sc[bfull], nfull);
+  if (brem >= 0) rrem = atomicAdd(&sc[brem], 1);
   __syncthreads();
   if (threadIdx.x < kBuckets) {
     const int n = sc[threadIdx.x];
@@ -223,10 +248,14 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
   }
   if (PASS == 1) {
     __syncthreads();
-    for (int k = 0; k < nchunks && k < 4; k++) {
-      const int b = mybucket[k];
-      const int64_t slot = (int64_t)soff[b] + sbase[b] + myrank[k];
-      if (slot < p.item_cap) p.items[slot] = make_int4((int)g, k, t, 0);
+    const int64_t f0 = (int64_t)soff[bfull] + sbase[bfull] + rfull;
+    for (int k = 0; k < nfull; k++) {
+      if (f0 + k < p.item_cap) p.items[f0 + k] = make_int4((int)g, k, t, rcbits);
+      else atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
+    }
+    if (brem >= 0) {
+      const int64_t slot = (int64_t)soff[brem] + sbase[brem] + rrem;
+      if (slot < p.item_cap) p.items[slot] = make_int4((int)g, nfull, t, rcbits);
       else atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
     }
   }
@@ -235,10 +264,11 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
 // COUNT = false: forces and kick.  COUNT = true: only count the accepted ordered
 // pairs 0 < r^2 < rc^2 (the algorithmic work of the kick, for the roofline).
 template <bool COUNT>
-__global__ void __launch_bounds__(kPPThreads, 3) k_pp_force(PPK p) {
+__global__ void __launch_bounds__(kPPThreads, 4) k_pp_force(PPK p) {
   extern __shared__ float4 pp_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float4 *buf = pp_smem + warp * kJTile;
+  float4 *buf = reinterpret_cast<float4 *>(reinterpret_cast<char *>(pp_smem) + warp * kPPSmemWarp);
+  int2 *rows = reinterpret_cast<int2 *>(buf + kJTile + 32);  // (end of the row in the walk, start - walk offset)
   int total = 0;
   {
     int v = lane < kBuckets ? p.bucket[lane] : 0;
@@ -257,50 +287,72 @@ __global__ void __launch_bounds__(kPPThreads, 3) k_pp_force(PPK p) {
     const int t = item.z;
     const TilePP tp = p.tiles[t];
     const int S = tp.S, rcp = tp.rcp;
-    const int64_t loc = g - tp.cell0;
-    const int x = (int)(loc % S), y = (int)((loc / S) % S), z = (int)(loc / ((int64_t)S * S));
-    const float rc = cell_range(p, t, x, y, z, rcp);
+    const float rc = __int_as_float(item.w);
     const float rc2 = rc * rc;
     const int R = min(stencil_radius(rc, rcp, p.rcs), rcp);
     const float h = (float)p.rcs / (float)rcp;
     PairLaw law;
     law.init(rc, p.app);
 
-    const int i0 = p.cs[g] + item.y * 32;
-    const int ni = min(32, p.cs[g + 1] - i0);
+    const int i0 = p.cs[g] + item.y * kPPChunk;
+    const int ni = min(kPPChunk, p.cs[g + 1] - i0);
     // lanes = ngrp groups of ni lanes; group `grp` walks every ngrp-th candidate
     const int ngrp = 32 / ni;
-    const int il = lane % ni, grp = lane / ni;
+    const int grp = div_small(lane, ni), il = lane - grp * ni;
     const bool has_i = grp < ngrp;  // the 32 mod ni leftover lanes idle
     const float4 pi = p.spos[i0 + il];
 
     // bounding box of the item's particles: candidates farther than rc from it are dropped
     // while staging, so the pair loop below only sees possibly-interacting candidates
-    const float blx = warp_min(pi.x), bhx = warp_max(pi.x), bly = warp_min(pi.y), bhy = warp_max(pi.y),
-                blz = warp_min(pi.z), bhz = warp_max(pi.z);
+    const float blx = warp_min_redux(pi.x), bhx = warp_max_redux(pi.x), bly = warp_min_redux(pi.y),
+                bhy = warp_max_redux(pi.y), blz = warp_min_redux(pi.z), bhz = warp_max_redux(pi.z);
     float sx_ = 0.f, cx_ = 0.f, sy_ = 0.f, cy_ = 0.f, sz_ = 0.f, cz_ = 0.f;
     int nbuf = 0;  // staged candidates (warp-uniform)
+    // Evaluate the staged candidates: group grp takes buf[grp + k*ngrp] in round k.  The loop
+    // bound is the same for every lane (no divergent loop exits): the slots past nbuf hold a
+    // far-away sentinel that the r < rc mask drops, and the lanes of an incomplete last group
+    // (grp == ngrp) compute values that the group merge below never reads.  The main loop has
+    // no branch: pairs inside the softening length (r <= app, common only in dense clumps) are
+    // masked out of it and their rounds recorded in a bit mask (at most 32 rounds per flush);
+    // a second loop then evaluates exactly those pairs, one per lane per step.
     auto flush = [&]() {
+      buf[nbuf + lane] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
       __syncwarp();
       float px = 0.f, py = 0.f, pz = 0.f;
-#pragma unroll 4
-      for (int q = has_i ? grp : nbuf; q < nbuf; q += ngrp) {
-        const float4 pj = buf[q];
+      const int nround = div_small(nbuf + ngrp - 1, ngrp);
+      unsigned softmask = 0u, bit = 1u;
+      const float4 *bp = buf + grp;
+#pragma unroll kPairUnroll
+      for (int k = 0; k < nround; k++, bp += ngrp, bit <<= 1) {
+        const float4 pj = *bp;
         const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
-        const float r2 = dx * dx + dy_ * dy_ + dz_ * dz_;
-        const bool ok = (r2 > 0.0f) & (r2 < rc2);
+        const float r2 = fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_));
         if (COUNT) {
-          npairs += ok ? 1ull : 0ull;
+          npairs += (r2 < rc2) & (r2 > 0.0f) & has_i ? 1ull : 0ull;  // r = 0: the particle itself
         } else {
           // evaluated for every candidate and masked: a divergent accept branch would
-          // run on nearly every iteration of a 32-lane warp anyway
-          const float s = ok ? law.scale(r2) : 0.0f;
+          // run on nearly every round of a 32-lane warp anyway
+          float s = law.scale(r2);
+          s = (r2 < rc2) & (r2 > law.app2) ? s : 0.0f;
+          softmask |= (r2 <= law.app2) & (r2 > 0.0f) & has_i ? bit : 0u;
           px = fmaf(s, dx, px);
           py = fmaf(s, dy_, py);
           pz = fmaf(s, dz_, pz);
         }
       }
       if (!COUNT) {
+        while (__any_sync(0xffffffffu, softmask != 0u)) {
+          if (softmask) {
+            const int k = __ffs(softmask) - 1;
+            softmask &= softmask - 1u;
+            const float4 pj = buf[grp + k * ngrp];
+            const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
+            const float s = law.soft(fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_)));
+            px = fmaf(s, dx, px);
+            py = fmaf(s, dy_, py);
+            pz = fmaf(s, dz_, pz);
+          }
+        }
         kahan_add(sx_, cx_, px);
         kahan_add(sy_, cy_, py);
         kahan_add(sz_, cz_, pz);
@@ -308,28 +360,62 @@ __global__ void __launch_bounds__(kPPThreads, 3) k_pp_force(PPK p) {
       nbuf = 0;
       __syncwarp();
     };
-    for (int dz = -R; dz <= R; dz++)
-      for (int dy = -R; dy <= R; dy++) {
-        if (!row_needed(dy, dz, h, rc2)) continue;
-        const int64_t b = g + ((int64_t)dz * S + dy) * S;
-        const int js = p.cs[b - R], je = p.cs[b + R + 1];
-        for (int jb = js; jb < je; jb += 32) {
-          const int q = jb + lane;
-          bool keep = q < je;
-          float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (keep) {
-            pj = p.spos[q];
-            const float ex = fmaxf(fmaxf(blx - pj.x, pj.x - bhx), 0.f);
-            const float ey = fmaxf(fmaxf(bly - pj.y, pj.y - bhy), 0.f);
-            const float ez = fmaxf(fmaxf(blz - pj.z, pj.z - bhz), 0.f);
-            keep = ex * ex + ey * ey + ez * ez < rc2;
+    // The needed stencil rows are laid end to end in a table of up to kMaxRows rows: row k
+    // covers walk positions [rows[k-1].x, rows[k].x), and walk position v is particle
+    // v + rows[k].y.  Stencils with more rows (large R) are walked in several tables.
+    const int side = 2 * R + 1, nr = side * side;
+    for (int r0 = 0; r0 < nr;) {
+      int nrows = 0, walk = 0;
+      for (; r0 < nr && nrows <= kMaxRows - 32; r0 += 32) {
+        const int ri = r0 + lane;
+        int js = 0, len = 0;
+        bool need = false;
+        if (ri < nr) {
+          const int q = div_small(ri, side);
+          const int dz = q - R, dy = ri - q * side - R;
+          need = row_needed(dy, dz, h, rc2);
+          if (need) {
+            const int64_t b = g + ((int64_t)dz * S + dy) * S;
+            js = p.cs[b - R];
+            len = p.cs[b + R + 1] - js;
           }
-          const unsigned m = __ballot_sync(0xffffffffu, keep);
-          if (keep) buf[nbuf + __popc(m & ((1u << lane) - 1u))] = pj;
-          nbuf += __popc(m);
-          if (nbuf > kJTile - 32) flush();
         }
+        const unsigned m = __ballot_sync(0xffffffffu, need);
+        int incl = len;  // inclusive scan of the lengths (0 for rows not needed)
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        if (need) rows[nrows + __popc(m & ((1u << lane) - 1u))] = make_int2(walk + incl, js - (walk + incl - len));
+        nrows += __popc(m);
+        walk += __shfl_sync(0xffffffffu, incl, 31);
       }
+      __syncwarp();
+      if (walk == 0) continue;
+      // Walk position -> particle.  Each lane's row index only moves forward and stops at the
+      // last row (rows[nrows-1].x = walk > v), and the lanes past the end load the last
+      // candidate again and drop it, so the loop below has no divergent branch or load.
+      int kr = 0;
+      auto locate = [&](int v) {
+        v = min(v, walk - 1);
+        while (__any_sync(0xffffffffu, v >= rows[kr].x)) kr += v >= rows[kr].x ? 1 : 0;
+        return v + rows[kr].y;
+      };
+      float4 nxt = p.spos[locate(lane)];
+      for (int vb = 0; vb < walk; vb += 32) {
+        const float4 pj = nxt;
+        nxt = p.spos[locate(vb + 32 + lane)];  // one step ahead
+        const float ex = fmaxf(fmaxf(blx - pj.x, pj.x - bhx), 0.f);
+        const float ey = fmaxf(fmaxf(bly - pj.y, pj.y - bhy), 0.f);
+        const float ez = fmaxf(fmaxf(blz - pj.z, pj.z - bhz), 0.f);
+        const bool keep = (vb + lane < walk) & (ex * ex + ey * ey + ez * ez < rc2);
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) buf[nbuf + __popc(m & ((1u << lane) - 1u))] = pj;
+        nbuf += __popc(m);
+        if (nbuf > kJTile - 32) flush();
+      }
+      __syncwarp();  // the next table overwrites this one
+    }
     if (nbuf) flush();
     // merge the lane groups of each i-particle (tree over groups, stride s*ni lanes);
     // Kahan c is the negated low part
