@@ -52,10 +52,14 @@ struct Ctx {
   int device = -1;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
+  // Host entry points upload vp on `copy` while PM3 runs; the compute stream waits on
+  // vp_ready just before the first kernel that reads vp (the PM3 gather or the PP force).
+  cudaStream_t copy = nullptr;
+  cudaEvent_t vp_ready = nullptr;
+  bool vp_pending = false;
   Buf xp, rhoc, idx, vp, cell_base;
   Buf tiles, count, cell_start, scan_tmp, spos, spill, spill_rank, counters, items, range_loc;
-  Buf rho, rhok, fk, force, dtab, jobs, out;
-  int dtab_n = -1;
+  Buf rho, rhok, force, jobs, out;
   void *h_stage = nullptr;  // pinned staging for small tables
   size_t h_stage_cap = 0;
   float *h_out = nullptr;   // pinned [8]: out[5], err
@@ -158,6 +162,8 @@ static int ensure_device() {
   g.device = dev;
   CU(cudaDeviceGetAttribute(&g.num_sms, cudaDevAttrMultiProcessorCount, dev));
   CU(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+  CU(cudaStreamCreateWithFlags(&g.copy, cudaStreamNonBlocking));
+  CU(cudaEventCreateWithFlags(&g.vp_ready, cudaEventDisableTiming));
   CU(cudaMallocHost(&g.h_out, sizeof(float) * 8));
   for (auto &slot : g.ring)
     for (auto &e : slot) CU(cudaEventCreate(&e));
@@ -205,6 +211,14 @@ static int upload(Buf &dst, const T *src, size_t count, size_t &stage_off) {
   memcpy((char *)g.h_stage + stage_off, src, bytes);
   CU(cudaMemcpyAsync(dst.p, (char *)g.h_stage + stage_off, bytes, cudaMemcpyHostToDevice, g.stream));
   stage_off += bytes;
+  return CUBE_OK;
+}
+
+// order the compute stream after a pending vp upload
+static int wait_vp() {
+  if (!g.vp_pending) return CUBE_OK;
+  CU(cudaStreamWaitEvent(g.stream, g.vp_ready, 0));
+  g.vp_pending = false;
   return CUBE_OK;
 }
 
@@ -343,27 +357,6 @@ static int get_green_host(const float *host, int n, float **out) {
   return CUBE_OK;
 }
 
-// spectral symbol of potential_to_force: D(k) = a sin k + (1-a) sin 2k / 2 with a = real(4) 4/3
-// (parameters.f90:49-50); 0 at k = 0 and at the Nyquist frequency
-static int get_dtab(int n) {
-  CK(grow(g.dtab, sizeof(float) * n));
-  if (g.dtab_n == n) return CUBE_OK;
-  std::vector<float> d(n);
-  const double a = (double)(4.0f / 3.0f), pi = 3.14159265358979323846;
-  for (int w = 0; w < n; w++) {
-    const int m = w < (n + 1) / 2 ? w : w - n;
-    if (m == 0 || (n % 2 == 0 && m == -n / 2)) {
-      d[w] = 0.f;
-      continue;
-    }
-    const double th = 2.0 * pi * (double)m / (double)n;
-    d[w] = (float)(a * sin(th) + (1 - a) * sin(2 * th) / 2);
-  }
-  CU(cudaMemcpy(g.dtab.p, d.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
-  g.dtab_n = n;
-  return CUBE_OK;
-}
-
 static const int kFftBuckets[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512};
 
 static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, const float *const *gk,
@@ -377,10 +370,8 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     const int64_t n3 = (int64_t)n * n * n, nk = (int64_t)n * n * (n / 2 + 1);
     float *G = nullptr;
     CK(get_green_periodic(n, rsf, &G));
-    CK(get_dtab(n));
     CK(grow(g.rho, sizeof(float) * n3));
     CK(grow(g.rhok, sizeof(cufftComplex) * nk));
-    CK(grow(g.fk, sizeof(cufftComplex) * nk * 3));
     CK(grow(g.force, sizeof(float) * n3 * 3));
     const double scale = (double)L.rcs / (double)(1.0f / (float)rsf);
     std::vector<MeshJob> jobs(L.ntile);
@@ -416,10 +407,8 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     a.cell_base = (const int64_t *)g.cell_base.p;
     a.rho = (float *)g.rho.p;
     a.rhok = (cufftComplex *)g.rhok.p;
-    a.fk = (cufftComplex *)g.fk.p;
     a.force = (float *)g.force.p;
     a.green = G;
-    a.dtab = (const float *)g.dtab.p;
     a.mass = mass;
     a.kick = kick;
     a.vp = d.vp;
@@ -427,13 +416,14 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     a.want_vmax = want_vmax;
     cufftHandle fw, bw;
     CK(get_plan(n, 1, CUFFT_R2C, &fw));
-    CK(get_plan(n, 3, CUFFT_C2R, &bw));
+    CK(get_plan(n, 1, CUFFT_C2R, &bw));
     CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3, g.stream));
     launch_pm3_deposit(a, g.stream);
     CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
     launch_pm3_kspace(a, g.stream);
-    CF(cufftExecC2R(bw, (cufftComplex *)g.fk.p, (cufftReal *)g.force.p));
-    launch_pm3_f2max(a, g.stream);
+    CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)g.rho.p));  // potential
+    launch_pm3_force(a, g.stream);
+    CK(wait_vp());
     launch_pm3_gather(a, g.stream);
     g.launches += 4;
     CU(cudaGetLastError());
@@ -451,9 +441,8 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     const int64_t n3 = (int64_t)n * n * n, nk = (int64_t)n * n * (n / 2 + 1);
     float *G = nullptr;
     CK(get_green_host(gk[lev - 2], n, &G));
-    CK(get_dtab(n));
     const double scale = (double)L.rcs / (double)(1.0f / (float)rsf);
-    const size_t per_slot = sizeof(float) * (size_t)n3 * 4 + sizeof(cufftComplex) * (size_t)nk * 4;
+    const size_t per_slot = sizeof(float) * (size_t)n3 * 4 + sizeof(cufftComplex) * (size_t)nk;
     const size_t budget = (size_t)8 << 30;
     int bmax = (int)std::max<size_t>(1, budget / per_slot);
     bmax = std::min<int>(bmax, 512);
@@ -467,7 +456,6 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
         }
       CK(grow(g.rho, sizeof(float) * n3 * nb));
       CK(grow(g.rhok, sizeof(cufftComplex) * nk * nb));
-      CK(grow(g.fk, sizeof(cufftComplex) * nk * 3 * nb));
       CK(grow(g.force, sizeof(float) * n3 * 3 * nb));
       std::vector<MeshJob> jobs(nj);
       for (int j = 0; j < nj; j++) {
@@ -507,10 +495,8 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       a.cell_base = (const int64_t *)g.cell_base.p;
       a.rho = (float *)g.rho.p;
       a.rhok = (cufftComplex *)g.rhok.p;
-      a.fk = (cufftComplex *)g.fk.p;
       a.force = (float *)g.force.p;
       a.green = G;
-      a.dtab = (const float *)g.dtab.p;
       a.mass = mass;
       a.kick = kick;
       a.vp = d.vp;
@@ -518,14 +504,15 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       a.want_vmax = want_vmax;
       cufftHandle fw, bw;
       CK(get_plan(n, nb, CUFFT_R2C, &fw));
-      CK(get_plan(n, 3 * nb, CUFFT_C2R, &bw));
+      CK(get_plan(n, nb, CUFFT_C2R, &bw));
       CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3 * nb, g.stream));
       launch_pm3_deposit(a, g.stream);
       CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
       launch_pm3_kspace(a, g.stream);
-      CF(cufftExecC2R(bw, (cufftComplex *)g.fk.p, (cufftReal *)g.force.p));
-      a.nslots = nj;  // f2max over the real jobs only
-      launch_pm3_f2max(a, g.stream);
+      CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)g.rho.p));  // potentials
+      a.nslots = nj;  // force and f2max of the real jobs only
+      launch_pm3_force(a, g.stream);
+      CK(wait_vp());
       launch_pm3_gather(a, g.stream);
       g.launches += 4;
       CU(cudaGetLastError());
@@ -602,6 +589,7 @@ static int run_pp(const Meta &m, const Dev &d, float mass, float kick, size_t &s
   launch_pp_items(p, g.stream);
   CU(cudaGetLastError());
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][6], g.stream));
+  CK(wait_vp());
   launch_pp_force(p, g.stream);
   g.launches += 3;
   CU(cudaGetLastError());
@@ -707,10 +695,19 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   CU(cudaMemcpyAsync(g.idx.p, idx_b_r, sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, g.stream));
   if (n_used) {
     CU(cudaMemcpyAsync(g.xp.p, xp, sizeof(int16_t) * 3 * n_used, cudaMemcpyHostToDevice, g.stream));
-    CU(cudaMemcpyAsync(g.vp.p, vp, sizeof(float) * 3 * n_used, cudaMemcpyHostToDevice, g.stream));
+    // vp travels beside the deposit and FFTs; the stream waits for it before the first use
+    CU(cudaMemcpyAsync(g.vp.p, vp, sizeof(float) * 3 * n_used, cudaMemcpyHostToDevice, g.copy));
+    CU(cudaEventRecord(g.vp_ready, g.copy));
+    g.vp_pending = true;
   }
   Dev d{(const int16_t *)g.xp.p, (const int32_t *)g.rhoc.p, (const int64_t *)g.idx.p, (float *)g.vp.p, n_used};
-  CK(run_kick(ires, ixyz3, ratio_sf, apm3, gk, d, mass, a_mid, dt, do_pm3, do_pp, m));
+  const int st = run_kick(ires, ixyz3, ratio_sf, apm3, gk, d, mass, a_mid, dt, do_pm3, do_pp, m);
+  const int wst = wait_vp();  // also on a failed or vp-free run: the D2H below must follow the upload
+  if (st != CUBE_OK || wst != CUBE_OK) {
+    cudaStreamSynchronize(g.copy);
+    cudaStreamSynchronize(g.stream);
+    return st != CUBE_OK ? st : wst;
+  }
   if (n_used) CU(cudaMemcpyAsync(vp, g.vp.p, sizeof(float) * 3 * n_used, cudaMemcpyDeviceToHost, g.stream));
   CU(cudaMemcpyAsync(g.h_out, g.out.p, sizeof(float) * 6, cudaMemcpyDeviceToHost, g.stream));
   CU(cudaStreamSynchronize(g.stream));
@@ -907,11 +904,8 @@ void c_pm3_fft_finalize(void) {
   g.hgreens.clear();
   release(g.rho);
   release(g.rhok);
-  release(g.fk);
   release(g.force);
-  release(g.dtab);
   release(g.jobs);
-  g.dtab_n = -1;
 }
 
 void c_gpu_velocity_finalize(void) {

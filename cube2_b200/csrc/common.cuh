@@ -143,12 +143,10 @@ struct PM3Args {
   const int16_t *xp;
   const int32_t *rhoc;
   const int64_t *cell_base;
-  float *rho;            // [nslots][n^3]
+  float *rho;            // [nslots][n^3] density, then potential
   cufftComplex *rhok;    // [nslots][n*n*(n/2+1)]
-  cufftComplex *fk;      // [nslots*3][n*n*(n/2+1)]
   float *force;          // [nslots*3][n^3]
   const float *green;    // [n*n*(n/2+1)]
-  const float *dtab;     // [n] finite-difference symbol D(k) per signed wavenumber index
   float mass, kick;
   float *vp;
   float *out;
@@ -156,7 +154,7 @@ struct PM3Args {
 };
 void launch_pm3_deposit(const PM3Args &a, cudaStream_t s);
 void launch_pm3_kspace(const PM3Args &a, cudaStream_t s);
-void launch_pm3_f2max(const PM3Args &a, cudaStream_t s);
+void launch_pm3_force(const PM3Args &a, cudaStream_t s);  // force arrays + f2max from the potential
 void launch_pm3_gather(const PM3Args &a, cudaStream_t s);
 void launch_green_fp64(int n, double apm_soft, double apm_range, double gridsize, int p_order, float *G,
                        cudaStream_t s);

@@ -6,16 +6,13 @@
 //            (the cost follows the particles, not the mesh, which matters for
 //            clustered boxes where most mesh bricks are nearly empty);
 //   R2C      cuFFT;
-//   k-space  one kernel multiplies by the Green table and by the spectral
-//            symbol of the 4-point difference, i*D(k) with
-//            D = a sin k + (1-a) sin 2k / 2, a = 4/3 -- the exact Fourier image
-//            of potential_to_force (kick.f90:545-568) on the FFT mesh -- and
-//            writes the three force spectra;
-//   C2R      cuFFT, batched over the 3 components (three separate arrays: a
-//            stride-4 interleaved output measured slower for both cuFFT and
-//            the gather);
-//   f2max    max |F|^2 over the physical mesh points (kick.f90:494), float4
-//            loads along x;
+//   k-space  the potential spectrum: rho(k) * G(k) * mass / n^3, in place
+//            (kick.f90:472-491 and the 1/nwork^3 of kick.f90:552);
+//   C2R      cuFFT, one transform per mesh;
+//   force    the 4-point difference of potential_to_force (kick.f90:545-568)
+//            on the periodic FFT mesh, four x points per thread, writing the
+//            three force arrays and the max |F|^2 over the physical mesh
+//            points (kick.f90:494) in the same pass;
 //   gather   TSC gather of the force at each active particle and the kick
 //            vp += dv * a_mid*dt/(6 pi) (kick.f90:497-540).
 #include <cmath>
@@ -35,12 +32,10 @@ struct PM3K {
   const int16_t *xp;
   const int32_t *rhoc;
   const int64_t *cell_base;
-  float *rho;
-  const cufftComplex *rhok;
-  cufftComplex *fk;
-  const float *force;  // [slot][3][n^3]
+  float *rho;           // density, then potential [slot][n^3]
+  cufftComplex *rhok;
+  float *force;  // [slot][3][n^3]
   const float *green;
-  const float *dtab;
   float gscale;  // mass / n^3
   float kick;
   float *vp;
@@ -101,67 +96,104 @@ __global__ void __launch_bounds__(kWarps * 32) k_deposit(PM3K p) {
   }
 }
 
-// fk[slot][d] = i * D_d(k) * G(k) * mass / n^3 * rhok[slot]
+// potential spectrum in place: rhok[slot] *= G(k) * mass / n^3
 __global__ void k_kspace(PM3K p) {
   const int64_t total = p.nk * p.nslots;
-  const int n = p.n, nh = n / 2 + 1;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int slot = (int)(e / p.nk);
-    const int64_t k = e - (int64_t)slot * p.nk;
-    const int kx = (int)(k % nh);
-    const int ky = (int)((k / nh) % n);
-    const int kz = (int)(k / ((int64_t)nh * n));
+    const int64_t k = e % p.nk;
     const float g = p.green[k] * p.gscale;
     const cufftComplex c = p.rhok[e];
-    const float re = c.x * g, im = c.y * g;
-    const float D[3] = {p.dtab[kx], p.dtab[ky], p.dtab[kz]};
-    cufftComplex *F = p.fk + (int64_t)slot * 3 * p.nk + k;
-#pragma unroll
-    for (int d = 0; d < 3; d++) F[d * p.nk] = make_float2(-D[d] * im, D[d] * re);
+    p.rhok[e] = make_float2(c.x * g, c.y * g);
   }
 }
 
-__global__ void k_f2max(PM3K p) {
+// a + d into [0, n) for |d| < n
+__device__ __forceinline__ int64_t wrap_near(int64_t a, int64_t n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+
+// weights of potential_to_force at offsets -2, -1, +1, +2 (parameters.f90:49-50, a = real(4) 4/3)
+struct FDW {
+  float m2, m1, p1, p2;
+  __device__ __forceinline__ FDW() {
+    const float a = 4.0f / 3.0f;
+    m2 = (a - 1.0f) / 4.0f;
+    m1 = -a / 2.0f;
+    p1 = a / 2.0f;
+    p2 = (1.0f - a) / 4.0f;
+  }
+  __device__ __forceinline__ float operator()(float fm2, float fm1, float fp1, float fp2) const {
+    return fm2 * m2 + fm1 * m1 + fp1 * p1 + fp2 * p2;  // sum(phi(i_n) * weight), kick.f90:562-564
+  }
+};
+
+__device__ __forceinline__ bool in_phys(const PM3K &p, int64_t x, int64_t y, int64_t z) {
+  return x >= p.fphys_lo && x < p.fphys_lo + p.fphys_n && y >= p.fphys_lo && y < p.fphys_lo + p.fphys_n &&
+         z >= p.fphys_lo && z < p.fphys_lo + p.fphys_n;
+}
+
+// Force from the potential on the periodic mesh, four consecutive x points per thread
+// (n % 4 == 0): 11 float4 loads (x-4..x+7 in the row, rows y+-1, y+-2, planes z+-1, z+-2) and
+// 3 float4 stores; |F|^2 of the physical points is reduced into out[0].
+__global__ void k_force_v4(PM3K p) {
+  const FDW w;
+  const int64_t n = p.n, n4 = p.n / 4;
+  const int64_t per_slot = n4 * n * n;
+  const int64_t total = per_slot * p.nslots;
   float m = 0.f;
-  const int64_t nph = (int64_t)p.fphys_n * p.fphys_n * p.fphys_n;
-  const int64_t total = nph * p.nslots;
-  const int64_t n = p.n;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int slot = (int)(e / nph);
-    const int64_t r = e - slot * nph;
-    const int64_t x = r % p.fphys_n + p.fphys_lo, y = (r / p.fphys_n) % p.fphys_n + p.fphys_lo,
-                  z = r / ((int64_t)p.fphys_n * p.fphys_n) + p.fphys_lo;
-    const int64_t q = (z * n + y) * n + x;
-    const float *F = p.force + (int64_t)slot * 3 * p.n3;
-    const float a = F[q], b = F[p.n3 + q], c = F[2 * p.n3 + q];
-    m = fmaxf(m, a * a + b * b + c * c);
+    const int64_t slot = e / per_slot, r = e - slot * per_slot;
+    const int64_t x4 = r % n4, y = (r / n4) % n, z = r / (n4 * n);
+    const float4 *phi = reinterpret_cast<const float4 *>(p.rho + slot * p.n3);
+    auto row = [&](int64_t yy, int64_t zz) { return phi + (wrap_near(zz, n) * n + wrap_near(yy, n)) * n4; };
+    const float4 *c = row(y, z);
+    const float4 l = __ldg(c + (x4 + n4 - 1) % n4), o = __ldg(c + x4), rr = __ldg(c + (x4 + 1) % n4);
+    const float4 ym2 = __ldg(row(y - 2, z) + x4), ym1 = __ldg(row(y - 1, z) + x4), yp1 = __ldg(row(y + 1, z) + x4),
+                 yp2 = __ldg(row(y + 2, z) + x4);
+    const float4 zm2 = __ldg(row(y, z - 2) + x4), zm1 = __ldg(row(y, z - 1) + x4), zp1 = __ldg(row(y, z + 1) + x4),
+                 zp2 = __ldg(row(y, z + 2) + x4);
+    const float4 fx = make_float4(w(l.z, l.w, o.y, o.z), w(l.w, o.x, o.z, o.w), w(o.x, o.y, o.w, rr.x),
+                                  w(o.y, o.z, rr.x, rr.y));
+    const float4 fy = make_float4(w(ym2.x, ym1.x, yp1.x, yp2.x), w(ym2.y, ym1.y, yp1.y, yp2.y),
+                                  w(ym2.z, ym1.z, yp1.z, yp2.z), w(ym2.w, ym1.w, yp1.w, yp2.w));
+    const float4 fz = make_float4(w(zm2.x, zm1.x, zp1.x, zp2.x), w(zm2.y, zm1.y, zp1.y, zp2.y),
+                                  w(zm2.z, zm1.z, zp1.z, zp2.z), w(zm2.w, zm1.w, zp1.w, zp2.w));
+    float4 *F = reinterpret_cast<float4 *>(p.force + slot * 3 * p.n3) + (z * n + y) * n4 + x4;
+    F[0] = fx;
+    F[n * n * n4] = fy;
+    F[2 * n * n * n4] = fz;
+    const int64_t x = 4 * x4;
+    if (in_phys(p, x, y, z)) m = fmaxf(m, fx.x * fx.x + fy.x * fy.x + fz.x * fz.x);
+    if (in_phys(p, x + 1, y, z)) m = fmaxf(m, fx.y * fx.y + fy.y * fy.y + fz.y * fz.y);
+    if (in_phys(p, x + 2, y, z)) m = fmaxf(m, fx.z * fx.z + fy.z * fy.z + fz.z * fz.z);
+    if (in_phys(p, x + 3, y, z)) m = fmaxf(m, fx.w * fx.w + fy.w * fy.w + fz.w * fz.w);
   }
   m = warp_max(m);
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&p.out[0], m);
 }
 
-// f2max with float4 loads along x (the physical region starts and ends on multiples of 4)
-__global__ void k_f2max_v4(PM3K p) {
-  float m = 0.f;
-  const int64_t g4 = p.fphys_n / 4;
-  const int64_t nph = g4 * p.fphys_n * p.fphys_n;
-  const int64_t total = nph * p.nslots;
+// the same, one point per thread, for any n
+__global__ void k_force(PM3K p) {
+  const FDW w;
   const int64_t n = p.n;
+  const int64_t total = p.n3 * p.nslots;
+  float m = 0.f;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int slot = (int)(e / nph);
-    const int64_t r = e - slot * nph;
-    const int64_t x = 4 * (r % g4) + p.fphys_lo, y = (r / g4) % p.fphys_n + p.fphys_lo,
-                  z = r / (g4 * p.fphys_n) + p.fphys_lo;
-    const int64_t q = (z * n + y) * n + x;
-    const float *F = p.force + (int64_t)slot * 3 * p.n3;
-    const float4 a = __ldg(reinterpret_cast<const float4 *>(F + q));
-    const float4 b = __ldg(reinterpret_cast<const float4 *>(F + p.n3 + q));
-    const float4 c = __ldg(reinterpret_cast<const float4 *>(F + 2 * p.n3 + q));
-    m = fmaxf(m, fmaxf(fmaxf(a.x * a.x + b.x * b.x + c.x * c.x, a.y * a.y + b.y * b.y + c.y * c.y),
-                       fmaxf(a.z * a.z + b.z * b.z + c.z * c.z, a.w * a.w + b.w * b.w + c.w * c.w)));
+    const int64_t slot = e / p.n3, r = e - slot * p.n3;
+    const int64_t x = r % n, y = (r / n) % n, z = r / (n * n);
+    const float *phi = p.rho + slot * p.n3;
+    auto at = [&](int64_t xx, int64_t yy, int64_t zz) {
+      return __ldg(phi + (wrap_near(zz, n) * n + wrap_near(yy, n)) * n + wrap_near(xx, n));
+    };
+    const float fx = w(at(x - 2, y, z), at(x - 1, y, z), at(x + 1, y, z), at(x + 2, y, z));
+    const float fy = w(at(x, y - 2, z), at(x, y - 1, z), at(x, y + 1, z), at(x, y + 2, z));
+    const float fz = w(at(x, y, z - 2), at(x, y, z - 1), at(x, y, z + 1), at(x, y, z + 2));
+    float *F = p.force + slot * 3 * p.n3 + r;
+    F[0] = fx;
+    F[p.n3] = fy;
+    F[2 * p.n3] = fz;
+    if (in_phys(p, x, y, z)) m = fmaxf(m, fx * fx + fy * fy + fz * fz);
   }
   m = warp_max(m);
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&p.out[0], m);
@@ -254,10 +286,8 @@ static PM3K make_k(const PM3Args &a) {
   p.cell_base = a.cell_base;
   p.rho = a.rho;
   p.rhok = a.rhok;
-  p.fk = a.fk;
   p.force = a.force;
   p.green = a.green;
-  p.dtab = a.dtab;
   p.gscale = (float)((double)a.mass / ((double)a.n * a.n * a.n));
   p.kick = a.kick;
   p.vp = a.vp;
@@ -280,12 +310,12 @@ void launch_pm3_kspace(const PM3Args &a, cudaStream_t s) {
   k_kspace<<<148 * 8, 256, 0, s>>>(p);
 }
 
-void launch_pm3_f2max(const PM3Args &a, cudaStream_t s) {
+void launch_pm3_force(const PM3Args &a, cudaStream_t s) {
   PM3K p = make_k(a);
-  if (a.fphys_lo % 4 == 0 && a.fphys_n % 4 == 0 && a.n % 4 == 0)
-    k_f2max_v4<<<148 * 8, 256, 0, s>>>(p);
+  if (a.n % 4 == 0)
+    k_force_v4<<<148 * 8, 256, 0, s>>>(p);
   else
-    k_f2max<<<148 * 8, 256, 0, s>>>(p);
+    k_force<<<148 * 8, 256, 0, s>>>(p);
 }
 
 void launch_pm3_gather(const PM3Args &a, cudaStream_t s) {
