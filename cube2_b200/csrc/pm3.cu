@@ -77,6 +77,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_deposit(PM3K p) {
     const int64_t ix = tsc(decode_pos(ci - p.ncb, q[0]) * p.scale - J.off[0], wx) + p.shift;
     const int64_t iy = tsc(decode_pos(cj - p.ncb, q[1]) * p.scale - J.off[1], wy) + p.shift;
     const int64_t iz = tsc(decode_pos(ck - p.ncb, q[2]) * p.scale - J.off[2], wz) + p.shift;
+    // the three x points of a row are one vector reduction when they lie in a 16-byte
+    // window, else a pair and a single (rows are 16-byte aligned when n % 4 == 0)
+    const bool vec = (n % 4 == 0) && ix >= 1 && ix + 1 < n;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       int64_t Z = iz + c - 1;
@@ -85,11 +88,29 @@ __global__ void __launch_bounds__(kWarps * 32) k_deposit(PM3K p) {
       for (int b = 0; b < 3; b++) {
         int64_t Y = iy + b - 1;
         if (p.wrap) Y = wrapi(Y, n); else if (Y < 0 || Y >= n) continue;
+        float *row = R + (Z * n + Y) * n;
+        const float w0 = (wx[0] * wy[b]) * wz[c], w1 = (wx[1] * wy[b]) * wz[c], w2 = (wx[2] * wy[b]) * wz[c];
+        if (vec) {
+          const int64_t x0 = ix - 1, o = x0 & 3, b4 = x0 - o;
+          if (o == 0) {
+            atomicAdd(reinterpret_cast<float4 *>(row + b4), make_float4(w0, w1, w2, 0.f));
+          } else if (o == 1) {
+            atomicAdd(reinterpret_cast<float4 *>(row + b4), make_float4(0.f, w0, w1, w2));
+          } else if (o == 2) {
+            atomicAdd(reinterpret_cast<float2 *>(row + b4 + 2), make_float2(w0, w1));
+            atomicAdd(row + b4 + 4, w2);
+          } else {
+            atomicAdd(row + b4 + 3, w0);
+            atomicAdd(reinterpret_cast<float2 *>(row + b4 + 4), make_float2(w1, w2));
+          }
+          continue;
+        }
+        const float wr[3] = {w0, w1, w2};
 #pragma unroll
         for (int a = 0; a < 3; a++) {
           int64_t X = ix + a - 1;
           if (p.wrap) X = wrapi(X, n); else if (X < 0 || X >= n) continue;
-          atomicAdd(R + (Z * n + Y) * n + X, (wx[a] * wy[b]) * wz[c]);
+          atomicAdd(row + X, wr[a]);
         }
       }
     }
@@ -133,7 +154,8 @@ __device__ __forceinline__ bool in_phys(const PM3K &p, int64_t x, int64_t y, int
 
 // Force from the potential on the periodic mesh, four consecutive x points per thread
 // (n % 4 == 0): 11 float4 loads (x-4..x+7 in the row, rows y+-1, y+-2, planes z+-1, z+-2) and
-// 3 float4 stores; |F|^2 of the physical points is reduced into out[0].
+// 3 float4 stores into the three force arrays (an interleaved (fx, fy, fz, 0) layout measured
+// twice as slow in the gather); |F|^2 of the physical points is reduced into out[0].
 __global__ void k_force_v4(PM3K p) {
   const FDW w;
   const int64_t n = p.n, n4 = p.n / 4;
