@@ -45,6 +45,9 @@ struct PM3K {
   int nslots;
 };
 
+// a + d into [0, n) for |d| < n
+__device__ __forceinline__ int64_t wrap_near(int64_t a, int64_t n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+
 // TSC weights in real(4) from a real(8) coordinate (kick.f90:439-445)
 __device__ __forceinline__ int64_t tsc(double m, float w[3]) {
   const double f = floor(m);
@@ -83,11 +86,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_deposit(PM3K p) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       int64_t Z = iz + c - 1;
-      if (p.wrap) Z = wrapi(Z, n); else if (Z < 0 || Z >= n) continue;
+      if (p.wrap) Z = wrap_near(Z, n); else if (Z < 0 || Z >= n) continue;
 #pragma unroll
       for (int b = 0; b < 3; b++) {
         int64_t Y = iy + b - 1;
-        if (p.wrap) Y = wrapi(Y, n); else if (Y < 0 || Y >= n) continue;
+        if (p.wrap) Y = wrap_near(Y, n); else if (Y < 0 || Y >= n) continue;
         float *row = R + (Z * n + Y) * n;
         const float w0 = (wx[0] * wy[b]) * wz[c], w1 = (wx[1] * wy[b]) * wz[c], w2 = (wx[2] * wy[b]) * wz[c];
         if (vec) {
@@ -109,7 +112,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_deposit(PM3K p) {
 #pragma unroll
         for (int a = 0; a < 3; a++) {
           int64_t X = ix + a - 1;
-          if (p.wrap) X = wrapi(X, n); else if (X < 0 || X >= n) continue;
+          if (p.wrap) X = wrap_near(X, n); else if (X < 0 || X >= n) continue;
           atomicAdd(row + X, wr[a]);
         }
       }
@@ -128,9 +131,6 @@ __global__ void k_kspace(PM3K p) {
     p.rhok[e] = make_float2(c.x * g, c.y * g);
   }
 }
-
-// a + d into [0, n) for |d| < n
-__device__ __forceinline__ int64_t wrap_near(int64_t a, int64_t n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
 
 // weights of potential_to_force at offsets -2, -1, +1, +2 (parameters.f90:49-50, a = real(4) 4/3)
 struct FDW {
@@ -221,7 +221,7 @@ __global__ void k_force(PM3K p) {
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&p.out[0], m);
 }
 
-__global__ void __launch_bounds__(kWarps * 32) k_gather(PM3K p) {
+__global__ void __launch_bounds__(kWarps * 32, 4) k_gather(PM3K p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t cells = (int64_t)p.ract[0] * p.ract[1] * p.ract[2];
   const int64_t wid = (int64_t)blockIdx.x * kWarps + warp;
@@ -248,13 +248,13 @@ __global__ void __launch_bounds__(kWarps * 32) k_gather(PM3K p) {
       float d0 = 0.f, d1 = 0.f, d2 = 0.f;
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        const int64_t Z = p.wrap ? wrapi(iz + c - 1, n) : iz + c - 1;
+        const int64_t Z = p.wrap ? wrap_near(iz + c - 1, n) : iz + c - 1;
 #pragma unroll
         for (int b = 0; b < 3; b++) {
-          const int64_t Y = p.wrap ? wrapi(iy + b - 1, n) : iy + b - 1;
+          const int64_t Y = p.wrap ? wrap_near(iy + b - 1, n) : iy + b - 1;
 #pragma unroll
           for (int a = 0; a < 3; a++) {
-            const int64_t X = p.wrap ? wrapi(ix + a - 1, n) : ix + a - 1;
+            const int64_t X = p.wrap ? wrap_near(ix + a - 1, n) : ix + a - 1;
             const int64_t m = (Z * n + Y) * n + X;
             const float w = (wx[a] * wy[b]) * wz[c];
             d0 += F[m] * w;
