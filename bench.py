@@ -38,6 +38,11 @@ if ROOT not in sys.path:
 METRIC = "particle kicks/s (PM3+PP) on 1 B200, learned vs plain at equal rms force error"
 UNIT = "particle-kicks/s"
 PP_FLOP_PER_PAIR = 38  # 3 sub, 5 r^2, rsqrt, 1/r^2, 2 ep, 18 polynomial+reciprocal, 1 diff, 1 scale, 6 accumulate
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_pp_force launch per stored
+# particle, from an ncu capture on clustered192 (855.4 MB + 121.1 MB over 9,025,370 stored
+# particles); the kernel streams the sorted particles and vp once per launch, so the figure is
+# scaled to a full launch by the stored particle count
+PP_DRAM_BYTES_PER_STORED = (855_393_024 + 121_076_736) / 9_025_370
 
 
 def parse():
@@ -241,7 +246,9 @@ def run_ours(args, rank, world, local_rank):
     roofline = {"kernel": "k_pp_force (PP pair force + kick)", "bound": "fp32", "achieved": achieved,
                 "peak": fp32_peak, "unit": "TFLOP/s", "frac": (achieved / fp32_peak) if achieved else None,
                 "peak_source": "FP32 FMA probe measured in this run (MEASURED_PEAKS.json has no FP32 figure)",
-                "flops_per_launch": int(flops), "pairs_per_launch": int(pairs), "traffic": None}
+                "flops_per_launch": int(flops), "pairs_per_launch": int(pairs),
+                "traffic": float(PP_DRAM_BYTES_PER_STORED * img.n_used),
+                "traffic_source": "ncu DRAM bytes of k_pp_force on clustered192, scaled by stored particles"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
