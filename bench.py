@@ -266,7 +266,8 @@ def run_ours(args, rank, world, local_rank):
                        "softening_fine_cells": L.app, "assignment": "TSC", "variant": "plain (no learned shell)",
                        "layout": L.as_dict(), "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (mesh 512^3 fp32 = 537 MB, particle arrays > 120 MB)"},
-            "stages_ms": {"pm3": pm3_ms, "pp_binning_and_worklist": ppb_ms, "pp_force": ppf_ms},
+            "stages_ms": {"pm3": pm3_ms, "pp_binning_and_worklist": ppb_ms, "pp_force": ppf_ms,
+                          "note": "the PP binning and work list run on a second stream beside PM3"},
             "roofline": roofline, "force_error": truth, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": ck, "cpu_baseline": cpu}
     if rank == 0:

@@ -57,6 +57,9 @@ struct Ctx {
   cudaStream_t copy = nullptr;
   cudaEvent_t vp_ready = nullptr;
   bool vp_pending = false;
+  // The PP binning and work list run on `side`, beside PM3 on the compute stream.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   Buf xp, rhoc, idx, vp, cell_base;
   Buf tiles, count, cell_start, scan_tmp, spos, spill, spill_rank, counters, items, range_loc;
   Buf rho, rhok, force, jobs, out;
@@ -67,7 +70,8 @@ struct Ctx {
   std::vector<HostGreen> hgreens;
   std::vector<Plan> plans;
   // Stage events of the last kRing timed calls.  Per call: 0 start, 1 after PM3,
-  // 2 PP start, 4 after the PP force kernel, 5 end, 6 after the PP work list.
+  // 2 PP start, 3 PP force kernel start, 4 after the PP force kernel, 5 end, 6 after the PP
+  // work list.  The PP binning and work list (2 to 6) may run beside PM3 (0 to 1).
   static constexpr int kRing = 256;
   cudaEvent_t ring[kRing][7] = {};
   bool ring_pm3[kRing] = {}, ring_pp[kRing] = {};
@@ -164,6 +168,9 @@ static int ensure_device() {
   CU(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
   CU(cudaStreamCreateWithFlags(&g.copy, cudaStreamNonBlocking));
   CU(cudaEventCreateWithFlags(&g.vp_ready, cudaEventDisableTiming));
+  CU(cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking));
+  CU(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
   CU(cudaMallocHost(&g.h_out, sizeof(float) * 8));
   for (auto &slot : g.ring)
     for (auto &e : slot) CU(cudaEventCreate(&e));
@@ -202,14 +209,14 @@ static int stage_end() {
 
 // upload a small host table through the pinned staging area (offset in bytes)
 template <class T>
-static int upload(Buf &dst, const T *src, size_t count, size_t &stage_off) {
+static int upload(Buf &dst, const T *src, size_t count, size_t &stage_off, cudaStream_t st = nullptr) {
   const size_t bytes = sizeof(T) * count;
   CK(grow(dst, bytes > 0 ? bytes : 16));
   if (!bytes) return CUBE_OK;
   stage_off = (stage_off + 255) & ~(size_t)255;
   if (stage_off + bytes > g.h_stage_cap) return fail(CUBE_ERR_CAPACITY);
   memcpy((char *)g.h_stage + stage_off, src, bytes);
-  CU(cudaMemcpyAsync(dst.p, (char *)g.h_stage + stage_off, bytes, cudaMemcpyHostToDevice, g.stream));
+  CU(cudaMemcpyAsync(dst.p, (char *)g.h_stage + stage_off, bytes, cudaMemcpyHostToDevice, st ? st : g.stream));
   stage_off += bytes;
   return CUBE_OK;
 }
@@ -430,6 +437,7 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     return CUBE_OK;
   }
   // buffered subtile meshes grouped by level (pm3_fft_cuda.cu:553-591)
+  const size_t soff0 = soff;
   for (int lev = 2; lev <= 6; lev++) {
     std::vector<int> locs;
     for (int q = 0; q < L.ns3; q++)
@@ -518,19 +526,19 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       CU(cudaGetLastError());
       // the job table is reused by the next batch
       CU(cudaStreamSynchronize(g.stream));
-      soff = 0;
+      soff = soff0;  // tables uploaded before PM3 (the PP grid) keep their staging slots
     }
   }
   return CUBE_OK;
 }
 
-// PP stage: binning, work list, force kernel.  With `pairs` non-null the force
-// kernel only counts accepted pairs and leaves vp untouched.
-static int run_pp(const Meta &m, const Dev &d, float mass, float kick, size_t &soff,
-                  unsigned long long *pairs = nullptr) {
+// PP binning and work list on stream `st`; fills the arguments of the force kernel.  With
+// `pairs` non-null the force kernel will only count accepted pairs and leave vp untouched.
+static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size_t &soff, PPArgs &p,
+                       cudaStream_t st, unsigned long long *pairs) {
   const Lay &L = g.L;
-  CK(upload(g.tiles, m.tiles.data(), m.tiles.size(), soff));
-  CK(upload(g.range_loc, m.range_loc.data(), m.range_loc.size(), soff));
+  CK(upload(g.tiles, m.tiles.data(), m.tiles.size(), soff, st));
+  CK(upload(g.range_loc, m.range_loc.data(), m.range_loc.size(), soff, st));
   CK(grow(g.count, sizeof(int32_t) * (size_t)m.ncells));
   CK(grow(g.cell_start, sizeof(int32_t) * (size_t)(m.ncells + 1)));
   CK(grow(g.scan_tmp, sizeof(int32_t) * scan_tmp_elems(m.ncells)));
@@ -560,13 +568,13 @@ static int run_pp(const Meta &m, const Dev &d, float mass, float kick, size_t &s
   b.spill_cap = spill_cap;
   b.scan_tmp = (int32_t *)g.scan_tmp.p;
   b.err = ctr + 2;
-  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][2], g.stream));
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][2], st));
   if (bin_smem_bytes(m.max_rcp) > 200 * 1024) return fail(CUBE_ERR_INVALID);  // rcp^3 histograms per warp
   b.spatial = 1;
-  launch_pp_binning(b, g.stream);
+  launch_pp_binning(b, st);
   g.launches += 7;  // count, spill sort, 3 scan passes, scatter, spill placement
   CU(cudaGetLastError());
-  PPArgs p{};
+  p = PPArgs{};
   p.L = &g.L;
   p.d_tiles = (const TilePP *)g.tiles.p;
   p.h_tiles = m.tiles.data();
@@ -586,15 +594,30 @@ static int run_pp(const Meta &m, const Dev &d, float mass, float kick, size_t &s
   p.err = ctr + 2;
   p.num_sms = g.num_sms;
   p.pairs = pairs;
-  launch_pp_items(p, g.stream);
+  launch_pp_items(p, st);
+  g.launches += 2;
   CU(cudaGetLastError());
-  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][6], g.stream));
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][6], st));
+  return CUBE_OK;
+}
+
+// PP force kernel on the compute stream, after run_pp_prep's work and the vp upload
+static int run_pp_force(const PPArgs &p) {
   CK(wait_vp());
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][3], g.stream));
   launch_pp_force(p, g.stream);
-  g.launches += 3;
+  g.launches += 1;
   CU(cudaGetLastError());
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][4], g.stream));
   return CUBE_OK;
+}
+
+// PP stage on the compute stream alone
+static int run_pp(const Meta &m, const Dev &d, float mass, float kick, size_t &soff,
+                  unsigned long long *pairs = nullptr) {
+  PPArgs p{};
+  CK(run_pp_prep(m, d, mass, kick, soff, p, g.stream, pairs));
+  return run_pp_force(p);
 }
 
 static bool configured() { return g.configured; }
@@ -625,9 +648,22 @@ static int run_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *ra
   launch_cell_table(g.L, d.rhoc, d.idx, (int64_t *)g.cell_base.p, g.stream);
   g.launches += 1;
   CU(cudaGetLastError());
-  if (do_pm3) CK(run_pm3(m, ires, ratio_sf, gk, d, mass, kick, !do_pp, soff));
-  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][1], g.stream));
-  if (do_pp) CK(run_pp(m, d, mass, kick, soff));
+  if (do_pm3 && do_pp) {
+    // the PP binning needs only xp and the cell table: it runs beside PM3
+    PPArgs pa{};
+    CU(cudaEventRecord(g.ev_fork, g.stream));
+    CU(cudaStreamWaitEvent(g.side, g.ev_fork, 0));
+    CK(run_pp_prep(m, d, mass, kick, soff, pa, g.side, nullptr));
+    CU(cudaEventRecord(g.ev_join, g.side));
+    CK(run_pm3(m, ires, ratio_sf, gk, d, mass, kick, false, soff));
+    if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][1], g.stream));
+    CU(cudaStreamWaitEvent(g.stream, g.ev_join, 0));
+    CK(run_pp_force(pa));
+  } else {
+    if (do_pm3) CK(run_pm3(m, ires, ratio_sf, gk, d, mass, kick, !do_pp, soff));
+    if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][1], g.stream));
+    if (do_pp) CK(run_pp(m, d, mass, kick, soff));
+  }
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][5], g.stream));
   CK(stage_end());
   // error word next to the outputs
@@ -643,7 +679,7 @@ static int finish_times(bool do_pm3, bool do_pp) {
   if (do_pm3) CU(cudaEventElapsedTime(&a, g.ring[g.ring_cur][0], g.ring[g.ring_cur][1]));
   if (do_pp) {
     CU(cudaEventElapsedTime(&b, g.ring[g.ring_cur][2], g.ring[g.ring_cur][6]));
-    CU(cudaEventElapsedTime(&c, g.ring[g.ring_cur][6], g.ring[g.ring_cur][4]));
+    CU(cudaEventElapsedTime(&c, g.ring[g.ring_cur][3], g.ring[g.ring_cur][4]));
   }
   CU(cudaEventElapsedTime(&t, g.ring[g.ring_cur][0], g.ring[g.ring_cur][5]));
   g.stage_ms[0] = a;
@@ -705,6 +741,7 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   const int wst = wait_vp();  // also on a failed or vp-free run: the D2H below must follow the upload
   if (st != CUBE_OK || wst != CUBE_OK) {
     cudaStreamSynchronize(g.copy);
+    cudaStreamSynchronize(g.side);
     cudaStreamSynchronize(g.stream);
     return st != CUBE_OK ? st : wst;
   }
@@ -1119,7 +1156,7 @@ int cube_timing_read(float *ms, int32_t max_calls, int32_t *n_calls) {
     if (g.ring_pm3[s]) CU(cudaEventElapsedTime(&a, e[0], e[1]));
     if (g.ring_pp[s]) {
       CU(cudaEventElapsedTime(&b, e[2], e[6]));
-      CU(cudaEventElapsedTime(&c, e[6], e[4]));
+      CU(cudaEventElapsedTime(&c, e[3], e[4]));
     }
     CU(cudaEventElapsedTime(&t, e[0], e[5]));
     ms[4 * q] = a;

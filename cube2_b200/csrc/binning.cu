@@ -53,6 +53,7 @@ struct BinK {
   int max_rcp3;
   int hist_words;  // shared ints per warp
   int spatial;     // order inside a PP cell by Morton sub-cell (rcp must divide 8)
+  int fast;        // every tile-local coarse coordinate lies in [-128, 127]: exact float decode
   const TilePP *tiles;
   const int16_t *xp;
   const int32_t *rhoc;
@@ -81,6 +82,12 @@ __device__ __forceinline__ int spill_count_of(const Spill *sp, int n, int64_t g)
     if (sp[m].gkey <= g) lo = m + 1; else hi = m;
   }
   return lo - a;
+}
+
+// decode_pos rounded to float, computed in float: exact (and so equal to the double path) when
+// |c| <= 127, since c needs at most 7 integer bits and (u + 0.5) / 2^16 needs 17 fraction bits
+__device__ __forceinline__ float decode_pos_f(int c, int16_t xp) {
+  return (float)c + ((float)(uint16_t)xp + 0.5f) * (1.0f / 65536.0f);
 }
 
 // Morton interleave of up to 2 bits per axis
@@ -121,9 +128,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
                       int64_t &gkey) {
     const int16_t *q = p.xp + 3 * (base + l);
     // pp_force_kernel.c:213-218: (float)((i-ncb) + ((int16)(xp+ishift)+rshift)*x_resolution)
-    x = __double2float_rn(decode_pos(lx, q[0]));
-    y = __double2float_rn(decode_pos(ly, q[1]));
-    z = __double2float_rn(decode_pos(lz, q[2]));
+    if (p.fast) {
+      x = decode_pos_f(lx, q[0]);
+      y = decode_pos_f(ly, q[1]);
+      z = decode_pos_f(lz, q[2]);
+    } else {
+      x = __double2float_rn(decode_pos(lx, q[0]));
+      y = __double2float_rn(decode_pos(ly, q[1]));
+      z = __double2float_rn(decode_pos(lz, q[2]));
+    }
     // pp_force_kernel.c:226-228: floor(rcp * (x - utile_shift*ntt)) + rcp, float product
     int kx = (int)floorf(__fmul_rn((float)rcp, x)) + rcp;
     int ky = (int)floorf(__fmul_rn((float)rcp, y)) + rcp;
@@ -144,7 +157,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
       const int fx = min(max((int)floorf(__fmul_rn(8.f, x)) - 8 * lx, 0), 7);
       const int fy = min(max((int)floorf(__fmul_rn(8.f, y)) - 8 * ly, 0), 7);
       const int fz = min(max((int)floorf(__fmul_rn(8.f, z)) - 8 * lz, 0), 7);
-      bin = b * s3 + morton2(fx % fs, fy % fs, fz % fs);
+      bin = b * s3 + morton2(fx & (fs - 1), fy & (fs - 1), fz & (fs - 1));  // fs is 2 or 4
     }
   };
 
@@ -404,6 +417,7 @@ void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
   p.R3 = (int64_t)p.R * p.R * p.R;
   p.max_rcp3 = a.max_rcp * a.max_rcp * a.max_rcp;
   p.spatial = a.spatial;
+  p.fast = L.nt + 1 <= 127;  // coarse coordinates -1 .. nt
   // histogram words per warp: rcp^3 PP sub-cells, at least 2 x 512 bins for the spatial order
   p.hist_words = p.max_rcp3 < 1024 ? 1024 : p.max_rcp3;
   p.tiles = a.d_tiles;

@@ -152,46 +152,85 @@ __device__ __forceinline__ bool in_phys(const PM3K &p, int64_t x, int64_t y, int
          z >= p.fphys_lo && z < p.fphys_lo + p.fphys_n;
 }
 
-// Force from the potential on the periodic mesh, four consecutive x points per thread
-// (n % 4 == 0): 11 float4 loads (x-4..x+7 in the row, rows y+-1, y+-2, planes z+-1, z+-2) and
-// 3 float4 stores into the three force arrays (an interleaved (fx, fy, fz, 0) layout measured
-// twice as slow in the gather); |F|^2 of the physical points is reduced into out[0].
-__global__ void k_force_v4(PM3K p) {
+// Force from the potential on the periodic mesh (n % 4 == 0).  A block owns 32 float4 columns
+// (128 x points) of kFzRows rows and marches through kFzChunk planes: each thread keeps the
+// five planes z-2 .. z+2 of its own column in registers and loads one new float4 per plane;
+// x neighbours come from the adjacent lanes (the edge lanes load theirs), y neighbours from a
+// shared tile of the block's rows plus two halo rows on each side.  Each potential value is
+// thus read about once from DRAM.  Stores go to the three force arrays (an interleaved
+// (fx, fy, fz, 0) layout measured twice as slow in the gather); |F|^2 of the physical points is
+// reduced into out[0].
+constexpr int kFzRows = 8;
+constexpr int kFzChunk = 32;
+
+__device__ __forceinline__ float4 shfl_f4(float4 v, int delta, bool up) {
+  float4 r;
+  r.x = up ? __shfl_up_sync(0xffffffffu, v.x, delta) : __shfl_down_sync(0xffffffffu, v.x, delta);
+  r.y = up ? __shfl_up_sync(0xffffffffu, v.y, delta) : __shfl_down_sync(0xffffffffu, v.y, delta);
+  r.z = up ? __shfl_up_sync(0xffffffffu, v.z, delta) : __shfl_down_sync(0xffffffffu, v.z, delta);
+  r.w = up ? __shfl_up_sync(0xffffffffu, v.w, delta) : __shfl_down_sync(0xffffffffu, v.w, delta);
+  return r;
+}
+
+__global__ void __launch_bounds__(kFzRows * 32) k_force_zm(PM3K p) {
+  __shared__ float4 tile[kFzRows + 4][32];
   const FDW w;
+  const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
   const int64_t n = p.n, n4 = p.n / 4;
-  const int64_t per_slot = n4 * n * n;
-  const int64_t total = per_slot * p.nslots;
+  const int nzc = (p.n + kFzChunk - 1) / kFzChunk;
+  const int64_t slot = blockIdx.z / nzc;
+  const int64_t z0 = (int64_t)(blockIdx.z % nzc) * kFzChunk, z1 = min(z0 + kFzChunk, n);
+  const int64_t x4 = (int64_t)blockIdx.x * 32 + lane, y0 = (int64_t)blockIdx.y * kFzRows, y = y0 + wy;
+  const bool act = x4 < n4 && y < n;
+  // idle lanes read a valid column; rows past n march the periodic image row, which the
+  // rows below them read as their y neighbours
+  const int64_t xs = min(x4, n4 - 1), ys = wrap_near(y, n);
+  const float4 *phi = reinterpret_cast<const float4 *>(p.rho + slot * p.n3);
+  auto at = [&](int64_t xx4, int64_t yy, int64_t zz) {
+    return __ldg(phi + (wrap_near(zz, n) * n + wrap_near(yy, n)) * n4 + wrap_near(xx4, n4));
+  };
+  float4 cm2 = at(xs, ys, z0 - 2), cm1 = at(xs, ys, z0 - 1), c0 = at(xs, ys, z0), cp1 = at(xs, ys, z0 + 1);
+  float4 *F = reinterpret_cast<float4 *>(p.force + slot * 3 * p.n3) + ys * n4 + xs;
+  const int64_t plane4 = n * n4;
   float m = 0.f;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t slot = e / per_slot, r = e - slot * per_slot;
-    const int64_t x4 = r % n4, y = (r / n4) % n, z = r / (n4 * n);
-    const float4 *phi = reinterpret_cast<const float4 *>(p.rho + slot * p.n3);
-    auto row = [&](int64_t yy, int64_t zz) { return phi + (wrap_near(zz, n) * n + wrap_near(yy, n)) * n4; };
-    const float4 *c = row(y, z);
-    const float4 l = __ldg(c + (x4 + n4 - 1) % n4), o = __ldg(c + x4), rr = __ldg(c + (x4 + 1) % n4);
-    const float4 ym2 = __ldg(row(y - 2, z) + x4), ym1 = __ldg(row(y - 1, z) + x4), yp1 = __ldg(row(y + 1, z) + x4),
-                 yp2 = __ldg(row(y + 2, z) + x4);
-    const float4 zm2 = __ldg(row(y, z - 2) + x4), zm1 = __ldg(row(y, z - 1) + x4), zp1 = __ldg(row(y, z + 1) + x4),
-                 zp2 = __ldg(row(y, z + 2) + x4);
-    const float4 fx = make_float4(w(l.z, l.w, o.y, o.z), w(l.w, o.x, o.z, o.w), w(o.x, o.y, o.w, rr.x),
-                                  w(o.y, o.z, rr.x, rr.y));
+  for (int64_t z = z0; z < z1; z++) {
+    const float4 cp2 = at(xs, ys, z + 2);
+    tile[wy + 2][lane] = c0;
+    if (wy < 4) {  // halo rows y0-2, y0-1 (warps 0, 1) and y0+kFzRows, y0+kFzRows+1 (warps 2, 3)
+      const int64_t hy = wy < 2 ? y0 - 2 + wy : y0 + kFzRows + wy - 2;
+      tile[wy < 2 ? wy : kFzRows + wy][lane] = at(xs, hy, z);
+    }
+    float4 l = shfl_f4(c0, 1, true), r = shfl_f4(c0, 1, false);
+    if (lane == 0) l = at(xs - 1, ys, z);
+    if (lane == 31 || x4 + 1 >= n4) r = at(xs + 1, ys, z);
+    __syncthreads();
+    const float4 ym2 = tile[wy][lane], ym1 = tile[wy + 1][lane], yp1 = tile[wy + 3][lane],
+                 yp2 = tile[wy + 4][lane];
+    const float4 fx = make_float4(w(l.z, l.w, c0.y, c0.z), w(l.w, c0.x, c0.z, c0.w), w(c0.x, c0.y, c0.w, r.x),
+                                  w(c0.y, c0.z, r.x, r.y));
     const float4 fy = make_float4(w(ym2.x, ym1.x, yp1.x, yp2.x), w(ym2.y, ym1.y, yp1.y, yp2.y),
                                   w(ym2.z, ym1.z, yp1.z, yp2.z), w(ym2.w, ym1.w, yp1.w, yp2.w));
-    const float4 fz = make_float4(w(zm2.x, zm1.x, zp1.x, zp2.x), w(zm2.y, zm1.y, zp1.y, zp2.y),
-                                  w(zm2.z, zm1.z, zp1.z, zp2.z), w(zm2.w, zm1.w, zp1.w, zp2.w));
-    float4 *F = reinterpret_cast<float4 *>(p.force + slot * 3 * p.n3) + (z * n + y) * n4 + x4;
-    F[0] = fx;
-    F[n * n * n4] = fy;
-    F[2 * n * n * n4] = fz;
-    const int64_t x = 4 * x4;
-    if (in_phys(p, x, y, z)) m = fmaxf(m, fx.x * fx.x + fy.x * fy.x + fz.x * fz.x);
-    if (in_phys(p, x + 1, y, z)) m = fmaxf(m, fx.y * fx.y + fy.y * fy.y + fz.y * fz.y);
-    if (in_phys(p, x + 2, y, z)) m = fmaxf(m, fx.z * fx.z + fy.z * fy.z + fz.z * fz.z);
-    if (in_phys(p, x + 3, y, z)) m = fmaxf(m, fx.w * fx.w + fy.w * fy.w + fz.w * fz.w);
+    const float4 fz = make_float4(w(cm2.x, cm1.x, cp1.x, cp2.x), w(cm2.y, cm1.y, cp1.y, cp2.y),
+                                  w(cm2.z, cm1.z, cp1.z, cp2.z), w(cm2.w, cm1.w, cp1.w, cp2.w));
+    if (act) {
+      float4 *Fz = F + z * plane4;
+      Fz[0] = fx;
+      Fz[n * plane4] = fy;
+      Fz[2 * n * plane4] = fz;
+      const int64_t x = 4 * x4;
+      if (in_phys(p, x, y, z)) m = fmaxf(m, fx.x * fx.x + fy.x * fy.x + fz.x * fz.x);
+      if (in_phys(p, x + 1, y, z)) m = fmaxf(m, fx.y * fx.y + fy.y * fy.y + fz.y * fz.y);
+      if (in_phys(p, x + 2, y, z)) m = fmaxf(m, fx.z * fx.z + fy.z * fy.z + fz.z * fz.z);
+      if (in_phys(p, x + 3, y, z)) m = fmaxf(m, fx.w * fx.w + fy.w * fy.w + fz.w * fz.w);
+    }
+    __syncthreads();  // the next plane overwrites the tile
+    cm2 = cm1;
+    cm1 = c0;
+    c0 = cp1;
+    cp1 = cp2;
   }
   m = warp_max(m);
-  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&p.out[0], m);
+  if (lane == 0) atomic_max_nonneg(&p.out[0], m);
 }
 
 // the same, one point per thread, for any n
@@ -334,9 +373,12 @@ void launch_pm3_kspace(const PM3Args &a, cudaStream_t s) {
 
 void launch_pm3_force(const PM3Args &a, cudaStream_t s) {
   PM3K p = make_k(a);
-  if (a.n % 4 == 0)
-    k_force_v4<<<148 * 8, 256, 0, s>>>(p);
-  else
+  if (a.n % 4 == 0) {
+    const int nzc = (a.n + kFzChunk - 1) / kFzChunk;
+    const dim3 grid((unsigned)((a.n / 4 + 31) / 32), (unsigned)((a.n + kFzRows - 1) / kFzRows),
+                    (unsigned)(nzc * a.nslots));
+    k_force_zm<<<grid, kFzRows * 32, 0, s>>>(p);
+  } else
     k_force<<<148 * 8, 256, 0, s>>>(p);
 }
 

@@ -189,7 +189,8 @@ int cube_force_truth_fp64(const double *pos, int64_t n, double box, double app, 
 
 /* Device time in ms of the last host-API kick's stages: [0] PM3 total,
  * [1] PP binning + work list, [2] PP force kernel, [3] whole device pipeline
- * (filled when timing is enabled). */
+ * (filled when timing is enabled).  In a kick with both parts the PP binning and
+ * work list run beside PM3, so [0] + [1] + [2] can exceed [3]. */
 int cube_stage_times(float ms[4]);
 int cube_enable_timing(int on);
 /* Stage times of every timed call since the previous read (oldest first, at
