@@ -60,8 +60,12 @@ struct Ctx {
   // The PP binning and work list run on `side`, beside PM3 on the compute stream.
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  static constexpr int kMaxTileEvents = 64;
+  cudaEvent_t ev_tile[kMaxTileEvents] = {};  // per-tile PP force done (host kicks)
+  cudaEvent_t ev_copied = nullptr;           // last per-tile vp copy enqueued
+  bool vp_copied = false;                    // this host kick's vp is already on its way back
   Buf xp, rhoc, idx, vp, cell_base;
-  Buf tiles, count, cell_start, scan_tmp, spos, spill, spill_rank, counters, items, range_loc;
+  Buf tiles, count, cell_start, scan_tmp, spos, spill, spill_rank, counters, items, range_loc, sched;
   Buf rho, rhok, force, jobs, out;
   void *h_stage = nullptr;  // pinned staging for small tables
   size_t h_stage_cap = 0;
@@ -171,6 +175,8 @@ static int ensure_device() {
   CU(cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking));
   CU(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
+  for (auto &e : g.ev_tile) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&g.ev_copied, cudaEventDisableTiming));
   CU(cudaMallocHost(&g.h_out, sizeof(float) * 8));
   for (auto &slot : g.ring)
     for (auto &e : slot) CU(cudaEventCreate(&e));
@@ -330,6 +336,10 @@ struct Dev {
   const int64_t *idx;
   float *vp;
   int64_t n_used;
+  // host kicks only: the caller's vp and spine; each tile's vp is copied back as soon as
+  // that tile's PP force kernel has finished
+  float *h_vp = nullptr;
+  const int64_t *h_idx = nullptr;
 };
 
 static int get_green_periodic(int n, int rsf, float **out) {
@@ -550,7 +560,8 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   for (auto &t : m.tiles) interior += (int64_t)L.nt * t.rcp * L.nt * t.rcp * L.nt * t.rcp;
   const int64_t item_cap = interior + d.n_used / kPPChunk + 16;
   CK(grow(g.items, sizeof(int4) * (size_t)item_cap));
-  int32_t *ctr = (int32_t *)g.counters.p;  // [0] spill_n [1] head [2] err [64..128) buckets
+  CK(grow(g.sched, sizeof(int32_t) * sched_ints(L.ntile)));
+  int32_t *ctr = (int32_t *)g.counters.p;  // [0] spill_n [2] err
   BinArgs b{};
   b.L = &g.L;
   b.d_tiles = (const TilePP *)g.tiles.p;
@@ -583,8 +594,7 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   p.spos = (const float4 *)g.spos.p;
   p.range_loc = (const float *)g.range_loc.p;
   p.items = (int4 *)g.items.p;
-  p.bucket = ctr + 64;
-  p.head = ctr + 1;
+  p.sched = (int32_t *)g.sched.p;
   p.item_cap = item_cap;
   p.vp = d.vp;
   p.mass2 = mass * mass;
@@ -609,6 +619,41 @@ static int run_pp_force(const PPArgs &p) {
   g.launches += 1;
   CU(cudaGetLastError());
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][4], g.stream));
+  return CUBE_OK;
+}
+
+// PP force kernel tile by tile for a host kick: launches alternate between the compute and
+// the side stream (one launch's tail overlaps the next one's start), and each tile's vp range
+// (its stored particles, a contiguous run of the spine) goes to the host on the copy stream as
+// soon as its launch is done.  The compute stream ends after the last copy.
+static int run_pp_force_tiles(const PPArgs &p, const Dev &d) {
+  const Lay &L = g.L;
+  CK(wait_vp());
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][3], g.stream));
+  CU(cudaEventRecord(g.ev_fork, g.stream));
+  CU(cudaStreamWaitEvent(g.side, g.ev_fork, 0));
+  const int64_t rows = (int64_t)L.nte * L.nte;
+  for (int t = 0; t < L.ntile; t++) {
+    cudaStream_t st = (t & 1) ? g.side : g.stream;
+    launch_pp_force(p, st, t, t + 1);
+    g.launches += 1;
+    CU(cudaGetLastError());
+    CU(cudaEventRecord(g.ev_tile[t], st));
+  }
+  // copies after all launches: a copy into pageable host memory returns only when done
+  for (int t = 0; t < L.ntile; t++) {
+    const int64_t lo = t ? d.h_idx[t * rows - 1] : 0, hi = d.h_idx[(t + 1) * rows - 1];
+    if (hi <= lo) continue;
+    CU(cudaStreamWaitEvent(g.copy, g.ev_tile[t], 0));
+    CU(cudaMemcpyAsync(d.h_vp + 3 * lo, d.vp + 3 * lo, sizeof(float) * 3 * (hi - lo), cudaMemcpyDeviceToHost,
+                       g.copy));
+  }
+  g.vp_copied = true;
+  CU(cudaEventRecord(g.ev_join, g.side));
+  CU(cudaStreamWaitEvent(g.stream, g.ev_join, 0));
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][4], g.stream));
+  CU(cudaEventRecord(g.ev_copied, g.copy));
+  CU(cudaStreamWaitEvent(g.stream, g.ev_copied, 0));
   return CUBE_OK;
 }
 
@@ -658,7 +703,10 @@ static int run_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *ra
     CK(run_pm3(m, ires, ratio_sf, gk, d, mass, kick, false, soff));
     if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][1], g.stream));
     CU(cudaStreamWaitEvent(g.stream, g.ev_join, 0));
-    CK(run_pp_force(pa));
+    if (d.h_vp && g.L.ntile <= Ctx::kMaxTileEvents)
+      CK(run_pp_force_tiles(pa, d));
+    else
+      CK(run_pp_force(pa));
   } else {
     if (do_pm3) CK(run_pm3(m, ires, ratio_sf, gk, d, mass, kick, !do_pp, soff));
     if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][1], g.stream));
@@ -737,6 +785,9 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
     g.vp_pending = true;
   }
   Dev d{(const int16_t *)g.xp.p, (const int32_t *)g.rhoc.p, (const int64_t *)g.idx.p, (float *)g.vp.p, n_used};
+  d.h_vp = vp;
+  d.h_idx = idx_b_r;
+  g.vp_copied = false;
   const int st = run_kick(ires, ixyz3, ratio_sf, apm3, gk, d, mass, a_mid, dt, do_pm3, do_pp, m);
   const int wst = wait_vp();  // also on a failed or vp-free run: the D2H below must follow the upload
   if (st != CUBE_OK || wst != CUBE_OK) {
@@ -745,7 +796,8 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
     cudaStreamSynchronize(g.stream);
     return st != CUBE_OK ? st : wst;
   }
-  if (n_used) CU(cudaMemcpyAsync(vp, g.vp.p, sizeof(float) * 3 * n_used, cudaMemcpyDeviceToHost, g.stream));
+  if (n_used && !g.vp_copied)
+    CU(cudaMemcpyAsync(vp, g.vp.p, sizeof(float) * 3 * n_used, cudaMemcpyDeviceToHost, g.stream));
   CU(cudaMemcpyAsync(g.h_out, g.out.p, sizeof(float) * 6, cudaMemcpyDeviceToHost, g.stream));
   CU(cudaStreamSynchronize(g.stream));
   CK(finish_times(do_pm3, do_pp));
@@ -951,7 +1003,7 @@ void c_gpu_velocity_finalize(void) {
   cudaSetDevice(g.device);
   cudaStreamSynchronize(g.stream);
   Buf *bufs[] = {&g.xp, &g.rhoc, &g.idx, &g.vp, &g.cell_base, &g.tiles, &g.count, &g.cell_start, &g.scan_tmp,
-                 &g.spos, &g.spill, &g.spill_rank, &g.counters, &g.items, &g.range_loc, &g.out};
+                 &g.spos, &g.spill, &g.spill_rank, &g.counters, &g.items, &g.range_loc, &g.sched, &g.out};
   for (Buf *b : bufs) release(*b);
 }
 

@@ -112,9 +112,8 @@ struct PPArgs {
   const float4 *spos;
   const float *range_loc;   // [ns3] PP range by subtile location
   int4 *items;              // [item_cap]
-  int32_t *bucket;          // [64]: counts, cursors
-  int32_t *n_items;         // device counter (= total)
-  int32_t *head;            // work-queue head
+  int32_t *sched;           // [sched_ints(ntile)], zeroed by launch_pp_items: bucket counts and
+                            // cursors per tile, tile bases, work-queue heads
   int64_t item_cap;
   float *vp;                // device vp [n_used][3]
   float mass2, kick;
@@ -124,8 +123,11 @@ struct PPArgs {
   int num_sms;
   unsigned long long *pairs;  // non-null: count accepted pairs instead of kicking
 };
+size_t sched_ints(int ntile);
 void launch_pp_items(const PPArgs &a, cudaStream_t s);
-void launch_pp_force(const PPArgs &a, cudaStream_t s);
+// force kernel over the items of tiles [t_lo, t_hi) (t_hi < 0: all tiles); each single tile and
+// the full range have their own queue head, so per-tile launches may run on several streams
+void launch_pp_force(const PPArgs &a, cudaStream_t s, int t_lo = 0, int t_hi = -1);
 
 // PM3
 struct PM3Args {

@@ -44,7 +44,9 @@ constexpr size_t kOffSpillRank = kOffSpill + na_align(sizeof(Spill) * kNaSpill);
 constexpr size_t kOffTiles = kOffSpillRank + na_align(sizeof(int32_t) * kNaSpill);
 constexpr size_t kOffRange = kOffTiles + na_align(sizeof(TilePP) * kNaTiles);
 constexpr size_t kOffCounters = kOffRange + na_align(sizeof(float) * kNaSub);          // int32 [128]
-constexpr size_t kNaBytes = kOffCounters + na_align(sizeof(int32_t) * 128);
+constexpr size_t kNaSchedInts = 2 * 32 * kNaTiles + 2 * (kNaTiles + 1);                 // sched_ints(64)
+constexpr size_t kOffSched = kOffCounters + na_align(sizeof(int32_t) * 128);            // PP schedule
+constexpr size_t kNaBytes = kOffSched + na_align(sizeof(int32_t) * kNaSchedInts);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
 
@@ -100,6 +102,7 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
   if (ncells > kNaCells) return CUBE_ERR_CAPACITY;
   if (interior + n_used / kPPChunk + 16 > (int64_t)kItemCap) return CUBE_ERR_CAPACITY;
   if (bin_smem_bytes(max_rcp) > 200 * 1024) return CUBE_ERR_INVALID;
+  if (sched_ints(L.ntile) > kNaSchedInts) return CUBE_ERR_CAPACITY;
 
   // device address of the scratch on the current device (once per device)
   int dev = 0;
@@ -120,7 +123,8 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
   int32_t *spill_rank = (int32_t *)(base + kOffSpillRank);
   TilePP *d_tiles = (TilePP *)(base + kOffTiles);
   float *d_range = (float *)(base + kOffRange);
-  int32_t *ctr = (int32_t *)(base + kOffCounters);  // [0] spill_n [1] head [2] err [64..128) buckets
+  int32_t *ctr = (int32_t *)(base + kOffCounters);  // [0] spill_n [2] err
+  int32_t *sched = (int32_t *)(base + kOffSched);    // zeroed by launch_pp_items
 
   // the scratch keeps the previous call's contents: reset what must start at zero
   if (cudaMemsetAsync(ctr, 0, sizeof(int32_t) * 128, s) != cudaSuccess) return CUBE_ERR_CUDA;
@@ -161,8 +165,7 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
   p.spos = spos;
   p.range_loc = d_range;
   p.items = items;
-  p.bucket = ctr + 64;
-  p.head = ctr + 1;
+  p.sched = sched;
   p.item_cap = (int64_t)kItemCap;
   p.vp = d_vp;
   p.mass2 = mass * mass;

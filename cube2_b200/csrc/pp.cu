@@ -150,10 +150,10 @@ struct PPK {
   const int32_t *cs;
   const float4 *spos;
   const float *range_loc;
-  int4 *items;      // (global cell, chunk, tile, PP range bits)
-  int32_t *bucket;  // [0,32) counts, [32,64) cursors
-  int32_t *head;
+  int4 *items;      // (global cell, chunk, tile, PP range bits), tile-major, heaviest bucket first
+  int32_t *sched;   // schedule words, layout in sched_ints()
   int64_t item_cap;
+  int t_lo, t_hi;   // tiles of this force launch; its queue head is sched_head(t_lo, t_hi)
   float *vp;
   float mass2, kick, app;
   float *out;
@@ -179,6 +179,15 @@ __device__ __forceinline__ bool row_needed(int dy, int dz, float h, float rc2) {
   return ay * ay + az * az < rc2;
 }
 
+// Schedule words (int32), for ntile tiles: [0, 32 ntile) item counts per (tile, bucket), turned
+// into the first item slot of each (tile, bucket) by k_pp_offsets; [32 ntile, 64 ntile) cursors;
+// then ntile + 1 tile bases (first item of each tile, and the total); then ntile + 1 queue
+// heads (one per single-tile launch, one for a launch over all tiles).
+__host__ __device__ inline int64_t sched_base(int ntile) { return 2 * (int64_t)kBuckets * ntile; }
+__host__ __device__ inline int64_t sched_head(int ntile, int t_lo, int t_hi) {
+  return sched_base(ntile) + ntile + 1 + (t_hi - t_lo == 1 ? t_lo : ntile);
+}
+
 // cost bucket of a chunk with ni i-particles and nj candidates, heavy = high index:
 // the warp walks the candidates in floor(32/ni) lane groups
 __device__ __forceinline__ int cost_bucket(int ni, int64_t nj) {
@@ -188,23 +197,18 @@ __device__ __forceinline__ int cost_bucket(int ni, int64_t nj) {
   return b > kBuckets - 1 ? kBuckets - 1 : b;
 }
 
-// Enumerate the chunks of the interior PP cells; pass 0 counts items per bucket,
-// pass 1 writes them, heaviest bucket first.  A cell's full chunks share one
-// bucket and its remainder chunk has another, so a thread reserves its slots
-// with at most two shared-memory atomics.
+// Enumerate the chunks of the interior PP cells; pass 0 counts items per (tile, bucket),
+// pass 1 writes them tile by tile, heaviest bucket first inside a tile.  A cell's full chunks
+// share one bucket and its remainder chunk has another, so a thread reserves its slots with at
+// most two shared-memory atomics.
 template <int PASS>
 __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
-  __shared__ int sc[kBuckets], sbase[kBuckets], soff[kBuckets];
-  if (threadIdx.x < kBuckets) sc[threadIdx.x] = 0;
-  if (PASS == 1 && threadIdx.x == 0) {
-    int acc = 0;
-    for (int b = kBuckets - 1; b >= 0; --b) {
-      soff[b] = acc;
-      acc += p.bucket[b];
-    }
-  }
-  __syncthreads();
+  __shared__ int sc[kBuckets], sbase[kBuckets];
   const int t = blockIdx.y;
+  int32_t *cnt = p.sched + (int64_t)kBuckets * t;                     // counts, then first slots
+  int32_t *cur = p.sched + (int64_t)kBuckets * (p.ntile + t);         // cursors
+  if (threadIdx.x < kBuckets) sc[threadIdx.x] = 0;
+  __syncthreads();
   const TilePP tp = p.tiles[t];
   const int rcp = tp.rcp, S = tp.S, npg = p.nt * rcp;
   const int64_t ncell = (int64_t)npg * npg * npg;
@@ -241,24 +245,44 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
   if (threadIdx.x < kBuckets) {
     const int n = sc[threadIdx.x];
     if (PASS == 0) {
-      if (n) atomicAdd(&p.bucket[threadIdx.x], n);
+      if (n) atomicAdd(&cnt[threadIdx.x], n);
     } else {
-      sbase[threadIdx.x] = n ? atomicAdd(&p.bucket[kBuckets + threadIdx.x], n) : 0;
+      sbase[threadIdx.x] = cnt[threadIdx.x] + (n ? atomicAdd(&cur[threadIdx.x], n) : 0);
     }
   }
   if (PASS == 1) {
     __syncthreads();
-    const int64_t f0 = (int64_t)soff[bfull] + sbase[bfull] + rfull;
+    const int64_t f0 = (int64_t)sbase[bfull] + rfull;
     for (int k = 0; k < nfull; k++) {
       if (f0 + k < p.item_cap) p.items[f0 + k] = make_int4((int)g, k, t, rcbits);
       else atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
     }
     if (brem >= 0) {
-      const int64_t slot = (int64_t)soff[brem] + sbase[brem] + rrem;
+      const int64_t slot = (int64_t)sbase[brem] + rrem;
       if (slot < p.item_cap) p.items[slot] = make_int4((int)g, nfull, t, rcbits);
       else atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
     }
   }
+}
+
+// Between the two item passes: turn the (tile, bucket) counts into first slots, tiles in
+// order and buckets heaviest first inside a tile, and record the tile bases.  One warp.
+__global__ void k_pp_offsets(int32_t *sched, int ntile) {
+  const int lane = threadIdx.x;
+  int32_t *base = sched + sched_base(ntile);
+  int acc = 0;
+  for (int t = 0; t < ntile; t++) {
+    const int c = sched[kBuckets * t + lane];
+    int incl = c;  // inclusive sum over the heavier buckets b' >= lane
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_down_sync(0xffffffffu, incl, o);
+      if (lane + o < 32) incl += v;
+    }
+    if (lane == 0) base[t] = acc;
+    sched[kBuckets * t + lane] = acc + incl - c;
+    acc += __shfl_sync(0xffffffffu, incl, 0);
+  }
+  if (lane == 0) base[ntile] = acc;
 }
 
 // COUNT = false: forces and kick.  COUNT = true: only count the accepted ordered
@@ -269,19 +293,18 @@ __global__ void __launch_bounds__(kPPThreads, 4) k_pp_force(PPK p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float4 *buf = reinterpret_cast<float4 *>(reinterpret_cast<char *>(pp_smem) + warp * kPPSmemWarp);
   int2 *rows = reinterpret_cast<int2 *>(buf + kJTile + 32);  // (end of the row in the walk, start - walk offset)
-  int total = 0;
-  {
-    int v = lane < kBuckets ? p.bucket[lane] : 0;
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    total = min((int64_t)v, p.item_cap);
-  }
+  // items [first, last) of tiles [t_lo, t_hi), popped through this launch's own queue head
+  const int32_t *tbase = p.sched + sched_base(p.ntile);
+  const int first = tbase[p.t_lo];
+  const int last = (int)min((int64_t)tbase[p.t_hi], p.item_cap);
+  int32_t *head = p.sched + sched_head(p.ntile, p.t_lo, p.t_hi);
   float f2w = 0.f, vm0 = 0.f, vm1 = 0.f, vm2 = 0.f;
   unsigned long long npairs = 0;
   for (;;) {
     int it = 0;
-    if (lane == 0) it = atomicAdd(p.head, 1);
+    if (lane == 0) it = first + atomicAdd(head, 1);
     it = __shfl_sync(0xffffffffu, it, 0);
-    if (it >= total) break;
+    if (it >= last) break;
     const int4 item = p.items[it];
     const int64_t g = (int64_t)(unsigned)item.x;
     const int t = item.z;
@@ -478,9 +501,10 @@ static PPK make_ppk(const PPArgs &a) {
   p.spos = a.spos;
   p.range_loc = a.range_loc;
   p.items = a.items;
-  p.bucket = a.bucket;
-  p.head = a.head;
+  p.sched = a.sched;
   p.item_cap = a.item_cap;
+  p.t_lo = 0;
+  p.t_hi = L.ntile;
   p.vp = a.vp;
   p.mass2 = a.mass2;
   p.kick = a.kick;
@@ -496,11 +520,14 @@ static PPK make_ppk(const PPArgs &a) {
   return p;
 }
 
+size_t sched_ints(int ntile) { return (size_t)sched_base(ntile) + 2 * ((size_t)ntile + 1); }
+
 void launch_pp_items(const PPArgs &a, cudaStream_t s) {
   PPK p = make_ppk(a);
-  cudaMemsetAsync(a.bucket, 0, sizeof(int32_t) * 2 * kBuckets, s);
+  cudaMemsetAsync(a.sched, 0, sizeof(int32_t) * sched_ints(a.L->ntile), s);
   dim3 grid((unsigned)((p.max_cells + 255) / 256), (unsigned)a.L->ntile);
   k_pp_items<0><<<grid, 256, 0, s>>>(p);
+  k_pp_offsets<<<1, 32, 0, s>>>(a.sched, a.L->ntile);
   k_pp_items<1><<<grid, 256, 0, s>>>(p);
 }
 
@@ -518,9 +545,11 @@ static int resident_blocks(const void *fn, int num_sms) {
   return cached[which] * num_sms;
 }
 
-void launch_pp_force(const PPArgs &a, cudaStream_t s) {
+void launch_pp_force(const PPArgs &a, cudaStream_t s, int t_lo, int t_hi) {
   PPK p = make_ppk(a);
-  cudaMemsetAsync(a.head, 0, sizeof(int32_t), s);
+  if (t_hi < 0) t_hi = a.L->ntile;
+  p.t_lo = t_lo;
+  p.t_hi = t_hi;
   if (a.pairs) {
     const void *fn = (const void *)k_pp_force<true>;
     k_pp_force<true><<<resident_blocks(fn, a.num_sms), kPPThreads, kPPSmem, s>>>(p);
