@@ -64,6 +64,18 @@ struct Ctx {
   cudaEvent_t ev_tile[kMaxTileEvents] = {};  // per-tile PP force done (host kicks)
   cudaEvent_t ev_copied = nullptr;           // last per-tile vp copy enqueued
   bool vp_copied = false;                    // this host kick's vp is already on its way back
+  // Host kicks upload xp tile by tile on `copy`; the deposit of a tile waits only for its
+  // own part, everything else that reads xp waits for all of it.
+  cudaEvent_t ev_xp[kMaxTileEvents] = {};
+  bool xp_pending = false;
+  int xp_tiles = 0;
+  // ... and vp tile by tile too: the PM3 gather of a tile waits for its vp, and the PP force
+  // of a tile (on side or side2) waits for that tile's gather (ev_ready) and the binning.
+  cudaEvent_t ev_vp[kMaxTileEvents] = {}, ev_ready[kMaxTileEvents] = {};
+  int vp_tiles = 0;          // > 0: vp was uploaded in this many tile parts
+  bool ready_tiles = false;  // ev_ready[t] recorded by this kick's PM3
+  cudaStream_t side2 = nullptr;
+  cudaEvent_t ev_pm3done = nullptr, ev_join2 = nullptr;
   Buf xp, rhoc, idx, vp, cell_base;
   Buf tiles, count, cell_start, scan_tmp, spos, spill, spill_rank, counters, items, range_loc, sched;
   Buf rho, rhok, force, jobs, out;
@@ -176,6 +188,12 @@ static int ensure_device() {
   CU(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
   for (auto &e : g.ev_tile) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto &e : g.ev_xp) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto &e : g.ev_vp) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto &e : g.ev_ready) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CU(cudaStreamCreateWithFlags(&g.side2, cudaStreamNonBlocking));
+  CU(cudaEventCreateWithFlags(&g.ev_pm3done, cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&g.ev_join2, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&g.ev_copied, cudaEventDisableTiming));
   CU(cudaMallocHost(&g.h_out, sizeof(float) * 8));
   for (auto &slot : g.ring)
@@ -227,10 +245,17 @@ static int upload(Buf &dst, const T *src, size_t count, size_t &stage_off, cudaS
   return CUBE_OK;
 }
 
+// order stream `st` after the pending upload of tile t's xp (t < 0: all of xp)
+static int wait_xp(cudaStream_t st, int t = -1) {
+  if (!g.xp_pending) return CUBE_OK;
+  CU(cudaStreamWaitEvent(st, g.ev_xp[t < 0 ? g.xp_tiles - 1 : t], 0));
+  return CUBE_OK;
+}
+
 // order the compute stream after a pending vp upload
 static int wait_vp() {
   if (!g.vp_pending) return CUBE_OK;
-  CU(cudaStreamWaitEvent(g.stream, g.vp_ready, 0));
+  CU(cudaStreamWaitEvent(g.stream, g.vp_tiles ? g.ev_vp[g.vp_tiles - 1] : g.vp_ready, 0));
   g.vp_pending = false;
   return CUBE_OK;
 }
@@ -435,19 +460,45 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     CK(get_plan(n, 1, CUFFT_R2C, &fw));
     CK(get_plan(n, 1, CUFFT_C2R, &bw));
     CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3, g.stream));
-    launch_pm3_deposit(a, g.stream);
+    if (g.xp_pending) {  // deposit each tile as soon as its particles are on the device
+      PM3Args at = a;
+      at.njobs = 1;
+      for (int t = 0; t < L.ntile; t++) {
+        CK(wait_xp(g.stream, t));
+        at.jobs = (const MeshJob *)g.jobs.p + t;
+        launch_pm3_deposit(at, g.stream);
+      }
+      g.launches += L.ntile - 1;
+    } else {
+      launch_pm3_deposit(a, g.stream);
+    }
     CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
     launch_pm3_kspace(a, g.stream);
     CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)g.rho.p));  // potential
     launch_pm3_force(a, g.stream);
-    CK(wait_vp());
-    launch_pm3_gather(a, g.stream);
+    if (g.vp_pending && g.vp_tiles == L.ntile) {  // gather each tile as soon as its vp is on the device
+      PM3Args at = a;
+      at.njobs = 1;
+      for (int t = 0; t < L.ntile; t++) {
+        CU(cudaStreamWaitEvent(g.stream, g.ev_vp[t], 0));
+        at.jobs = (const MeshJob *)g.jobs.p + t;
+        launch_pm3_gather(at, g.stream);
+        CU(cudaEventRecord(g.ev_ready[t], g.stream));
+      }
+      g.vp_pending = false;
+      g.ready_tiles = true;
+      g.launches += L.ntile - 1;
+    } else {
+      CK(wait_vp());
+      launch_pm3_gather(a, g.stream);
+    }
     g.launches += 4;
     CU(cudaGetLastError());
     return CUBE_OK;
   }
   // buffered subtile meshes grouped by level (pm3_fft_cuda.cu:553-591)
   const size_t soff0 = soff;
+  CK(wait_xp(g.stream));
   for (int lev = 2; lev <= 6; lev++) {
     std::vector<int> locs;
     for (int q = 0; q < L.ns3; q++)
@@ -579,6 +630,7 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   b.spill_cap = spill_cap;
   b.scan_tmp = (int32_t *)g.scan_tmp.p;
   b.err = ctr + 2;
+  CK(wait_xp(st));
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][2], st));
   if (bin_smem_bytes(m.max_rcp) > 200 * 1024) return fail(CUBE_ERR_INVALID);  // rcp^3 histograms per warp
   b.spatial = 1;
@@ -622,19 +674,23 @@ static int run_pp_force(const PPArgs &p) {
   return CUBE_OK;
 }
 
-// PP force kernel tile by tile for a host kick: launches alternate between the compute and
-// the side stream (one launch's tail overlaps the next one's start), and each tile's vp range
-// (its stored particles, a contiguous run of the spine) goes to the host on the copy stream as
-// soon as its launch is done.  The compute stream ends after the last copy.
+// PP force kernel tile by tile for a host kick.  The launches alternate between the side
+// streams (one launch's tail overlaps the next one's start); a tile's launch waits for the
+// binning and for that tile's PM3 gather, and its vp range (its stored particles, a contiguous
+// run of the spine) goes to the host on the copy stream as soon as the launch is done.  The
+// compute stream ends after the last copy.
 static int run_pp_force_tiles(const PPArgs &p, const Dev &d) {
   const Lay &L = g.L;
-  CK(wait_vp());
-  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][3], g.stream));
-  CU(cudaEventRecord(g.ev_fork, g.stream));
-  CU(cudaStreamWaitEvent(g.side, g.ev_fork, 0));
+  if (!g.ready_tiles) {  // PM3 gathered all tiles at once
+    CK(wait_vp());
+    CU(cudaEventRecord(g.ev_pm3done, g.stream));
+  }
+  CU(cudaStreamWaitEvent(g.side2, g.ev_join, 0));  // binning (on side) done
+  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][3], g.side));
   const int64_t rows = (int64_t)L.nte * L.nte;
   for (int t = 0; t < L.ntile; t++) {
-    cudaStream_t st = (t & 1) ? g.side : g.stream;
+    cudaStream_t st = (t & 1) ? g.side2 : g.side;
+    CU(cudaStreamWaitEvent(st, g.ready_tiles ? g.ev_ready[t] : g.ev_pm3done, 0));
     launch_pp_force(p, st, t, t + 1);
     g.launches += 1;
     CU(cudaGetLastError());
@@ -650,7 +706,9 @@ static int run_pp_force_tiles(const PPArgs &p, const Dev &d) {
   }
   g.vp_copied = true;
   CU(cudaEventRecord(g.ev_join, g.side));
+  CU(cudaEventRecord(g.ev_join2, g.side2));
   CU(cudaStreamWaitEvent(g.stream, g.ev_join, 0));
+  CU(cudaStreamWaitEvent(g.stream, g.ev_join2, 0));
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][4], g.stream));
   CU(cudaEventRecord(g.ev_copied, g.copy));
   CU(cudaStreamWaitEvent(g.stream, g.ev_copied, 0));
@@ -700,13 +758,15 @@ static int run_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *ra
     CU(cudaStreamWaitEvent(g.side, g.ev_fork, 0));
     CK(run_pp_prep(m, d, mass, kick, soff, pa, g.side, nullptr));
     CU(cudaEventRecord(g.ev_join, g.side));
+    g.ready_tiles = false;
     CK(run_pm3(m, ires, ratio_sf, gk, d, mass, kick, false, soff));
     if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][1], g.stream));
-    CU(cudaStreamWaitEvent(g.stream, g.ev_join, 0));
-    if (d.h_vp && g.L.ntile <= Ctx::kMaxTileEvents)
+    if (d.h_vp && g.L.ntile <= Ctx::kMaxTileEvents) {
       CK(run_pp_force_tiles(pa, d));
-    else
+    } else {
+      CU(cudaStreamWaitEvent(g.stream, g.ev_join, 0));
       CK(run_pp_force(pa));
+    }
   } else {
     if (do_pm3) CK(run_pm3(m, ires, ratio_sf, gk, d, mass, kick, !do_pp, soff));
     if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][1], g.stream));
@@ -778,10 +838,40 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   CU(cudaMemcpyAsync(g.rhoc.p, rhoc, sizeof(int32_t) * nrows * L.nte, cudaMemcpyHostToDevice, g.stream));
   CU(cudaMemcpyAsync(g.idx.p, idx_b_r, sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, g.stream));
   if (n_used) {
-    CU(cudaMemcpyAsync(g.xp.p, xp, sizeof(int16_t) * 3 * n_used, cudaMemcpyHostToDevice, g.stream));
-    // vp travels beside the deposit and FFTs; the stream waits for it before the first use
-    CU(cudaMemcpyAsync(g.vp.p, vp, sizeof(float) * 3 * n_used, cudaMemcpyHostToDevice, g.copy));
-    CU(cudaEventRecord(g.vp_ready, g.copy));
+    // xp tile by tile, so that the deposit of the first tiles overlaps the copy of the rest
+    // (the copy stream first waits for the compute stream's earlier work on these buffers)
+    CU(cudaEventRecord(g.ev_fork, g.stream));
+    CU(cudaStreamWaitEvent(g.copy, g.ev_fork, 0));
+    const int64_t rows = (int64_t)L.nte * L.nte;
+    const bool tiled = L.ntile <= Ctx::kMaxTileEvents;
+    for (int t = 0; tiled && t < L.ntile; t++) {
+      const int64_t lo = t ? idx_b_r[t * rows - 1] : 0, hi = idx_b_r[(t + 1) * rows - 1];
+      if (hi > lo)
+        CU(cudaMemcpyAsync((int16_t *)g.xp.p + 3 * lo, xp + 3 * lo, sizeof(int16_t) * 3 * (hi - lo),
+                           cudaMemcpyHostToDevice, g.copy));
+      CU(cudaEventRecord(g.ev_xp[t], g.copy));
+    }
+    if (tiled) {
+      g.xp_pending = true;
+      g.xp_tiles = L.ntile;
+    } else {
+      CU(cudaMemcpyAsync(g.xp.p, xp, sizeof(int16_t) * 3 * n_used, cudaMemcpyHostToDevice, g.stream));
+    }
+    // vp travels beside the deposit and FFTs, tile by tile; its users wait for their part
+    g.vp_tiles = 0;
+    if (tiled) {
+      for (int t = 0; t < L.ntile; t++) {
+        const int64_t lo = t ? idx_b_r[t * rows - 1] : 0, hi = idx_b_r[(t + 1) * rows - 1];
+        if (hi > lo)
+          CU(cudaMemcpyAsync((float *)g.vp.p + 3 * lo, vp + 3 * lo, sizeof(float) * 3 * (hi - lo),
+                             cudaMemcpyHostToDevice, g.copy));
+        CU(cudaEventRecord(g.ev_vp[t], g.copy));
+      }
+      g.vp_tiles = L.ntile;
+    } else {
+      CU(cudaMemcpyAsync(g.vp.p, vp, sizeof(float) * 3 * n_used, cudaMemcpyHostToDevice, g.copy));
+      CU(cudaEventRecord(g.vp_ready, g.copy));
+    }
     g.vp_pending = true;
   }
   Dev d{(const int16_t *)g.xp.p, (const int32_t *)g.rhoc.p, (const int64_t *)g.idx.p, (float *)g.vp.p, n_used};
@@ -789,10 +879,14 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   d.h_idx = idx_b_r;
   g.vp_copied = false;
   const int st = run_kick(ires, ixyz3, ratio_sf, apm3, gk, d, mass, a_mid, dt, do_pm3, do_pp, m);
-  const int wst = wait_vp();  // also on a failed or vp-free run: the D2H below must follow the upload
+  // also on a failed run: later work on these buffers must follow the uploads
+  const int xst = wait_xp(g.stream);
+  g.xp_pending = false;
+  const int wst = xst != CUBE_OK ? xst : wait_vp();
   if (st != CUBE_OK || wst != CUBE_OK) {
     cudaStreamSynchronize(g.copy);
     cudaStreamSynchronize(g.side);
+    cudaStreamSynchronize(g.side2);
     cudaStreamSynchronize(g.stream);
     return st != CUBE_OK ? st : wst;
   }
