@@ -404,30 +404,33 @@ static const int kFftBuckets[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 
 static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, const float *const *gk,
                    const Dev &d, float mass, float kick, bool want_vmax, size_t &soff) {
   const Lay &L = g.L;
-  if (L.pm3_mode == CUBE_PM3_PERIODIC) {
+  if (L.pm3_mode == CUBE_PM3_PERIODIC || L.pm3_mode == CUBE_PM3_TILE_PERIODIC) {
+    // one periodic mesh over the image, or one per parent tile (each tile its own periodic box)
+    const bool per_tile = L.pm3_mode == CUBE_PM3_TILE_PERIODIC;
     const int rsf = ratio_sf[m.ires_loc[0] - 1];
     for (int q = 0; q < L.ns3; q++)
       if (ratio_sf[m.ires_loc[q] - 1] != rsf) return fail(CUBE_ERR_INVALID);
-    const int n = L.ng * rsf;
+    const int n = (per_tile ? L.nt * L.rcs : L.ng) * rsf;
+    const int nslots = per_tile ? L.ntile : 1;
     const int64_t n3 = (int64_t)n * n * n, nk = (int64_t)n * n * (n / 2 + 1);
     float *G = nullptr;
     CK(get_green_periodic(n, rsf, &G));
-    CK(grow(g.rho, sizeof(float) * n3));
-    CK(grow(g.rhok, sizeof(cufftComplex) * nk));
-    CK(grow(g.force, sizeof(float) * n3 * 3));
+    CK(grow(g.rho, sizeof(float) * n3 * nslots));
+    CK(grow(g.rhok, sizeof(cufftComplex) * nk * nslots));
+    CK(grow(g.force, sizeof(float) * n3 * 3 * nslots));
     const double scale = (double)L.rcs / (double)(1.0f / (float)rsf);
     std::vector<MeshJob> jobs(L.ntile);
     for (int t = 0; t < L.ntile; t++) {
       const int tx = t % L.nnt, ty = (t / L.nnt) % L.nnt, tz = t / (L.nnt * L.nnt);
       MeshJob &J = jobs[t];
       J.t = t;
-      J.slot = 0;
+      J.slot = per_tile ? t : 0;
       J.range = 0.f;
       const int tc[3] = {tx, ty, tz};
       for (int q = 0; q < 3; q++) {
         J.lo[q] = L.ncb;
         J.alo[q] = L.ncb;
-        J.off[q] = -(double)tc[q] * L.nt * scale;
+        J.off[q] = per_tile ? 0.0 : -(double)tc[q] * L.nt * scale;
       }
     }
     CK(upload(g.jobs, jobs.data(), jobs.size(), soff));
@@ -435,7 +438,7 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     a.L = &g.L;
     a.rsf = rsf;
     a.n = n;
-    a.nslots = 1;
+    a.nslots = nslots;
     a.jobs = (const MeshJob *)g.jobs.p;
     a.njobs = L.ntile;
     for (int q = 0; q < 3; q++) a.rdep[q] = a.ract[q] = L.nt;
@@ -457,9 +460,9 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     a.out = (float *)g.out.p;
     a.want_vmax = want_vmax;
     cufftHandle fw, bw;
-    CK(get_plan(n, 1, CUFFT_R2C, &fw));
-    CK(get_plan(n, 1, CUFFT_C2R, &bw));
-    CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3, g.stream));
+    CK(get_plan(n, nslots, CUFFT_R2C, &fw));
+    CK(get_plan(n, nslots, CUFFT_C2R, &bw));
+    CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3 * nslots, g.stream));
     if (g.xp_pending) {  // deposit each tile as soon as its particles are on the device
       PM3Args at = a;
       at.njobs = 1;
@@ -916,7 +919,8 @@ int cube_set_layout(const cube_layout *l) {
   if (l->ng % rcs || (l->ng / rcs) % l->nnt || ((l->ng / rcs) / l->nnt) % l->nns) return fail(CUBE_ERR_INVALID);
   if (l->ngb % rcs || l->ngb < rcs) return fail(CUBE_ERR_INVALID);
   if (l->p_order != 2) return fail(CUBE_ERR_INVALID);
-  if (l->pm3_mode != CUBE_PM3_SUBTILE && l->pm3_mode != CUBE_PM3_PERIODIC) return fail(CUBE_ERR_INVALID);
+  if (l->pm3_mode != CUBE_PM3_SUBTILE && l->pm3_mode != CUBE_PM3_PERIODIC && l->pm3_mode != CUBE_PM3_TILE_PERIODIC)
+    return fail(CUBE_ERR_INVALID);
   if (!(l->app >= 0.f)) return fail(CUBE_ERR_INVALID);
   Lay L{};
   L.ng = l->ng;

@@ -59,6 +59,15 @@ def zeldovich_lattice(n: int, rms_disp: float, seed: int, slope: float = -2.0):
     return pos, vel, delta
 
 
+def zeldovich_box(m: int, box: float, rms_disp: float, seed: int, slope: float = -2.0):
+    """An m^3 lattice in a periodic box of side ``box`` fine cells, displaced by the Zel'dovich
+    field of a P ~ k^slope Gaussian delta on the m^3 lattice, rms |Psi| = rms_disp fine cells.
+    Returns (pos float64[m^3,3] in [0,box), vel float32[m^3,3] = Psi in fine cells)."""
+    pos, vel, _ = zeldovich_lattice(m, rms_disp * m / box, seed, slope)
+    scale = box / m
+    return np.mod(pos * scale, box), (vel * scale).astype(np.float32)
+
+
 def lognormal_poisson(n: int, sigma: float, seed: int, mean_per_cell: float = 1.0,
                       slope: float = -2.0):
     """Poisson sample of a lognormal density on an n^3 fine grid.

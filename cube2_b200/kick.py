@@ -26,6 +26,7 @@ LIB_PATH = os.path.join(HERE, "libcube2_b200.so")
 
 CUBE_PM3_SUBTILE = 0
 CUBE_PM3_PERIODIC = 1
+CUBE_PM3_TILE_PERIODIC = 2
 
 _STATUS = {0: "ok", 1: "invalid argument or subtile metadata", 2: "layout not configured", 3: "CUDA runtime error",
            4: "cuFFT error", 5: "device capacity check failed", 6: "no CUDA device visible",

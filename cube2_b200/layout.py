@@ -161,6 +161,35 @@ def build_image(pos: np.ndarray, vel: np.ndarray, layout: Layout) -> Image:
                  n_particles=int(np.asarray(pos).shape[0]))
 
 
+def build_tile_batch(boxes, tile: Layout, nnt: int) -> Image:
+    """A batch of nnt^3 independent periodic boxes as one image of nnt^3 parent tiles.
+
+    ``boxes`` is a list of (pos, vel) per box, positions in [0, tile.ng)^3, in tile order
+    t = (tz*nnt + ty)*nnt + tx.  Every box is cell-sorted with ``build_image`` on the one-tile
+    layout ``tile`` (so its buffer holds its own periodic copies) and the tiles are stored one
+    after the other, with the spine ``idx_b_r`` running over the whole batch.  This is the
+    input of the per-tile periodic PM3 geometry (CUBE_PM3_TILE_PERIODIC).  ``pid`` numbers the
+    particles of box t after those of boxes 0..t-1.
+    """
+    if tile.nnt != 1:
+        raise ValueError("boxes are laid out with a one-tile layout")
+    if len(boxes) != nnt ** 3:
+        raise ValueError("need nnt^3 boxes")
+    L = Layout(ng=tile.ng * nnt, nnt=nnt, nns=tile.nns, ratio_cs=tile.ratio_cs, ngb=tile.ngb, app=tile.app)
+    imgs = [build_image(p, v, tile) for p, v in boxes]
+    nte = tile.nte
+    xp = np.concatenate([im.xp for im in imgs])
+    vp = np.concatenate([im.vp for im in imgs])
+    rhoc = np.stack([im.rhoc.reshape(nte, nte, nte) for im in imgs]).reshape(nnt, nnt, nnt, nte, nte, nte)
+    offs = np.cumsum([0] + [im.n_used for im in imgs])
+    idx = np.stack([im.idx_b_r.reshape(nte, nte) + offs[t] for t, im in enumerate(imgs)])
+    poffs = np.cumsum([0] + [im.n_particles for im in imgs])
+    pid = np.concatenate([im.pid + poffs[t] for t, im in enumerate(imgs)])
+    active = np.concatenate([im.active for im in imgs])
+    return Image(L, xp, vp, rhoc.astype(np.int32), idx.reshape(nnt, nnt, nnt, nte, nte).astype(np.int64),
+                 pid.astype(np.int64), active, n_particles=int(poffs[-1]))
+
+
 def ixyz3_table(layout: Layout) -> np.ndarray:
     """Subtile index table (initialize.f90:207-224): rows [sx,sy,sz,tx,ty,tz], 1-based."""
     nnt, nns = layout.nnt, layout.nns

@@ -9,7 +9,14 @@
   (seed 2000); fine-cell occupancy 0 to several hundred.  PM3 mesh 512^3, PP
   cutoff 2 fine cells, softening 0.1.  2^3 tiles (nnt = 2).
 
-Both use ratio_cs = 4, a one coarse-cell tile buffer (ngb = 4), TSC, equal
+* ``batch512``      512 independent periodic boxes of 32^3 fine cells stored as
+  the 8^3 parent tiles of one image (PM3 geometry CUBE_PM3_TILE_PERIODIC: a
+  64^3 mesh per box).  Box t holds an m^3 lattice displaced by its own
+  Zel'dovich field (seed 3000 + t, rms 0.5 cell), m^3 the nearest cube to a
+  lognormal count (median 32^3, sigma 1, clipped to 2048 .. 200000; seed
+  3000), so the boxes are uneven.  ``batch8`` is the same with 8 boxes.
+
+All use ratio_cs = 4, a one coarse-cell tile buffer (ngb = 4), TSC, equal
 particle mass 1, PM3 softening apm3f = 4 mesh cells on a ratio_sf = 2 mesh
 (so the PP range apm3f / ratio_sf is 2 fine cells) and the full periodic
 force (apm_range = 0).
@@ -21,7 +28,7 @@ import os
 import numpy as np
 
 from . import ic
-from .layout import RATIO_SF, Image, Layout, apm3_table, build_image, ixyz3_table
+from .layout import RATIO_SF, Image, Layout, apm3_table, build_image, build_tile_batch, ixyz3_table
 
 WORKLOADS = {
     "zeldovich64": dict(layout=dict(ng=64, nnt=1, nns=2, ratio_cs=4, ngb=4, app=0.1), kind="zeldovich", n=64,
@@ -31,7 +38,30 @@ WORKLOADS = {
     # profiling size: same statistics, 192^3 box (~7M particles), 384^3 mesh (> L2 per array)
     "clustered192": dict(layout=dict(ng=192, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1), kind="lognormal", n=192,
                          sigma=1.5, seed=2000, rsf=2, apm3f=4.0),
+    # 512 independent periodic boxes of 32^3 fine cells, uneven particle counts, one launch per stage
+    "batch512": dict(layout=dict(ng=256, nnt=8, nns=2, ratio_cs=4, ngb=4, app=0.1), kind="batch", box=32,
+                     median=32768, sigma=1.0, clip=(2048, 200000), seed=3000, rsf=2, apm3f=4.0),
+    # the same with 8 boxes and smaller counts (tests)
+    "batch8": dict(layout=dict(ng=64, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1), kind="batch", box=32,
+                   median=4096, sigma=1.0, clip=(512, 20000), seed=3100, rsf=2, apm3f=4.0),
 }
+
+
+def batch_counts(name: str) -> np.ndarray:
+    """Lattice side per box of a batch workload: the count N_t = clip(round(median exp(sigma z)))
+    of each box (z standard normal, seeded), rounded to the nearest cube m^3."""
+    w = WORKLOADS[name]
+    nb = w["layout"]["nnt"] ** 3
+    rng = np.random.Generator(np.random.PCG64(w["seed"]))
+    cnt = np.clip(np.round(w["median"] * np.exp(w["sigma"] * rng.standard_normal(nb))), *w["clip"])
+    return np.maximum(np.round(np.cbrt(cnt)).astype(np.int64), 1)
+
+
+def tile_layout(name: str) -> Layout:
+    """One-box layout of a batch workload (the layout each box is cell-sorted with)."""
+    w = WORKLOADS[name]
+    lw = dict(w["layout"])
+    return Layout(ng=w["box"], nnt=1, nns=lw["nns"], ratio_cs=lw["ratio_cs"], ngb=lw["ngb"], app=lw["app"])
 
 
 def cache_dir() -> str:
@@ -48,11 +78,16 @@ def make(name: str, use_cache: bool = True) -> Image:
     if use_cache and os.path.exists(path):
         z = np.load(path)
         return Image(L, z["xp"], z["vp"], z["rhoc"], z["idx_b_r"], z["pid"], z["active"], int(z["n_particles"]))
-    if w["kind"] == "zeldovich":
-        pos, vel, _ = ic.zeldovich_lattice(w["n"], w["rms"], w["seed"])
+    if w["kind"] == "batch":
+        boxes = [ic.zeldovich_box(int(m), float(w["box"]), 0.5, w["seed"] + t) for t, m in
+                 enumerate(batch_counts(name))]
+        img = build_tile_batch(boxes, tile_layout(name), L.nnt)
     else:
-        pos, vel, _ = ic.lognormal_poisson(w["n"], w["sigma"], w["seed"])
-    img = build_image(pos, vel, L)
+        if w["kind"] == "zeldovich":
+            pos, vel, _ = ic.zeldovich_lattice(w["n"], w["rms"], w["seed"])
+        else:
+            pos, vel, _ = ic.lognormal_poisson(w["n"], w["sigma"], w["seed"])
+        img = build_image(pos, vel, L)
     if use_cache:
         np.savez(path, xp=img.xp, vp=img.vp, rhoc=img.rhoc, idx_b_r=img.idx_b_r, pid=img.pid, active=img.active,
                  n_particles=img.n_particles)

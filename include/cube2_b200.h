@@ -44,8 +44,11 @@ enum cube_status {
 
 /* PM3 mesh geometry */
 enum cube_pm3_mode {
-  CUBE_PM3_SUBTILE = 0, /* the reference's per-subtile buffered meshes, Green tables from the caller */
-  CUBE_PM3_PERIODIC = 1 /* one periodic mesh of side ng*ratio_sf over the image, Green table tabulated here */
+  CUBE_PM3_SUBTILE = 0,       /* the reference's per-subtile buffered meshes, Green tables from the caller */
+  CUBE_PM3_PERIODIC = 1,      /* one periodic mesh of side ng*ratio_sf over the image, Green table tabulated here */
+  CUBE_PM3_TILE_PERIODIC = 2  /* every parent tile is its own periodic box (a batch of independent boxes whose
+                                 buffers hold the tile's own periodic copies): one periodic mesh of side
+                                 nt*ratio_cs*ratio_sf per tile, transformed as one batch */
 };
 
 typedef struct cube_layout {
