@@ -119,7 +119,7 @@ def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
     from cube2_b200 import workloads as W
-    from cube2_b200.kick import FineKick, force_truth_fp64
+    from cube2_b200.kick import CUBE_PM3_PERIODIC, CUBE_PM3_TILE_PERIODIC, FineKick, force_truth_fp64
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -129,7 +129,8 @@ def run_ours(args, rank, world, local_rank):
     img = W.make(args.workload)
     L = img.layout
     isort, ires, ix, apm3, rs = W.tables(args.workload)
-    fk = FineKick(L, apm3f=w["apm3f"])
+    batch = w["kind"] == "batch"  # independent periodic boxes, one PM3 mesh per parent tile
+    fk = FineKick(L, pm3_mode=CUBE_PM3_TILE_PERIODIC if batch else CUBE_PM3_PERIODIC, apm3f=w["apm3f"])
     N = img.n_particles
     a_mid, dt = np.float32(6 * np.pi), np.float32(1.0)  # dv = force
 
@@ -190,6 +191,27 @@ def run_ours(args, rank, world, local_rank):
     ms_step = ms / max(args.steps, 1)
     value = N * world * args.steps / (ms * 1e-3)
 
+    # the same kick replayed as one captured CUDA graph (cube_kick_graph_*)
+    graph = None
+    try:
+        kg = fk.kick_graph(d_rhoc, d_idx, d_xp, img.n_used, d_vp, d_out, isort, ires, ix, apm3, rs, 1.0, a_mid, dt)
+        for _ in range(max(args.warmup, 0)):
+            kg.launch(stream)
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(args.steps):
+            kg.launch(stream)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        kg.close()
+        gms = g0.elapsed_time(g1) / max(args.steps, 1)
+        graph = {"ms_per_step": gms, "value": N / (gms * 1e-3), "unit": UNIT,
+                 "what": "the device kick captured once as a CUDA graph and replayed per step"}
+    except Exception as e:  # the graph is reported beside the main number, never instead of it
+        graph = {"error": repr(e)}
+
     # e2e through the host C-ABI with pinned buffers
     e2e = None
     if not args.no_e2e:
@@ -227,9 +249,13 @@ def run_ours(args, rank, world, local_rank):
         act = np.nonzero(img.active)[0]
         rng = np.random.default_rng(12345)
         samp = rng.choice(act, min(args.truth_targets, act.size), replace=False)
-        pos = W.physical_positions(img)
         t_tr = time.perf_counter()
-        Ft = force_truth_fp64(pos, float(L.ng), L.app, img.pid[samp])
+        if batch:  # every box is its own periodic box: the truth is summed per box
+            samp = np.sort(samp[:min(samp.size, 2000)])
+            Ft = batch_truth(args.workload, img, samp, force_truth_fp64)
+        else:
+            pos = W.physical_positions(img)
+            Ft = force_truth_fp64(pos, float(L.ng), L.app, img.pid[samp])
         t_tr = time.perf_counter() - t_tr
         F = v[samp] / kick_coef
         dF = np.linalg.norm(F - Ft, axis=1)
@@ -250,8 +276,14 @@ def run_ours(args, rank, world, local_rank):
                 "traffic": float(PP_DRAM_BYTES_PER_STORED * img.n_used),
                 "traffic_source": "ncu DRAM bytes of k_pp_force on clustered192, scaled by stored particles"}
 
+    loop = per_box_loop(args.workload, fk, img, stream, a_mid, dt, ms_step) if batch and rank == 0 else None
+    if batch:
+        fk.configure()
+
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if batch:
+        cpu = {"unavailable": "the reference CPU baseline is timed on the single-image workloads"}
+    elif rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cpu = cpu_reference(args.workload, img, sample=True)
         except Exception as e:  # the baseline must not hide our number
@@ -260,20 +292,88 @@ def run_ours(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32 (int16 fixed-point positions, fp64 Green table)",
-            "data": "synthetic (seeded lognormal Poisson sample; see cube2_b200/workloads.py)",
+            "data": ("synthetic (512 seeded Zel'dovich boxes of uneven size; see cube2_b200/workloads.py)" if batch
+                     else "synthetic (seeded lognormal Poisson sample; see cube2_b200/workloads.py)"),
             "config": {"workload": args.workload, "particles": N, "n_used_stored": img.n_used,
-                       "pm3_mesh": L.ng * w["rsf"], "pp_cutoff_fine_cells": w["apm3f"] / w["rsf"],
+                       "pm3_mesh": (f"{w['box'] * w['rsf']}^3 per box x {L.nnt ** 3} boxes" if batch
+                                    else L.ng * w["rsf"]),
+                       "pp_cutoff_fine_cells": w["apm3f"] / w["rsf"],
                        "softening_fine_cells": L.app, "assignment": "TSC", "variant": "plain (no learned shell)",
                        "layout": L.as_dict(), "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (mesh 512^3 fp32 = 537 MB, particle arrays > 120 MB)"},
+                       "l2": ("inputs larger than L2 (meshes 512 x 64^3 fp32 = 537 MB, particle arrays > 290 MB)"
+                              if batch else "inputs larger than L2 (mesh 512^3 fp32 = 537 MB, particle arrays > 120 MB)")},
             "stages_ms": {"pm3": pm3_ms, "pp_binning_and_worklist": ppb_ms, "pp_force": ppf_ms,
                           "note": "the PP binning and work list run on a second stream beside PM3"},
             "roofline": roofline, "force_error": truth, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": ck, "cpu_baseline": cpu}
+            "clocks": ck, "cpu_baseline": cpu, "graph": graph}
+    if loop is not None:
+        line["per_box_loop"] = loop
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+def _batch_boxes(workload: str):
+    from cube2_b200 import ic
+    from cube2_b200 import workloads as W
+    w = W.WORKLOADS[workload]
+    return [ic.zeldovich_box(int(m), float(w["box"]), 0.5, w["seed"] + t) for t, m in enumerate(W.batch_counts(workload))]
+
+
+def batch_truth(workload: str, img, samp, force_truth_fp64):
+    """FP64 truth for the sampled stored particles of a batch: each box is summed alone."""
+    from cube2_b200 import workloads as W
+    from cube2_b200.layout import build_image
+    tl = W.tile_layout(workload)
+    boxes = _batch_boxes(workload)
+    n_per = np.array([b[0].shape[0] for b in boxes])
+    poffs = np.concatenate([[0], np.cumsum(n_per)])
+    pid = img.pid[samp]
+    box = np.searchsorted(poffs, pid, side="right") - 1
+    F = np.zeros((samp.size, 3))
+    for t in np.unique(box):
+        sel = np.nonzero(box == t)[0]
+        one = build_image(boxes[t][0], boxes[t][1], tl)
+        pos = W.physical_positions(one)
+        F[sel] = force_truth_fp64(pos, float(tl.ng), tl.app, pid[sel] - poffs[t])
+    return F
+
+
+def per_box_loop(workload: str, fk_batch, img, stream, a_mid, dt, ms_batched):
+    """The same boxes kicked one call per box (device-resident, one-tile layout), timed with
+    CUDA events over one pass after a warm-up pass: the launch-per-tile loop the batch replaces."""
+    import torch
+    from cube2_b200 import workloads as W
+    from cube2_b200.kick import CUBE_PM3_PERIODIC, FineKick
+    from cube2_b200.layout import RATIO_SF, apm3_table, build_image, ixyz3_table
+    w = W.WORKLOADS[workload]
+    tl = W.tile_layout(workload)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ones = [build_image(p, v, tl) for p, v in _batch_boxes(workload)]
+
+    def up(a):
+        return torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).to(dev)
+    bufs = [(up(o.rhoc), up(o.idx_b_r), up(o.xp), up(o.vp), o.n_used) for o in ones]
+    d_out = torch.zeros(8, dtype=torch.float32, device=dev)
+    fk1 = FineKick(tl, pm3_mode=CUBE_PM3_PERIODIC, apm3f=w["apm3f"])
+    t1 = (np.arange(1, tl.ns3 + 1, dtype=np.int32), np.full(tl.ns3, 2, np.int32), ixyz3_table(tl),
+          apm3_table(w["apm3f"]), RATIO_SF.copy())
+
+    def one_pass():
+        for b in bufs:
+            fk1.kick_fine_device(b[0], b[1], b[2], b[4], b[3], d_out, *t1, 1.0, a_mid, dt, stream=stream)
+    one_pass()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    one_pass()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"ms_per_step": ms, "value": img.n_particles / (ms * 1e-3), "unit": UNIT, "calls_per_step": len(bufs),
+            "batched_speedup": ms / ms_batched,
+            "what": "one cube_kick_fine_device call per box (one-tile layout, periodic mesh per call)"}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -342,6 +442,10 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     from cube2_b200 import workloads as W
+    if W.WORKLOADS[args.workload]["kind"] == "batch":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference CPU path is timed on the single-image "
+                          "workloads; batch workloads compare against a per-box launch loop instead"}))
+        return
     img = W.make(args.workload)
     times = []
     res = None

@@ -98,6 +98,9 @@ struct Ctx {
   // Pinned staging areas for the small per-call tables, used round robin so the
   // host can enqueue the next kick while earlier ones still copy out of theirs.
   static constexpr int kStage = 4;
+  // a captured graph's own staging area, used instead of the ring while it is captured
+  void *stage_override = nullptr;
+  size_t stage_override_cap = 0;
   void *stage_buf[kStage] = {};
   cudaEvent_t stage_evs[kStage] = {};
   bool stage_used[kStage] = {};
@@ -205,6 +208,11 @@ static int ensure_device() {
 // Make every staging area hold `bytes` and select the next one, waiting until
 // the call that last used it has finished copying out of it.
 static int stage_begin(size_t bytes) {
+  if (g.stage_override) {
+    if (bytes > g.stage_override_cap) return fail(CUBE_ERR_CAPACITY);
+    g.h_stage = g.stage_override;
+    return CUBE_OK;
+  }
   if (bytes > g.h_stage_cap) {
     CU(cudaDeviceSynchronize());
     for (auto &b : g.stage_buf)
@@ -224,6 +232,7 @@ static int stage_begin(size_t bytes) {
 
 // Mark the current staging area busy until the stream passes this point.
 static int stage_end() {
+  if (g.stage_override) return CUBE_OK;
   const int s = g.stage_slot;
   CU(cudaEventRecord(g.stage_evs[s], g.stream));
   g.stage_used[s] = true;
@@ -238,7 +247,7 @@ static int upload(Buf &dst, const T *src, size_t count, size_t &stage_off, cudaS
   CK(grow(dst, bytes > 0 ? bytes : 16));
   if (!bytes) return CUBE_OK;
   stage_off = (stage_off + 255) & ~(size_t)255;
-  if (stage_off + bytes > g.h_stage_cap) return fail(CUBE_ERR_CAPACITY);
+  if (stage_off + bytes > (g.stage_override ? g.stage_override_cap : g.h_stage_cap)) return fail(CUBE_ERR_CAPACITY);
   memcpy((char *)g.h_stage + stage_off, src, bytes);
   CU(cudaMemcpyAsync(dst.p, (char *)g.h_stage + stage_off, bytes, cudaMemcpyHostToDevice, st ? st : g.stream));
   stage_off += bytes;
@@ -1060,6 +1069,113 @@ int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32
   }
   g.stream = own;
   return s;
+}
+
+// A captured kick: the graph, its executable form, the pinned staging area its table uploads
+// read from, and the number of library kernels one replay launches.
+struct cube_kick_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  void *stage = nullptr;
+  int device = -1;
+  long long launches = 0;
+};
+
+int cube_kick_graph_create(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                           const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r,
+                           const int16_t *d_xp, int64_t n_used, float *d_vp, float mass, float a_mid, float dt,
+                           float *d_out, cube_kick_graph **out) {
+  (void)isort;
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!out) return fail(CUBE_ERR_INVALID);
+  *out = nullptr;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  // the subtile geometry synchronises the host between mesh batches, which a graph cannot hold
+  if (g.L.pm3_mode == CUBE_PM3_SUBTILE) return fail(CUBE_ERR_INVALID);
+  if (!apm3 || !d_rhoc || !d_idx_b_r || !d_xp || !d_vp || !d_out) return fail(CUBE_ERR_INVALID);
+  if (n_used < 0 || n_used >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  const float *gk[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  // 1. a kick on a scratch copy of vp sizes every buffer, plan and table outside the capture
+  {
+    float *scratch = nullptr;
+    CU(cudaMalloc(&scratch, sizeof(float) * 3 * (size_t)std::max<int64_t>(n_used, 1)));
+    cudaError_t e = cudaMemcpyAsync(scratch, d_vp, sizeof(float) * 3 * n_used, cudaMemcpyDeviceToDevice, g.stream);
+    Meta m;
+    Dev d{d_xp, d_rhoc, d_idx_b_r, scratch, n_used};
+    int st = e == cudaSuccess ? run_kick(ires, ixyz3, ratio_sf, apm3, gk, d, mass, a_mid, dt, true, true, m)
+                              : fail(CUBE_ERR_CUDA);
+    cudaStreamSynchronize(g.stream);
+    cudaFree(scratch);
+    if (st != CUBE_OK) return st;
+  }
+  // 2. the capture, with the graph's own staging area and without the timing events
+  cube_kick_graph *kg = new cube_kick_graph;
+  kg->device = g.device;
+  const size_t stage_bytes = (size_t)4 << 20;
+  if (cudaMallocHost(&kg->stage, stage_bytes) != cudaSuccess) {
+    delete kg;
+    return fail(CUBE_ERR_CUDA);
+  }
+  const bool timing = g.timing;
+  g.timing = false;
+  g.stage_override = kg->stage;
+  g.stage_override_cap = stage_bytes;
+  const long long l0 = g.launches;
+  int st = CUBE_OK;
+  if (cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    st = fail(CUBE_ERR_CUDA);
+  } else {
+    Meta m;
+    Dev d{d_xp, d_rhoc, d_idx_b_r, d_vp, n_used};
+    st = run_kick(ires, ixyz3, ratio_sf, apm3, gk, d, mass, a_mid, dt, true, true, m);
+    if (st == CUBE_OK &&
+        cudaMemcpyAsync(d_out, g.out.p, sizeof(float) * 6, cudaMemcpyDeviceToDevice, g.stream) != cudaSuccess)
+      st = fail(CUBE_ERR_CUDA);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(g.stream, &graph);  // always ends the capture
+    kg->graph = graph;
+    if (st == CUBE_OK && (e != cudaSuccess || !graph)) st = fail(CUBE_ERR_CUDA);
+  }
+  g.stage_override = nullptr;
+  g.stage_override_cap = 0;
+  g.timing = timing;
+  kg->launches = g.launches - l0;
+  g.launches = l0;
+  if (st == CUBE_OK && cudaGraphInstantiate(&kg->exec, kg->graph, 0) != cudaSuccess) st = fail(CUBE_ERR_CUDA);
+  if (st != CUBE_OK) {
+    cudaGetLastError();  // a failed capture leaves its error behind
+    if (kg->graph) cudaGraphDestroy(kg->graph);
+    cudaFreeHost(kg->stage);
+    delete kg;
+    return st;
+  }
+  *out = kg;
+  return CUBE_OK;
+}
+
+int cube_kick_graph_launch(cube_kick_graph *kg, void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!kg || !kg->exec) return fail(CUBE_ERR_INVALID);
+  CU(cudaSetDevice(kg->device));
+  CU(cudaGraphLaunch(kg->exec, (cudaStream_t)stream));
+  g.launches += kg->launches;
+  return CUBE_OK;
+}
+
+int cube_kick_graph_destroy(cube_kick_graph *kg) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!kg) return CUBE_OK;
+  cudaSetDevice(kg->device);
+  if (kg->exec) cudaGraphExecDestroy(kg->exec);
+  if (kg->graph) cudaGraphDestroy(kg->graph);
+  cudaStreamSynchronize(nullptr);
+  if (kg->stage) cudaFreeHost(kg->stage);
+  delete kg;
+  return CUBE_OK;
 }
 
 void c_pm3_force_kernel(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const int32_t *ratio_sf,

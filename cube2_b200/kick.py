@@ -53,7 +53,8 @@ EXPORTS = ("cube_set_layout", "cube_get_layout", "cube_last_error", "cube_error_
            "c_pp_force_kernel", "c_pm3_fft_finalize", "c_gpu_velocity_finalize", "cube_pm3_force", "cube_pp_force",
            "cube_kick_fine", "cube_kick_fine_device", "cube_pp_bin_tile", "cube_pp_pair_count", "cube_green_table",
            "cube_force_truth_fp64", "cube_stage_times", "cube_enable_timing", "cube_timing_read",
-           "cube_launch_count", "cube_fp32_peak_probe", "cube_pp_force_noalloc")
+           "cube_launch_count", "cube_fp32_peak_probe", "cube_pp_force_noalloc", "cube_kick_graph_create",
+           "cube_kick_graph_launch", "cube_kick_graph_destroy")
 
 
 def lib() -> ctypes.CDLL:
@@ -91,6 +92,28 @@ def _c32(a):
 
 def _f32(a):
     return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class KickGraph:
+    """A captured device kick; ``launch(stream)`` replays it, ``close()`` frees it."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self.handle = handle
+
+    def launch(self, stream=None):
+        s = None if stream is None else ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+        _check(lib().cube_kick_graph_launch(self.handle, s), "cube_kick_graph_launch")
+
+    def close(self):
+        if self.handle:
+            lib().cube_kick_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class FineKick:
@@ -182,6 +205,20 @@ class FineKick:
                                          s)
         _check(st, "cube_kick_fine_device")
         del keep
+
+    def kick_graph(self, d_rhoc, d_idx, d_xp, n_used, d_vp, d_out, isort, ires, ixyz3, apm3, ratio_sf, mass,
+                   a_mid, dt) -> "KickGraph":
+        """Capture the device kick on these arrays as a CUDA graph (cube_kick_graph_create)."""
+        def dp(x):
+            return ctypes.c_void_p(x if isinstance(x, int) else x.data_ptr())
+        isort, ires, ixyz3, ratio_sf, apm3 = _c32(isort), _c32(ires), _c32(ixyz3), _c32(ratio_sf), _f32(apm3)
+        h = ctypes.c_void_p()
+        st = lib().cube_kick_graph_create(_p(isort), _p(ires), _p(ixyz3), _p(apm3), _p(ratio_sf), dp(d_rhoc),
+                                          dp(d_idx), dp(d_xp), ctypes.c_int64(int(n_used)), dp(d_vp),
+                                          ctypes.c_float(mass), ctypes.c_float(a_mid), ctypes.c_float(dt), dp(d_out),
+                                          ctypes.byref(h))
+        _check(st, "cube_kick_graph_create")
+        return KickGraph(h)
 
     # -- inspection ------------------------------------------------------------------------------
     def pp_bin_tile(self, img: Image, tile: int, ires, ixyz3, ratio_sf, spatial: bool = False):

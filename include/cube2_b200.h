@@ -130,6 +130,26 @@ int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32
                           const int16_t *d_xp, int64_t n_used, const float *const gk[5], float *d_vp, float mass,
                           float a_mid, float dt, float *d_out, void *stream);
 
+/* ---- the device kick as one CUDA graph (no reference counterpart) ---- */
+
+/* cube_kick_fine_device captured once as a CUDA graph and replayed per step, so that a
+ * time loop pays one graph launch per kick.  Creation runs one kick on a scratch copy of
+ * d_vp (d_vp itself is untouched) to size every buffer, then captures the kick on the
+ * library's own stream.  The graph keeps the device pointers, n_used, the tables
+ * (ires, ixyz3, apm3, ratio_sf) and mass/a_mid/dt of this call: a replay kicks the
+ * current contents of these arrays, and a new graph is needed when the layout, the
+ * subtile levels or n_used change.  Geometries CUBE_PM3_PERIODIC and
+ * CUBE_PM3_TILE_PERIODIC only (CUBE_ERR_INVALID for CUBE_PM3_SUBTILE).  A replay must not
+ * overlap another call of the library. */
+typedef struct cube_kick_graph cube_kick_graph;
+int cube_kick_graph_create(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
+                           const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r,
+                           const int16_t *d_xp, int64_t n_used, float *d_vp, float mass, float a_mid, float dt,
+                           float *d_out, cube_kick_graph **graph);
+/* Enqueue one replay on `stream` (a cudaStream_t; NULL = the default stream). */
+int cube_kick_graph_launch(cube_kick_graph *graph, void *stream);
+int cube_kick_graph_destroy(cube_kick_graph *graph);
+
 /* ---- allocation-free PP kick ---- */
 
 /* Largest input cube_pp_force_noalloc accepts: stored particles (n_used) and
