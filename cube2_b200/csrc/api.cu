@@ -79,6 +79,7 @@ struct Ctx {
   Buf xp, rhoc, idx, vp, cell_base;
   Buf tiles, count, cell_start, scan_tmp, spos, spill, spill_rank, counters, items, range_loc, sched;
   Buf rho, rhok, force, jobs, out;
+  Buf mlp_pos, mlp_rho;  // learned shell: positions of the stored copies, fine-grid CIC density
   void *h_stage = nullptr;  // pinned staging for small tables
   size_t h_stage_cap = 0;
   float *h_out = nullptr;   // pinned [8]: out[5], err
@@ -1071,6 +1072,164 @@ int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32
   return s;
 }
 
+// ---- learned PP shell ----
+
+struct cube_mlp {
+  cube::MlpParams p;
+};
+
+static void mlp_free(cube_mlp *h) {
+  MlpParams &p = h->p;
+  void *bufs[] = {p.master, p.grad, p.mom, p.vel, p.wb, p.wt, p.xb, p.a[0], p.a[1], p.a[2], p.dyb, p.dzb, p.dzt,
+                  p.at, p.tb, p.z[0], p.z[1], p.z[2], p.y, p.dy, p.dz, p.da, p.b4pad};
+  for (void *b : bufs)
+    if (b) cudaFree(b);
+  delete h;
+}
+
+int cube_mlp_create(const float *params, int32_t batch_cap, cube_mlp **out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!params || !out || batch_cap <= 0 || batch_cap % 16) return fail(CUBE_ERR_INVALID);
+  *out = nullptr;
+  CK(ensure_device());
+  cube_mlp *h = new cube_mlp;
+  MlpParams &p = h->p;
+  p.device = g.device;
+  p.cap = batch_cap;
+  const size_t B = (size_t)batch_cap, W = kMlpW;
+  bool ok = true;
+  auto al = [&](auto **ptr, size_t bytes) {
+    if (ok && cudaMalloc((void **)ptr, bytes) != cudaSuccess) ok = false;
+  };
+  al(&p.master, sizeof(float) * kMlpParams);
+  al(&p.grad, sizeof(float) * kMlpParams);
+  al(&p.mom, sizeof(float) * kMlpParams);
+  al(&p.vel, sizeof(float) * kMlpParams);
+  al(&p.wb, sizeof(__nv_bfloat16) * kMlpWbElems);
+  al(&p.wt, sizeof(__nv_bfloat16) * kMlpWbElems);
+  al(&p.xb, sizeof(__nv_bfloat16) * B * kMlpK1);
+  for (int l = 0; l < 3; l++) {
+    al(&p.a[l], sizeof(__nv_bfloat16) * B * W);
+    al(&p.z[l], sizeof(float) * B * W);
+  }
+  al(&p.dyb, sizeof(__nv_bfloat16) * B * kMlpOutPad);
+  al(&p.dzb, sizeof(__nv_bfloat16) * B * W);
+  al(&p.dzt, sizeof(__nv_bfloat16) * B * W);
+  al(&p.at, sizeof(__nv_bfloat16) * B * W);
+  al(&p.tb, sizeof(float) * B * kMlpOut);
+  al(&p.y, sizeof(float) * B * kMlpOutPad);
+  al(&p.dy, sizeof(float) * B * kMlpOutPad);
+  al(&p.dz, sizeof(float) * B * W);
+  al(&p.da, sizeof(float) * B * W);
+  al(&p.b4pad, sizeof(float) * kMlpOutPad);
+  if (ok) ok = cudaMemcpy(p.master, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice) == cudaSuccess;
+  if (ok) ok = cudaMemset(p.mom, 0, sizeof(float) * kMlpParams) == cudaSuccess &&
+               cudaMemset(p.vel, 0, sizeof(float) * kMlpParams) == cudaSuccess &&
+               cudaMemset(p.grad, 0, sizeof(float) * kMlpParams) == cudaSuccess;
+  if (ok) {
+    launch_mlp_pack(p, g.stream);
+    ok = cudaStreamSynchronize(g.stream) == cudaSuccess;
+  }
+  if (!ok) {
+    mlp_free(h);
+    return fail(CUBE_ERR_CUDA);
+  }
+  *out = h;
+  return CUBE_OK;
+}
+
+int cube_mlp_destroy(cube_mlp *h) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!h) return CUBE_OK;
+  cudaSetDevice(h->p.device);
+  cudaDeviceSynchronize();
+  mlp_free(h);
+  return CUBE_OK;
+}
+
+int cube_mlp_get_params(cube_mlp *h, float *params, float *grads) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!h || (!params && !grads)) return fail(CUBE_ERR_INVALID);
+  CU(cudaSetDevice(h->p.device));
+  CU(cudaDeviceSynchronize());
+  if (params) CU(cudaMemcpy(params, h->p.master, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost));
+  if (grads) CU(cudaMemcpy(grads, h->p.grad, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost));
+  return CUBE_OK;
+}
+
+// positions of the stored copies and the fine-grid density of the image, on stream s
+static int mlp_prepare(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
+                       cudaStream_t s) {
+  const Lay &L = g.L;
+  if (L.pm3_mode != CUBE_PM3_PERIODIC) return fail(CUBE_ERR_INVALID);  // one periodic image
+  CK(grow(g.cell_base, sizeof(int64_t) * (size_t)L.ntile * L.nte * L.nte * L.nte));
+  CK(grow(g.mlp_pos, sizeof(float4) * (size_t)std::max<int64_t>(n_used, 1)));
+  CK(grow(g.mlp_rho, sizeof(float) * (size_t)L.ng * L.ng * L.ng));
+  launch_cell_table(L, d_rhoc, d_idx_b_r, (int64_t *)g.cell_base.p, s);
+  launch_mlp_pos(L, d_xp, d_rhoc, (const int64_t *)g.cell_base.p, (float4 *)g.mlp_pos.p, s);
+  launch_mlp_density((const float4 *)g.mlp_pos.p, n_used, L.ng, (float *)g.mlp_rho.p, s);
+  g.launches += 3;
+  CU(cudaGetLastError());
+  return CUBE_OK;
+}
+
+int cube_mlp_features(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
+                      void *d_X, void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!d_rhoc || !d_idx_b_r || !d_xp || !d_X || n_used < 0) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  cudaStream_t s = stream ? (cudaStream_t)stream : g.stream;
+  CK(mlp_prepare(d_rhoc, d_idx_b_r, d_xp, n_used, s));
+  launch_mlp_features((const float4 *)g.mlp_pos.p, n_used, (const float *)g.mlp_rho.p, g.L.ng,
+                      (__nv_bfloat16 *)d_X, s);
+  g.launches += 1;
+  CU(cudaGetLastError());
+  return CUBE_OK;
+}
+
+int cube_mlp_train_step(cube_mlp *h, const void *d_X, const float *d_T, const int32_t *d_rows, int32_t batch,
+                        float lr, float *d_loss, void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!h || !d_X || !d_T || !d_rows || !d_loss) return fail(CUBE_ERR_INVALID);
+  CU(cudaSetDevice(h->p.device));
+  const int st = mlp_train_step(h->p, (const __nv_bfloat16 *)d_X, d_T, d_rows, batch, lr, d_loss,
+                                stream ? (cudaStream_t)stream : g.stream);
+  return st == CUBE_OK ? CUBE_OK : fail(st);
+}
+
+int cube_mlp_forward(cube_mlp *h, const void *d_X, int64_t rows, float *d_Y, void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!h || !d_X || !d_Y || rows < 0) return fail(CUBE_ERR_INVALID);
+  CU(cudaSetDevice(h->p.device));
+  const int st = mlp_forward(h->p, (const __nv_bfloat16 *)d_X, rows, d_Y, stream ? (cudaStream_t)stream : g.stream);
+  return st == CUBE_OK ? CUBE_OK : fail(st);
+}
+
+int cube_mlp_kick(cube_mlp *h, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp,
+                  int64_t n_used, float *d_vp, float scale, float a_mid, float dt, void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!h || !d_rhoc || !d_idx_b_r || !d_xp || !d_vp || n_used < 0) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  cudaStream_t s = stream ? (cudaStream_t)stream : g.stream;
+  CK(mlp_prepare(d_rhoc, d_idx_b_r, d_xp, n_used, s));
+  // the kick coefficient of run_kick (kick.f90:529), times the network's output scale
+  const float kick = (float)((double)(a_mid * dt / 6.0f) / 3.14159265358979323846);
+  launch_mlp_apply(h->p, (const float4 *)g.mlp_pos.p, (const float *)g.mlp_rho.p, g.L.ng, n_used, d_vp,
+                   kick * scale, g.num_sms, s);
+  g.launches += 1;
+  CU(cudaGetLastError());
+  return CUBE_OK;
+}
+
 // A captured kick: the graph, its executable form, the pinned staging area its table uploads
 // read from, and the number of library kernels one replay launches.
 struct cube_kick_graph {
@@ -1209,6 +1368,8 @@ void c_pm3_fft_finalize(void) {
   release(g.rhok);
   release(g.force);
   release(g.jobs);
+  release(g.mlp_pos);
+  release(g.mlp_rho);
 }
 
 void c_gpu_velocity_finalize(void) {

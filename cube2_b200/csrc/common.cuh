@@ -1,6 +1,7 @@
 // Internal declarations shared by the kernels and the C-ABI layer.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cufft.h>
 #include <stdint.h>
@@ -59,6 +60,11 @@ __device__ __forceinline__ double decode_pos(int c, int16_t xp) {
 __device__ __forceinline__ void atomic_max_nonneg(float *addr, float v) {
   // non-negative floats order like their bit patterns
   atomicMax(reinterpret_cast<int *>(addr), __float_as_int(v));
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
 
 __device__ __forceinline__ float warp_max(float v) {
@@ -166,6 +172,42 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
                      const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp,
                      int64_t n_used, float *d_vp, float mass, float a_mid, float dt, float *d_out, cudaStream_t s);
 size_t noalloc_scratch_bytes();
+
+// Learned PP shell (mlp.cu).  FP32 master parameters, flat:
+// W1 [128][80] b1 [128] W2 [128][128] b2 [128] W3 [128][128] b3 [128] W4 [3][128] b4 [3].
+// BF16 copies per layer l: wb [Np][K] and their transposes wt [K][Np] (W4 padded to 16 rows).
+constexpr int kMlpIn = 67, kMlpK1 = 80, kMlpW = 128, kMlpOut = 3, kMlpOutPad = 16;
+__host__ __device__ constexpr int mlp_K(int l) { return l == 0 ? kMlpK1 : kMlpW; }
+__host__ __device__ constexpr int mlp_N(int l) { return l == 3 ? kMlpOut : kMlpW; }
+__host__ __device__ constexpr int mlp_Np(int l) { return l == 3 ? kMlpOutPad : kMlpW; }
+__host__ __device__ constexpr int mlp_woff(int l) {
+  return l == 0 ? 0 : mlp_woff(l - 1) + mlp_N(l - 1) * mlp_K(l - 1) + mlp_N(l - 1);
+}
+__host__ __device__ constexpr int mlp_boff(int l) { return mlp_woff(l) + mlp_N(l) * mlp_K(l); }
+__host__ __device__ constexpr int mlp_wboff(int l) { return l == 0 ? 0 : mlp_wboff(l - 1) + mlp_Np(l - 1) * mlp_K(l - 1); }
+constexpr int kMlpParams = mlp_boff(3) + kMlpOut;
+constexpr int kMlpWbElems = mlp_wboff(3) + kMlpOutPad * kMlpW;
+
+struct MlpParams {
+  float *master = nullptr, *grad = nullptr, *mom = nullptr, *vel = nullptr;  // [kMlpParams]
+  __nv_bfloat16 *wb = nullptr, *wt = nullptr;                                // [kMlpWbElems]
+  int step = 0;
+  int cap = 0;  // training batch capacity (rows)
+  // training scratch for cap rows
+  __nv_bfloat16 *xb = nullptr, *a[3] = {}, *dyb = nullptr, *dzb = nullptr, *dzt = nullptr, *at = nullptr;
+  float *tb = nullptr, *z[3] = {}, *y = nullptr, *dy = nullptr, *dz = nullptr, *da = nullptr, *b4pad = nullptr;
+  int device = -1;
+};
+void launch_mlp_pos(const Lay &L, const int16_t *xp, const int32_t *rhoc, const int64_t *cell_base, float4 *pos,
+                    cudaStream_t s);
+void launch_mlp_density(const float4 *pos, int64_t n, int ng, float *rho, cudaStream_t s);
+void launch_mlp_features(const float4 *pos, int64_t n, const float *rho, int ng, __nv_bfloat16 *X, cudaStream_t s);
+void launch_mlp_apply(const MlpParams &m, const float4 *pos, const float *rho, int ng, int64_t n, float *vp,
+                      float coef, int num_sms, cudaStream_t s);
+void launch_mlp_pack(MlpParams &m, cudaStream_t s);
+int mlp_train_step(MlpParams &m, const __nv_bfloat16 *X, const float *T, const int32_t *rows, int batch, float lr,
+                   float *loss, cudaStream_t s);
+int mlp_forward(MlpParams &m, const __nv_bfloat16 *X, int64_t nrows, float *Y, cudaStream_t s);
 
 // FP32 FMA throughput probe (5 launches); returns the time and the FLOPs executed
 cudaError_t fma_probe(cudaStream_t s, int num_sms, float *ms, double *flops);

@@ -54,7 +54,8 @@ EXPORTS = ("cube_set_layout", "cube_get_layout", "cube_last_error", "cube_error_
            "cube_kick_fine", "cube_kick_fine_device", "cube_pp_bin_tile", "cube_pp_pair_count", "cube_green_table",
            "cube_force_truth_fp64", "cube_stage_times", "cube_enable_timing", "cube_timing_read",
            "cube_launch_count", "cube_fp32_peak_probe", "cube_pp_force_noalloc", "cube_kick_graph_create",
-           "cube_kick_graph_launch", "cube_kick_graph_destroy")
+           "cube_kick_graph_launch", "cube_kick_graph_destroy", "cube_mlp_create", "cube_mlp_destroy",
+           "cube_mlp_get_params", "cube_mlp_features", "cube_mlp_train_step", "cube_mlp_forward", "cube_mlp_kick")
 
 
 def lib() -> ctypes.CDLL:

@@ -150,6 +150,39 @@ int cube_kick_graph_create(const int32_t *isort, const int32_t *ires, const int3
 int cube_kick_graph_launch(cube_kick_graph *graph, void *stream);
 int cube_kick_graph_destroy(cube_kick_graph *graph);
 
+/* ---- learned PP shell (no reference counterpart) ---- */
+
+/* A small MLP that predicts, per particle, the force that the cutoff-1 split (PM3
+ * softened at 1 fine cell plus PP within 1 fine cell) misses against the cutoff-2 split,
+ * from the CIC density of the image on the 4^3 fine cells around the particle (as
+ * log(1 + rho)) and the particle's offset in its cell: 67 inputs (padded to 80, BF16),
+ * layers 128, 128, 128 with tanh-GELU, 3 outputs; BF16 tensor-core GEMMs with FP32
+ * accumulation.  Parameters (FP32, flat, CUBE_MLP_PARAMS floats): W1 [128][80], b1 [128],
+ * W2 [128][128], b2 [128], W3 [128][128], b3 [128], W4 [3][128], b4 [3].  The single
+ * periodic image geometry (CUBE_PM3_PERIODIC) only. */
+#define CUBE_MLP_PARAMS 43779
+#define CUBE_MLP_INPUTS 80
+typedef struct cube_mlp cube_mlp;
+/* Upload the parameters; training steps take at most batch_cap rows (a multiple of 16). */
+int cube_mlp_create(const float *params, int32_t batch_cap, cube_mlp **mlp);
+int cube_mlp_destroy(cube_mlp *mlp);
+/* Current parameters and the gradients of the last training step (either may be NULL). */
+int cube_mlp_get_params(cube_mlp *mlp, float *params, float *grads);
+/* Input rows d_X (BF16 [n_used][80], zeros for buffer copies) of every stored copy of the
+ * image, in storage order (the training input). */
+int cube_mlp_features(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
+                      void *d_X, void *stream);
+/* One Adam step (lr, betas 0.9 / 0.999, eps 1e-8) on the rows d_rows[0..batch) of d_X with
+ * targets d_T [rows][3]: mean squared error, added to *d_loss. */
+int cube_mlp_train_step(cube_mlp *mlp, const void *d_X, const float *d_T, const int32_t *d_rows, int32_t batch,
+                        float lr, float *d_loss, void *stream);
+/* Outputs d_Y [rows][3] of the rows of d_X. */
+int cube_mlp_forward(cube_mlp *mlp, const void *d_X, int64_t rows, float *d_Y, void *stream);
+/* vp += a_mid*dt/(6 pi) * scale * MLP(inputs) for the interior copies of the image
+ * (inputs, density and network in one pass; the cutoff-1 kick itself is a separate call). */
+int cube_mlp_kick(cube_mlp *mlp, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp,
+                  int64_t n_used, float *d_vp, float scale, float a_mid, float dt, void *stream);
+
 /* ---- allocation-free PP kick ---- */
 
 /* Largest input cube_pp_force_noalloc accepts: stored particles (n_used) and
