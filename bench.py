@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-truth", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     return ap.parse_args()
 
 
@@ -279,6 +280,13 @@ def run_ours(args, rank, world, local_rank):
     loop = per_box_loop(args.workload, fk, img, stream, a_mid, dt, ms_step) if batch and rank == 0 else None
     if batch:
         fk.configure()
+    learned = None
+    if not batch and not args.no_learned and rank == 0:
+        try:
+            learned = learned_variant(args, img, (isort, ires, ix, apm3, rs), stream, truth, value, ms_step)
+        except Exception as e:  # reported beside the plain number, never instead of it
+            learned = {"error": repr(e)}
+        fk.configure()
 
     cpu = None
     if batch:
@@ -305,13 +313,101 @@ def run_ours(args, rank, world, local_rank):
             "stages_ms": {"pm3": pm3_ms, "pp_binning_and_worklist": ppb_ms, "pp_force": ppf_ms,
                           "note": "the PP binning and work list run on a second stream beside PM3"},
             "roofline": roofline, "force_error": truth, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": ck, "cpu_baseline": cpu, "graph": graph}
+            "clocks": ck, "cpu_baseline": cpu, "graph": graph, "learned": learned}
     if loop is not None:
         line["per_box_loop"] = loop
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+LEARNED_BOUND = 0.01  # rms force error bound of the learned shell against the FP64 truth
+
+
+def learned_variant(args, img, tables, stream, truth_plain, value_plain, ms_plain):
+    """The learned-shell kick on the same image: cutoff 1 (PM3 softened at 1 fine cell, PP
+    within 1 fine cell) plus the MLP, trained here on config-3-style boxes with the library's
+    own kernels.  Timed like the plain kick; its error against the FP64 truth is checked on the
+    same sampled particles, and above LEARNED_BOUND the kick falls back to the plain one."""
+    import torch
+    from cube2_b200 import ic
+    from cube2_b200 import learned as Ln
+    from cube2_b200 import workloads as W
+    from cube2_b200.kick import CUBE_PM3_PERIODIC, FineKick, force_truth_fp64
+    from cube2_b200.layout import RATIO_SF, Layout, apm3_table, build_image, ixyz3_table
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t0 = time.perf_counter()
+    # training data: three lognormal boxes (sigma 0.5, 1.0, 1.5; seeds 4001..4003), ~2.6M samples
+    Lt = Layout(ng=96, nnt=1, nns=2, ratio_cs=4, ngb=4, app=0.1)
+    tt = (np.arange(1, Lt.ns3 + 1, dtype=np.int32), np.full(Lt.ns3, 2, np.int32), ixyz3_table(Lt), None, RATIO_SF)
+    boxes = [build_image(*ic.lognormal_poisson(96, sg, seed)[:2], Lt) for sg, seed in ((0.5, 4001), (1.0, 4002),
+                                                                                       (1.5, 4003))]
+    X, T, scale = Ln.training_set(boxes, [tt] * 3, dev)
+    Xs, mu, sd = Ln.standardize(X, X.shape[0])
+    net = Ln.ShellNet(batch_cap=8192, seed=1)
+    steps = 6000
+    hist = Ln.train(net, Xs, T, steps=steps, batch=8192, lr=1e-3, log_every=1000)
+    shell = Ln.ShellNet(Ln.fold(net.params(), mu, sd), batch_cap=16)
+    net.close()
+    t_train = time.perf_counter() - t0
+    del X, Xs, T
+    # the learned kick on the bench image
+    L = img.layout
+    isort, ires, ix, _, rs = tables
+    fk1 = FineKick(L, pm3_mode=CUBE_PM3_PERIODIC, apm3f=Ln.SHORT.apm3f)
+    a1 = apm3_table(Ln.SHORT.apm3f)
+    rho, idx, xp, vp = Ln.device_image(img, dev)
+    vp0 = vp.clone()
+    out = torch.zeros(8, device=dev)
+    a_mid, dt = float(np.float32(6 * np.pi)), 1.0
+
+    def kick(with_shell=True):
+        fk1.kick_fine_device(rho, idx, xp, img.n_used, vp, out, isort, ires, ix, a1, rs, 1.0, a_mid, dt, stream=stream)
+        if with_shell:
+            shell.kick(rho, idx, xp, img.n_used, vp, scale, a_mid, dt, stream=stream)
+    for _ in range(max(args.warmup, 0)):
+        kick()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        kick()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    res = {"ms_per_step": ms, "value": img.n_particles / (ms * 1e-3), "unit": UNIT,
+           "speedup_vs_plain": ms_plain / ms, "pp_cutoff_fine_cells": Ln.SHORT.cutoff,
+           "train": {"samples": int(boxes[0].active.sum() + boxes[1].active.sum() + boxes[2].active.sum()),
+                     "steps": steps, "batch": 8192, "seconds": t_train, "loss": hist,
+                     "fields": "lognormal Poisson 96^3, sigma 0.5 / 1.0 / 1.5 (seeds 4001..4003)"}}
+    # errors against the FP64 truth on the plain run's sampled particles
+    if truth_plain is not None and not args.no_truth:
+        act = np.nonzero(img.active)[0]
+        rng = np.random.default_rng(12345)
+        samp = rng.choice(act, min(args.truth_targets, act.size), replace=False)
+        Ft = force_truth_fp64(W.physical_positions(img), float(L.ng), L.app, img.pid[samp])
+        kc = Ln.kick_coef(a_mid, dt)
+
+        def err(with_shell):
+            vp.copy_(vp0)
+            kick(with_shell)
+            torch.cuda.synchronize()
+            F = (vp - vp0).cpu().numpy().reshape(-1, 3).astype(np.float64)[samp] / kc
+            d = np.linalg.norm(F - Ft, axis=1)
+            m = np.linalg.norm(Ft, axis=1)
+            return float(np.sqrt(np.sum(d ** 2) / np.sum(m ** 2))), float(np.percentile(d / np.maximum(m, 1e-30), 99))
+        rms, p99 = err(True)
+        rms0, p990 = err(False)
+        res["force_error"] = {"rms_rel": rms, "p99_rel": p99, "targets": int(samp.size)}
+        res["force_error_cutoff1_without_shell"] = {"rms_rel": rms0, "p99_rel": p990}
+        res["bound"] = LEARNED_BOUND
+        res["fallback"] = bool(rms > LEARNED_BOUND)
+        res["note"] = ("the sampled error exceeds the bound: the kick falls back to the plain cutoff-2 kick, "
+                       "whose value is the line's value" if rms > LEARNED_BOUND else
+                       "within the bound: the learned kick stands")
+    shell.close()
+    return res
 
 
 def _batch_boxes(workload: str):

@@ -94,7 +94,8 @@ __global__ void k_mlp_cic(const float4 *pos, int64_t n, int ng, float *rho) {
   }
 }
 
-// the 67 inputs (padded to kMlpK1 with zeros) of the particle at q into out[0..kMlpK1)
+// the 67 inputs (padded to kMlpK1 with zeros) of the particle at q into out[0..kMlpK1); lrho holds
+// log(1 + rho) per fine cell
 __device__ __forceinline__ void mlp_inputs(float4 q, const float *__restrict__ rho, int ng, bf16 *out) {
   const float xs[3] = {q.x - 0.5f, q.y - 0.5f, q.z - 0.5f};
   int i0[3];
@@ -112,7 +113,7 @@ __device__ __forceinline__ void mlp_inputs(float4 q, const float *__restrict__ r
       const int64_t Y = wrap_cell(wrap_cell(i0[1] + dy, ng), ng);
       const float *row = rho + (Z * ng + Y) * ng;
 #pragma unroll
-      for (int dx = -1; dx <= 2; dx++) out[k++] = __float2bfloat16_rn(log1pf(__ldg(row + wrap_cell(i0[0] + dx, ng))));
+      for (int dx = -1; dx <= 2; dx++) out[k++] = __float2bfloat16_rn(__ldg(row + wrap_cell(i0[0] + dx, ng)));
     }
   }
   out[64] = __float2bfloat16_rn(f[0]);
@@ -149,14 +150,22 @@ __device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
+// tanh by the hardware approximation (tanh.approx.f32, relative error about 2^-11, below the
+// BF16 rounding of the activations); training and inference use the same function
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ float gelu_f(float z) {
   const float c = 0.7978845608028654f;  // sqrt(2/pi)
-  return 0.5f * z * (1.0f + tanhf(c * (z + 0.044715f * z * z * z)));
+  return 0.5f * z * (1.0f + tanh_hw(c * (z + 0.044715f * z * z * z)));
 }
 
 __device__ __forceinline__ float gelu_grad_f(float z) {
   const float c = 0.7978845608028654f;
-  const float t = tanhf(c * (z + 0.044715f * z * z * z));
+  const float t = tanh_hw(c * (z + 0.044715f * z * z * z));
   return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * c * (1.0f + 3.0f * 0.044715f * z * z);
 }
 
@@ -330,9 +339,10 @@ __global__ void k_mlp_pack(const float *master, bf16 *wb, bf16 *wt) {
 // fused inference + kick
 
 constexpr int kLd1 = kMlpK1 + 8, kLdW = kMlpW + 8;  // padded smem row strides (bf16)
+constexpr int kApplyWarps = 10;                     // 94 KB of weights + 11.5 KB per warp
 constexpr size_t kApplySmem = sizeof(bf16) * ((size_t)kMlpW * kLd1 + 2 * (size_t)kMlpW * kLdW + 8 * (size_t)kLdW) +
                               sizeof(float) * (3 * kMlpW + 8) +
-                              sizeof(bf16) * (size_t)kWarps * 16 * (kLd1 + 2 * kLdW);
+                              sizeof(bf16) * (size_t)kApplyWarps * 16 * (kLd1 + 2 * kLdW);
 
 struct MlpApplyK {
   const bf16 *wb;
@@ -385,7 +395,7 @@ __device__ __forceinline__ void warp_layer(const bf16 *in, int ldi, const bf16 *
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(kWarps * 32, 1) k_mlp_apply(MlpApplyK p) {
+__global__ void __launch_bounds__(kApplyWarps * 32, 1) k_mlp_apply(MlpApplyK p) {
   extern __shared__ __align__(16) unsigned char mlp_smem[];
   bf16 *w1 = reinterpret_cast<bf16 *>(mlp_smem);
   bf16 *w2 = w1 + kMlpW * kLd1;
@@ -411,7 +421,8 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_mlp_apply(MlpApplyK p) {
 
   const int g = lane >> 2, t = lane & 3;
   const int64_t ntiles = (p.n + 15) / 16;
-  for (int64_t tile = (int64_t)blockIdx.x * kWarps + warp; tile < ntiles; tile += (int64_t)gridDim.x * kWarps) {
+  for (int64_t tile = (int64_t)blockIdx.x * kApplyWarps + warp; tile < ntiles;
+       tile += (int64_t)gridDim.x * kApplyWarps) {
     const int64_t r0 = tile * 16;
     // inputs of the 16 rows: two lanes per row, 40 inputs each
     {
@@ -475,9 +486,16 @@ void launch_mlp_pos(const Lay &L, const int16_t *xp, const int32_t *rhoc, const 
   k_mlp_pos<<<(unsigned)((p.ncells + kWarps - 1) / kWarps), kWarps * 32, 0, s>>>(p);
 }
 
+// the network reads log(1 + rho): transformed once per cell rather than per stencil read
+__global__ void k_mlp_log1p(float *rho, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    rho[i] = log1pf(rho[i]);
+}
+
 void launch_mlp_density(const float4 *pos, int64_t n, int ng, float *rho, cudaStream_t s) {
   cudaMemsetAsync(rho, 0, sizeof(float) * (size_t)ng * ng * ng, s);
   k_mlp_cic<<<148 * 8, 256, 0, s>>>(pos, n, ng, rho);
+  k_mlp_log1p<<<148 * 8, 256, 0, s>>>(rho, (int64_t)ng * ng * ng);
 }
 
 void launch_mlp_features(const float4 *pos, int64_t n, const float *rho, int ng, bf16 *X, cudaStream_t s) {
@@ -498,7 +516,7 @@ void launch_mlp_apply(const MlpParams &m, const float4 *pos, const float *rho, i
     attr = true;
   }
   MlpApplyK p{m.wb, m.master, pos, rho, ng, n, vp, coef};
-  k_mlp_apply<<<num_sms, kWarps * 32, kApplySmem, s>>>(p);
+  k_mlp_apply<<<num_sms, kApplyWarps * 32, kApplySmem, s>>>(p);
 }
 
 // Forward + backward + Adam on one batch of `batch` rows picked by `rows` from X / T.

@@ -212,14 +212,17 @@ def train(net: ShellNet, X, T, steps: int, batch: int = 4096, lr: float = 1e-3, 
     n = X.shape[0] if holdout is None else holdout
     loss = torch.zeros(1, device=dev)
     hist = []
+    since = 0
     for k in range(steps):
         rows = torch.randint(0, n, (batch,), generator=g, dtype=torch.int32).to(dev)
         lr_k = 0.5 * lr * (1.0 + np.cos(np.pi * k / max(steps, 1)))
-        loss.zero_()
-        net.train_step(X, T, rows, batch, lr_k, loss, stream)
-        if log_every and (k % log_every == 0 or k == steps - 1):
+        net.train_step(X, T, rows, batch, lr_k, loss, stream)  # adds this batch's mean loss
+        since += 1
+        if log_every and ((k + 1) % log_every == 0 or k == steps - 1):
             torch.cuda.synchronize()
-            hist.append((k, float(loss.item())))
+            hist.append((k + 1, float(loss.item()) / since))  # mean batch loss since the last entry
+            loss.zero_()
+            since = 0
     torch.cuda.synchronize()
     return hist
 
