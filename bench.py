@@ -60,6 +60,17 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The maximum of x over the ranks (each rank's device time; the job ends with the slowest)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
         os.environ.get("LOCAL_RANK", "0"))
@@ -185,10 +196,7 @@ def run_ours(args, rank, world, local_rank):
     launches = fk.launch_count() - launches0
     stages = fk.timing_read()
     fk.enable_timing(False)
-    if world > 1:
-        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, world, dev)
     ms_step = ms / max(args.steps, 1)
     value = N * world * args.steps / (ms * 1e-3)
 
@@ -230,10 +238,7 @@ def run_ours(args, rank, world, local_rank):
         for _ in range(args.steps):
             fk.kick_fine(himg, isort, ires, ix, apm3, rs, 1.0, a_mid, dt, vp=vp_host)
         te = time.perf_counter() - te
-        if world > 1:
-            tt = torch.tensor([te], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te = max_over_ranks(te, world, dev)
         h2d = img.xp.nbytes + img.vp.nbytes + img.rhoc.nbytes + img.idx_b_r.nbytes
         d2h = img.vp.nbytes + 24
         e2e = {"value": N * world * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
