@@ -200,6 +200,13 @@ def run_ours(args, rank, world, local_rank):
     ms_step = ms / max(args.steps, 1)
     value = N * world * args.steps / (ms * 1e-3)
 
+    # the PP kernel shape the autotuner picked during the warm-up (cube_pp_shapes)
+    from cube2_b200.kick import pp_shapes
+    table, cur = pp_shapes()
+    pp_shape = {**{k: table[cur][k] for k in ("chunk", "jtile", "unroll", "blocks")}, "index": cur,
+                "tuning_ms": [round(float(t["ms"]), 3) for t in table],
+                "what": "autotuned on the first kick: work list + PP force kernel timed per shape"}
+
     # the same kick replayed as one captured CUDA graph (cube_kick_graph_*)
     graph = None
     try:
@@ -318,7 +325,7 @@ def run_ours(args, rank, world, local_rank):
             "stages_ms": {"pm3": pm3_ms, "pp_binning_and_worklist": ppb_ms, "pp_force": ppf_ms,
                           "note": "the PP binning and work list run on a second stream beside PM3"},
             "roofline": roofline, "force_error": truth, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": ck, "cpu_baseline": cpu, "graph": graph, "learned": learned}
+            "clocks": ck, "cpu_baseline": cpu, "graph": graph, "pp_shape": pp_shape, "learned": learned}
     if loop is not None:
         line["per_box_loop"] = loop
     if rank == 0:

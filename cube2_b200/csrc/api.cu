@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "common.cuh"
@@ -80,6 +81,14 @@ struct Ctx {
   Buf tiles, count, cell_start, scan_tmp, spos, spill, spill_rank, counters, items, range_loc, sched;
   Buf rho, rhok, force, jobs, out;
   Buf mlp_pos, mlp_rho;  // learned shell: positions of the stored copies, fine-grid CIC density
+  // PP kernel shape: fixed (pp_fixed >= 0, cube_pp_set_shape) or autotuned, keyed by
+  // pp_shape_key; pp_ms holds the last tuning's times, pp_last the shape of the last PP kick
+  int pp_fixed = -1;
+  std::unordered_map<uint64_t, int> pp_tuned;
+  float pp_ms[kMaxPPShapes] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+  int pp_last = 0;
+  Buf pp_scratch;  // tuning runs kick these velocities, not the caller's
+  cudaEvent_t tune_ev[2 * kMaxPPShapes] = {};
   void *h_stage = nullptr;  // pinned staging for small tables
   size_t h_stage_cap = 0;
   float *h_out = nullptr;   // pinned [8]: out[5], err
@@ -606,6 +615,86 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
   return CUBE_OK;
 }
 
+static void fnv_mix(uint64_t &h, const void *data, size_t n) {
+  const unsigned char *b = (const unsigned char *)data;
+  for (size_t i = 0; i < n; i++) h = (h ^ b[i]) * 1099511628211ull;
+}
+
+// What the fastest PP shape depends on: the layout's PP geometry, the per-tile PP grids, the PP
+// ranges by subtile and the octave of the stored-particle count.
+static uint64_t pp_shape_key(const Meta &m, int64_t n_used) {
+  uint64_t h = 1469598103934665603ull;
+  const int geo[6] = {g.L.ng, g.L.nnt, g.L.nns, g.L.rcs, g.L.ngb, 0};
+  fnv_mix(h, geo, sizeof(geo));
+  fnv_mix(h, &g.L.app, sizeof(float));
+  for (const TilePP &t : m.tiles) fnv_mix(h, &t.rcp, sizeof(int));
+  fnv_mix(h, m.range_loc.data(), sizeof(float) * m.range_loc.size());
+  int octave = 0;
+  while (octave < 63 && (n_used >> octave) > 1) octave++;
+  fnv_mix(h, &octave, sizeof(int));
+  return h;
+}
+
+// PP kernel shape for this kick (p.shape).  A fixed shape is used as is.  Otherwise the shape is
+// looked up by pp_shape_key; on a miss every shape is timed on this kick's own binned particles
+// (work list + force kernel, kicking scratch velocities), twice, and the fastest by the better of
+// its two times is kept.  The binning has been enqueued on `st` already; the host waits for the
+// timings, once per key.  A kick being captured into a graph cannot wait and uses shape 0.
+static int choose_pp_shape(const Meta &m, int64_t n_used, PPArgs &p, cudaStream_t st) {
+  if (g.pp_fixed >= 0) {
+    p.shape = g.pp_last = g.pp_fixed;
+    return CUBE_OK;
+  }
+  const uint64_t key = pp_shape_key(m, n_used);
+  auto hit = g.pp_tuned.find(key);
+  if (hit != g.pp_tuned.end()) {
+    p.shape = g.pp_last = hit->second;
+    return CUBE_OK;
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CU(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    p.shape = g.pp_last = 0;
+    return CUBE_OK;
+  }
+  const int ns = pp_num_shapes();
+  for (int k = 0; k < 2 * ns; k++)
+    if (!g.tune_ev[k]) CU(cudaEventCreate(&g.tune_ev[k]));
+  const size_t nv = 3 * (size_t)std::max<int64_t>(n_used, 1);
+  CK(grow(g.pp_scratch, sizeof(float) * (nv + 8)));
+  CU(cudaMemsetAsync(g.pp_scratch.p, 0, sizeof(float) * (nv + 8), st));
+  PPArgs q = p;
+  q.vp = (float *)g.pp_scratch.p;
+  q.out = q.vp + nv;
+  float best[kMaxPPShapes];
+  for (int k = 0; k < ns; k++) best[k] = 3.0e38f;
+  for (int rep = 0; rep < 2; rep++) {
+    for (int k = 0; k < ns; k++) {
+      q.shape = k;
+      CU(cudaEventRecord(g.tune_ev[2 * k], st));
+      launch_pp_items(q, st);
+      launch_pp_force(q, st);
+      CU(cudaEventRecord(g.tune_ev[2 * k + 1], st));
+    }
+    CU(cudaGetLastError());
+    g.launches += 4 * ns;
+    CU(cudaEventSynchronize(g.tune_ev[2 * ns - 1]));
+    for (int k = 0; k < ns; k++) {
+      float ms = 0;
+      CU(cudaEventElapsedTime(&ms, g.tune_ev[2 * k], g.tune_ev[2 * k + 1]));
+      best[k] = std::min(best[k], ms);
+    }
+  }
+  int pick = 0;
+  for (int k = 0; k < ns; k++) {
+    g.pp_ms[k] = best[k];
+    if (best[k] < best[pick]) pick = k;
+  }
+  g.pp_tuned[key] = pick;
+  p.shape = g.pp_last = pick;
+  return CUBE_OK;
+}
+
 // PP binning and work list on stream `st`; fills the arguments of the force kernel.  With
 // `pairs` non-null the force kernel will only count accepted pairs and leave vp untouched.
 static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size_t &soff, PPArgs &p,
@@ -622,7 +711,7 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   CK(grow(g.spill_rank, sizeof(int32_t) * spill_cap));
   int64_t interior = 0;
   for (auto &t : m.tiles) interior += (int64_t)L.nt * t.rcp * L.nt * t.rcp * L.nt * t.rcp;
-  const int64_t item_cap = interior + d.n_used / kPPChunk + 16;
+  const int64_t item_cap = interior + d.n_used / pp_min_chunk() + 16;
   CK(grow(g.items, sizeof(int4) * (size_t)item_cap));
   CK(grow(g.sched, sizeof(int32_t) * sched_ints(L.ntile)));
   int32_t *ctr = (int32_t *)g.counters.p;  // [0] spill_n [2] err
@@ -669,8 +758,10 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   p.err = ctr + 2;
   p.num_sms = g.num_sms;
   p.pairs = pairs;
+  p.shape = 0;
+  if (!pairs) CK(choose_pp_shape(m, d.n_used, p, st));
   launch_pp_items(p, st);
-  g.launches += 2;
+  g.launches += 3;
   CU(cudaGetLastError());
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][6], st));
   return CUBE_OK;
@@ -954,6 +1045,31 @@ int cube_set_layout(const cube_layout *l) {
   g.pub = *l;
   g.configured = true;
   t_last_error = CUBE_OK;
+  return CUBE_OK;
+}
+
+int cube_pp_set_shape(int32_t shape) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (shape < -1 || shape >= pp_num_shapes()) return fail(CUBE_ERR_INVALID);
+  g.pp_fixed = shape;
+  if (shape < 0) g.pp_tuned.clear();
+  return CUBE_OK;
+}
+
+int cube_pp_shapes(cube_pp_shape_info *out, int32_t cap, int32_t *n_shapes, int32_t *current) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (cap < 0 || (cap > 0 && !out)) return fail(CUBE_ERR_INVALID);
+  const int ns = pp_num_shapes();
+  if (n_shapes) *n_shapes = ns;
+  if (current) *current = g.pp_last;
+  for (int k = 0; k < std::min<int>(cap, ns); k++) {
+    const PPShapeDesc d = pp_shape_desc(k);
+    out[k].chunk = d.chunk;
+    out[k].jtile = d.jtile;
+    out[k].unroll = d.unroll;
+    out[k].blocks = d.blocks;
+    out[k].ms = g.pp_ms[k];
+  }
   return CUBE_OK;
 }
 

@@ -46,7 +46,14 @@ struct MeshJob {
 };
 
 constexpr int kWarps = 8;  // warps per block in warp-per-cell kernels
-constexpr int kPPChunk = 8;  // i-particles per PP work item (a crowded PP cell is split into chunks)
+constexpr int kPPChunk = 16;  // i-particles per PP work item of the default shape (a crowded PP cell is split into chunks)
+
+// PP force kernel shape (pp.cu): i-particles per work item, staged candidates per warp, pair-loop
+// unroll, resident blocks per SM the registers are budgeted for
+struct PPShapeDesc {
+  int chunk, jtile, unroll, blocks;
+};
+constexpr int kMaxPPShapes = 16;
 
 // ---------------------------------------------------------------------------------------------
 // device helpers
@@ -128,8 +135,13 @@ struct PPArgs {
   int32_t *err;
   int num_sms;
   unsigned long long *pairs;  // non-null: count accepted pairs instead of kicking
+  int shape;                  // kernel shape index (pp_shape_desc); 0 with `pairs`
 };
 size_t sched_ints(int ntile);
+int pp_num_shapes();
+PPShapeDesc pp_shape_desc(int i);
+int pp_min_chunk();  // smallest chunk of any shape: the work list capacity is sized for it
+// work list for the shape a.shape (shape 0 with a.pairs)
 void launch_pp_items(const PPArgs &a, cudaStream_t s);
 // force kernel over the items of tiles [t_lo, t_hi) (t_hi < 0: all tiles); each single tile and
 // the full range have their own queue head, so per-tile launches may run on several streams

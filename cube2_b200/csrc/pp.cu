@@ -2,7 +2,7 @@
 // (pp_force_kernel.c:282-325, pp_force_kernel.cu:192-250) and the kick of the
 // interior particles (pp_force_kernel.c:339-364).
 //
-// Work decomposition.  An item is one interior PP cell, or a kPPChunk-particle
+// Work decomposition.  An item is one interior PP cell, or a C-particle
 // chunk of a crowded one (the kick's binning orders a cell's particles by
 // Morton sub-cell, so a chunk occupies a compact sub-volume).  A particle of
 // range rc needs the cells within R = ceil(rc * rcp / ratio_cs) of its own
@@ -26,22 +26,38 @@
 // Kahan-compensated sums updated once per flush of the staging buffer; the
 // groups of a particle are merged with warp shuffles (TwoSum), and the owning
 // lane applies af*mass^2, the kick, f2max and vmax.
+#include <type_traits>
+#include <utility>
+
 #include "common.cuh"
 
 namespace cube {
 
 constexpr int kPPThreads = 256;
 constexpr int kPPWarps = kPPThreads / 32;
-constexpr int kJTile = 128;   // staged candidates per warp (+32 sentinel slots)
 constexpr int kMaxRows = 96;  // stencil rows per row table (a multiple of 32)
 constexpr int kBuckets = 32;
-#ifndef PP_UNROLL
-#define PP_UNROLL 2  // unroll factor of the pair-evaluation loop
-#endif
-constexpr int kPairUnroll = PP_UNROLL;
-static_assert(kJTile / (32 / kPPChunk) <= 32, "a flush has at most 32 rounds (one bit each)");
-constexpr size_t kPPSmemWarp = sizeof(float4) * (kJTile + 32) + sizeof(int2) * kMaxRows;
-constexpr size_t kPPSmem = kPPSmemWarp * kPPWarps;
+
+// Kernel shapes the autotuner picks from (the host times each on the kick's own particles):
+// chunk = i-particles per work item, so a crowded PP cell of n particles gets ceil(n / chunk)
+// warps; jtile = candidates a warp stages in shared memory between two flushes; unroll = unroll
+// factor of the pair loop; blocks = resident blocks per SM the registers are budgeted for
+// (4: 64 registers a thread, 3: 80).  Shape 0 is the default and the one the pair-count mode uses.
+constexpr PPShapeDesc kShapes[] = {{16, 64, 2, 4},  {8, 128, 1, 4},  {8, 128, 4, 4},  {4, 128, 2, 4},
+                                   {4, 256, 2, 4},  {8, 256, 2, 4},  {8, 128, 2, 4},  {16, 128, 2, 4},
+                                   {16, 128, 4, 4}, {8, 128, 2, 3},  {16, 128, 2, 3}, {16, 64, 1, 4},
+                                   {16, 64, 4, 4},  {16, 64, 2, 3},  {32, 64, 2, 4},  {32, 32, 2, 4}};
+constexpr int kNumShapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
+static_assert(kNumShapes <= kMaxPPShapes, "shape table");
+constexpr int min_shape_chunk() {
+  int c = kShapes[0].chunk;
+  for (int i = 1; i < kNumShapes; i++) c = kShapes[i].chunk < c ? kShapes[i].chunk : c;
+  return c;
+}
+constexpr int kMinChunk = min_shape_chunk();  // the work list capacity is sized for it
+static_assert(kShapes[0].chunk == kPPChunk, "shape 0 is the default shape");
+constexpr size_t pp_smem_warp(int jtile) { return sizeof(float4) * (jtile + 32) + sizeof(int2) * kMaxRows; }
+constexpr size_t pp_smem_block(int jtile) { return pp_smem_warp(jtile) * kPPWarps; }
 
 // basic_functions.f08:95-109 / pp_force_kernel.c:45-74 in FP32, same operation order
 __device__ __forceinline__ float F_ra(float r, float apm) {
@@ -128,6 +144,9 @@ struct DivTable {
 __constant__ DivTable c_div = DivTable();
 __device__ __forceinline__ int div_small(int n, int d) { return (n * c_div.m[d]) >> 20; }
 
+__device__ __forceinline__ int lowest_bit(unsigned m) { return __ffs(m) - 1; }
+__device__ __forceinline__ int lowest_bit(unsigned long long m) { return __ffsll(m) - 1; }
+
 __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   float y = x - c;
   float t = s + y;
@@ -201,7 +220,7 @@ __device__ __forceinline__ int cost_bucket(int ni, int64_t nj) {
 // pass 1 writes them tile by tile, heaviest bucket first inside a tile.  A cell's full chunks
 // share one bucket and its remainder chunk has another, so a thread reserves its slots with at
 // most two shared-memory atomics.
-template <int PASS>
+template <int PASS, int C>
 __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
   __shared__ int sc[kBuckets], sbase[kBuckets];
   const int t = blockIdx.y;
@@ -233,9 +252,9 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
           const int64_t b = g + ((int64_t)dz * S + dy) * S;
           nj += p.cs[b + Rc + 1] - p.cs[b - Rc];
         }
-      nfull = ni / kPPChunk;
-      bfull = cost_bucket(kPPChunk, nj);
-      if (ni % kPPChunk) brem = cost_bucket(ni % kPPChunk, nj);
+      nfull = ni / C;
+      bfull = cost_bucket(C, nj);
+      if (ni % C) brem = cost_bucket(ni % C, nj);
     }
   }
   int rfull = 0, rrem = 0;
@@ -287,12 +306,18 @@ __global__ void k_pp_offsets(int32_t *sched, int ntile) {
 
 // COUNT = false: forces and kick.  COUNT = true: only count the accepted ordered
 // pairs 0 < r^2 < rc^2 (the algorithmic work of the kick, for the roofline).
-template <bool COUNT>
-__global__ void __launch_bounds__(kPPThreads, 4) k_pp_force(PPK p) {
+// Shape: C i-particles per item, J staged candidates per flush, pair loop unrolled U times,
+// registers budgeted for B resident blocks per SM.
+template <bool COUNT, int C, int J, int U, int B>
+__global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
+  // a flush has at most J / floor(32 / C) rounds, one bit each in the soft-pair mask
+  constexpr int kRounds = J / (32 / C);
+  static_assert(kRounds <= 64, "at most 64 rounds per flush");
+  using Mask = typename std::conditional<(kRounds > 32), unsigned long long, unsigned>::type;
   extern __shared__ float4 pp_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float4 *buf = reinterpret_cast<float4 *>(reinterpret_cast<char *>(pp_smem) + warp * kPPSmemWarp);
-  int2 *rows = reinterpret_cast<int2 *>(buf + kJTile + 32);  // (end of the row in the walk, start - walk offset)
+  float4 *buf = reinterpret_cast<float4 *>(reinterpret_cast<char *>(pp_smem) + warp * pp_smem_warp(J));
+  int2 *rows = reinterpret_cast<int2 *>(buf + J + 32);  // (end of the row in the walk, start - walk offset)
   // items [first, last) of tiles [t_lo, t_hi), popped through this launch's own queue head
   const int32_t *tbase = p.sched + sched_base(p.ntile);
   const int first = tbase[p.t_lo];
@@ -317,8 +342,8 @@ __global__ void __launch_bounds__(kPPThreads, 4) k_pp_force(PPK p) {
     PairLaw law;
     law.init(rc, p.app);
 
-    const int i0 = p.cs[g] + item.y * kPPChunk;
-    const int ni = min(kPPChunk, p.cs[g + 1] - i0);
+    const int i0 = p.cs[g] + item.y * C;
+    const int ni = min(C, p.cs[g + 1] - i0);
     // lanes = ngrp groups of ni lanes; group `grp` walks every ngrp-th candidate
     const int ngrp = 32 / ni;
     const int grp = div_small(lane, ni), il = lane - grp * ni;
@@ -343,9 +368,9 @@ __global__ void __launch_bounds__(kPPThreads, 4) k_pp_force(PPK p) {
       __syncwarp();
       float px = 0.f, py = 0.f, pz = 0.f;
       const int nround = div_small(nbuf + ngrp - 1, ngrp);
-      unsigned softmask = 0u, bit = 1u;
+      Mask softmask = 0u, bit = 1u;
       const float4 *bp = buf + grp;
-#pragma unroll kPairUnroll
+#pragma unroll U
       for (int k = 0; k < nround; k++, bp += ngrp, bit <<= 1) {
         const float4 pj = *bp;
         const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
@@ -366,7 +391,7 @@ __global__ void __launch_bounds__(kPPThreads, 4) k_pp_force(PPK p) {
       if (!COUNT) {
         while (__any_sync(0xffffffffu, softmask != 0u)) {
           if (softmask) {
-            const int k = __ffs(softmask) - 1;
+            const int k = lowest_bit(softmask);
             softmask &= softmask - 1u;
             const float4 pj = buf[grp + k * ngrp];
             const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
@@ -435,7 +460,7 @@ __global__ void __launch_bounds__(kPPThreads, 4) k_pp_force(PPK p) {
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         if (keep) buf[nbuf + __popc(m & ((1u << lane) - 1u))] = pj;
         nbuf += __popc(m);
-        if (nbuf > kJTile - 32) flush();
+        if (nbuf > J - 32) flush();
       }
       __syncwarp();  // the next table overwrites this one
     }
@@ -522,27 +547,50 @@ static PPK make_ppk(const PPArgs &a) {
 
 size_t sched_ints(int ntile) { return (size_t)sched_base(ntile) + 2 * ((size_t)ntile + 1); }
 
+int pp_num_shapes() { return kNumShapes; }
+PPShapeDesc pp_shape_desc(int i) { return kShapes[i >= 0 && i < kNumShapes ? i : 0]; }
+int pp_min_chunk() { return kMinChunk; }
+
+template <int C>
+static void launch_items_c(const PPK &p, dim3 grid, cudaStream_t s, int32_t *sched, int ntile) {
+  k_pp_items<0, C><<<grid, 256, 0, s>>>(p);
+  k_pp_offsets<<<1, 32, 0, s>>>(sched, ntile);
+  k_pp_items<1, C><<<grid, 256, 0, s>>>(p);
+}
+
 void launch_pp_items(const PPArgs &a, cudaStream_t s) {
   PPK p = make_ppk(a);
   cudaMemsetAsync(a.sched, 0, sizeof(int32_t) * sched_ints(a.L->ntile), s);
   dim3 grid((unsigned)((p.max_cells + 255) / 256), (unsigned)a.L->ntile);
-  k_pp_items<0><<<grid, 256, 0, s>>>(p);
-  k_pp_offsets<<<1, 32, 0, s>>>(a.sched, a.L->ntile);
-  k_pp_items<1><<<grid, 256, 0, s>>>(p);
+  switch (pp_shape_desc(a.pairs ? 0 : a.shape).chunk) {
+    case 4: launch_items_c<4>(p, grid, s, a.sched, a.L->ntile); break;
+    case 16: launch_items_c<16>(p, grid, s, a.sched, a.L->ntile); break;
+    case 32: launch_items_c<32>(p, grid, s, a.sched, a.L->ntile); break;
+    default: launch_items_c<8>(p, grid, s, a.sched, a.L->ntile); break;
+  }
 }
 
-// one persistent block per resident slot: blocks beyond the resident count would
-// only start once the queue is empty
-static int resident_blocks(const void *fn, int num_sms) {
-  static int cached[2] = {0, 0};
-  const int which = fn == (const void *)k_pp_force<true> ? 1 : 0;
-  if (!cached[which]) {
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPPSmem);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPPThreads, kPPSmem);
-    cached[which] = per_sm > 0 ? per_sm : 1;
+// One persistent block per resident slot: blocks beyond the resident count would only start
+// once the queue is empty.  The count is looked up once per kernel (slot = shape, or the
+// pair-count kernel).
+template <bool COUNT, int S>
+static void launch_force_shape(const PPK &p, int num_sms, cudaStream_t s) {
+  constexpr PPShapeDesc d = kShapes[S];
+  constexpr size_t smem = pp_smem_block(d.jtile);
+  auto fn = k_pp_force<COUNT, d.chunk, d.jtile, d.unroll, d.blocks>;
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, (const void *)fn, kPPThreads, smem);
+    per_sm = n > 0 ? n : 1;
   }
-  return cached[which] * num_sms;
+  fn<<<per_sm * num_sms, kPPThreads, smem, s>>>(p);
+}
+
+template <int... I>
+static void launch_force_any(int shape, const PPK &p, int num_sms, cudaStream_t s, std::integer_sequence<int, I...>) {
+  ((shape == I ? launch_force_shape<false, I>(p, num_sms, s) : void()), ...);
 }
 
 void launch_pp_force(const PPArgs &a, cudaStream_t s, int t_lo, int t_hi) {
@@ -551,11 +599,10 @@ void launch_pp_force(const PPArgs &a, cudaStream_t s, int t_lo, int t_hi) {
   p.t_lo = t_lo;
   p.t_hi = t_hi;
   if (a.pairs) {
-    const void *fn = (const void *)k_pp_force<true>;
-    k_pp_force<true><<<resident_blocks(fn, a.num_sms), kPPThreads, kPPSmem, s>>>(p);
+    launch_force_shape<true, 0>(p, a.num_sms, s);  // the work list was built with shape 0
   } else {
-    const void *fn = (const void *)k_pp_force<false>;
-    k_pp_force<false><<<resident_blocks(fn, a.num_sms), kPPThreads, kPPSmem, s>>>(p);
+    const int shape = a.shape >= 0 && a.shape < kNumShapes ? a.shape : 0;
+    launch_force_any(shape, p, a.num_sms, s, std::make_integer_sequence<int, kNumShapes>{});
   }
 }
 

@@ -55,7 +55,8 @@ EXPORTS = ("cube_set_layout", "cube_get_layout", "cube_last_error", "cube_error_
            "cube_force_truth_fp64", "cube_stage_times", "cube_enable_timing", "cube_timing_read",
            "cube_launch_count", "cube_fp32_peak_probe", "cube_pp_force_noalloc", "cube_kick_graph_create",
            "cube_kick_graph_launch", "cube_kick_graph_destroy", "cube_mlp_create", "cube_mlp_destroy",
-           "cube_mlp_get_params", "cube_mlp_features", "cube_mlp_train_step", "cube_mlp_forward", "cube_mlp_kick")
+           "cube_mlp_get_params", "cube_mlp_features", "cube_mlp_train_step", "cube_mlp_forward", "cube_mlp_kick",
+           "cube_pp_set_shape", "cube_pp_shapes")
 
 
 def lib() -> ctypes.CDLL:
@@ -93,6 +94,27 @@ def _c32(a):
 
 def _f32(a):
     return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class CPPShape(ctypes.Structure):
+    _fields_ = [("chunk", ctypes.c_int32), ("jtile", ctypes.c_int32), ("unroll", ctypes.c_int32),
+                ("blocks", ctypes.c_int32), ("ms", ctypes.c_float)]
+
+
+def pp_set_shape(shape: int = -1):
+    """Use PP kernel shape `shape` for every PP kick, or autotune (-1, the default)."""
+    _check(lib().cube_pp_set_shape(ctypes.c_int32(shape)), "cube_pp_set_shape")
+
+
+def pp_shapes():
+    """(table, current): the PP kernel shapes as dicts (chunk, jtile, unroll, blocks, ms of the
+    last tuning or -1) and the index of the shape the last PP kick used."""
+    n, cur = ctypes.c_int32(), ctypes.c_int32()
+    _check(lib().cube_pp_shapes(None, 0, ctypes.byref(n), ctypes.byref(cur)), "cube_pp_shapes")
+    arr = (CPPShape * n.value)()
+    _check(lib().cube_pp_shapes(arr, n.value, None, None), "cube_pp_shapes")
+    table = [{k: getattr(e, k) for k, _ in CPPShape._fields_} for e in arr]
+    return table, cur.value
 
 
 class KickGraph:

@@ -150,6 +150,26 @@ int cube_kick_graph_create(const int32_t *isort, const int32_t *ires, const int3
 int cube_kick_graph_launch(cube_kick_graph *graph, void *stream);
 int cube_kick_graph_destroy(cube_kick_graph *graph);
 
+/* ---- PP kernel shape autotuner (no reference counterpart) ---- */
+
+/* The PP force kernel comes in several shapes: `chunk` i-particles per work item (a
+ * crowded PP cell of n particles is split into ceil(n / chunk) items, one warp each),
+ * `jtile` candidates a warp stages in shared memory between flushes, the pair loop
+ * unrolled `unroll` times, registers budgeted for `blocks` resident blocks per SM.  By
+ * default the first PP kick of each (layout, per-tile PP grids, PP ranges, octave of
+ * n_used) times every shape on its own particles (work list + force kernel, into scratch
+ * velocities; the host waits for it once) and that key keeps the fastest; a kick being
+ * captured into a graph that meets an untimed key uses shape 0.  Results of different
+ * shapes differ only by FP32 summation order. */
+typedef struct cube_pp_shape_info {
+  int32_t chunk, jtile, unroll, blocks;
+  float ms; /* the last tuning's time of the shape (work list + force kernel), -1 if never timed */
+} cube_pp_shape_info;
+/* shape >= 0: use that shape for every PP kick; -1: autotune (default; forgets earlier picks). */
+int cube_pp_set_shape(int32_t shape);
+/* The shape table (up to `cap` entries), its size and the shape of the last PP kick. */
+int cube_pp_shapes(cube_pp_shape_info *out, int32_t cap, int32_t *n_shapes, int32_t *current);
+
 /* ---- learned PP shell (no reference counterpart) ---- */
 
 /* A small MLP that predicts, per particle, the force that the cutoff-1 split (PM3

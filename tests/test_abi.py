@@ -60,6 +60,19 @@ def test_layout_validation(cube_lib):
     assert (got.ng, got.nnt, got.nns, got.ngb, got.pm3_mode) == (32, 2, 2, 4, 1)
 
 
+def test_pp_shape_table_and_index_check(cube_lib):
+    """The PP kernel shape table is readable without a GPU; a shape index outside it is refused."""
+    from cube2_b200 import kick as K
+    table, cur = K.pp_shapes()
+    assert len(table) >= 8 and table[0]["chunk"] == 16 and 0 <= cur < len(table)
+    assert all(t["chunk"] in (4, 8, 16, 32) and t["jtile"] % 32 == 0 and t["unroll"] >= 1 for t in table)
+    for bad in (-2, len(table)):
+        with pytest.raises(K.CubeError):
+            K.pp_set_shape(bad)
+    K.pp_set_shape(len(table) - 1)
+    K.pp_set_shape(-1)
+
+
 def _call_pp(fk, img, ires, ixyz3, idx_b_r=None, rhoc=None):
     from cube2_b200.kick import _p
     from cube2_b200.layout import RATIO_SF, apm3_table
