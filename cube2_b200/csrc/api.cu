@@ -88,6 +88,10 @@ struct Ctx {
   float pp_ms[kMaxPPShapes] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
   int pp_last = 0;
   Buf pp_scratch;  // tuning runs kick these velocities, not the caller's
+  // drift and buffer rebuild scratch
+  Buf dr_cb, dr_cb_new, dr_runrank, dr_run_base, dr_runs, dr_ctr, dr_dest_runs, dr_dest_start, dr_scan_tmp,
+      dr_cursor, dr_phys, dr_list, dr_off, dr_rows, dr_total;
+  Buf dh_rhoc, dh_idx, dh_xp, dh_vp, dh_pid, dh_rhoc2, dh_idx2, dh_xp2, dh_vp2, dh_pid2;  // host-array drift
   cudaEvent_t tune_ev[2 * kMaxPPShapes] = {};
   void *h_stage = nullptr;  // pinned staging for small tables
   size_t h_stage_cap = 0;
@@ -1186,6 +1190,190 @@ int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32
   }
   g.stream = own;
   return s;
+}
+
+// ---- drift and buffer rebuild ----
+
+// drift.f90:26 in float: nlayer = 2 * ceiling(dt_mid * vz_max / ratio_cs) + 2
+static int drift_nlayer(float dt_mid, float vz_max, int rcs, int *nlayer) {
+  volatile float prod = dt_mid * vz_max;
+  volatile float q = prod / (float)rcs;
+  if (!std::isfinite(q) || q < 0.0f || q > 1.0e6f) return fail(CUBE_ERR_INVALID);
+  *nlayer = 2 * (int)std::ceil(q) + 2;
+  return CUBE_OK;
+}
+
+// One drift of the image plus the rebuild of its buffers, device arrays, on stream st.
+static int drift_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, const float *d_vp,
+                        const int64_t *d_pid, int64_t n_used, float dt_mid, float vz_max, int32_t *d_rhoc_new,
+                        int64_t *d_idx_b_r_new, int16_t *d_xp_new, float *d_vp_new, int64_t *d_pid_new,
+                        int64_t cap_new, int64_t *n_used_new, int64_t *n_physical, cudaStream_t st) {
+  const Lay &L = g.L;
+  if (!d_rhoc || !d_idx_b_r || !d_rhoc_new || !d_idx_b_r_new || !n_used_new) return fail(CUBE_ERR_INVALID);
+  if (n_used < 0 || n_used >= ((int64_t)1 << 31) - 1 || cap_new < 0) return fail(CUBE_ERR_INVALID);
+  if (n_used > 0 && (!d_xp || !d_vp)) return fail(CUBE_ERR_INVALID);
+  if (cap_new > 0 && (!d_xp_new || !d_vp_new || (d_pid && !d_pid_new))) return fail(CUBE_ERR_INVALID);
+  const int64_t ncs = (int64_t)L.ntile * L.nte * L.nte * L.nte;
+  const int64_t ndest = (int64_t)L.nc * L.nc * L.nc;
+  const int64_t nrows = (int64_t)L.ntile * L.nte * L.nte;
+  if (ncs >= ((int64_t)1 << 31) || ndest >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
+  if (L.nt < L.ncb) return fail(CUBE_ERR_INVALID);  // a buffer mirrors at most one tile deep
+  int nlayer = 0;
+  CK(drift_nlayer(dt_mid, vz_max, L.rcs, &nlayer));
+  const int64_t run_cap = std::max<int64_t>(n_used, 1);
+  CK(grow(g.dr_cb, sizeof(int64_t) * ncs));
+  CK(grow(g.dr_cb_new, sizeof(int64_t) * ncs));
+  CK(grow(g.dr_runrank, sizeof(uint32_t) * run_cap));
+  CK(grow(g.dr_run_base, sizeof(int32_t) * ncs));
+  CK(grow(g.dr_runs, drift_run_bytes() * run_cap));
+  CK(grow(g.dr_ctr, sizeof(int32_t) * 8));
+  CK(grow(g.dr_dest_runs, sizeof(int32_t) * ndest));
+  CK(grow(g.dr_dest_start, sizeof(int32_t) * (ndest + 1)));
+  CK(grow(g.dr_scan_tmp, sizeof(int32_t) * scan_tmp_elems(ndest)));
+  CK(grow(g.dr_cursor, sizeof(int32_t) * ndest));
+  CK(grow(g.dr_phys, sizeof(int32_t) * ndest));
+  CK(grow(g.dr_list, sizeof(int32_t) * run_cap));
+  CK(grow(g.dr_off, sizeof(int64_t) * run_cap));
+  CK(grow(g.dr_rows, sizeof(int64_t) * nrows));
+  CK(grow(g.dr_total, sizeof(int64_t) * 2));
+  int32_t *ctr = (int32_t *)g.dr_ctr.p;
+  CU(cudaMemsetAsync(ctr, 0, sizeof(int32_t) * 8, st));
+  CU(cudaMemsetAsync(g.dr_dest_runs.p, 0, sizeof(int32_t) * ndest, st));
+  CU(cudaMemsetAsync(g.dr_phys.p, 0, sizeof(int32_t) * ndest, st));
+  CU(cudaMemsetAsync(g.dr_cursor.p, 0, sizeof(int32_t) * ndest, st));
+  launch_cell_table(L, d_rhoc, d_idx_b_r, (int64_t *)g.dr_cb.p, st);
+  DriftArgs a{};
+  a.L = &g.L;
+  a.nlayer = nlayer;
+  a.dt_mid = dt_mid;
+  a.num_sms = g.num_sms;
+  a.n_used = n_used;
+  a.rhoc = d_rhoc;
+  a.cell_base = (const int64_t *)g.dr_cb.p;
+  a.xp = d_xp;
+  a.vp = d_vp;
+  a.pid = d_pid;
+  a.runrank = (uint32_t *)g.dr_runrank.p;
+  a.run_base = (int32_t *)g.dr_run_base.p;
+  a.runs = g.dr_runs.p;
+  a.run_cap = (int32_t)run_cap;
+  a.ctr = ctr;
+  a.dest_runs = (int32_t *)g.dr_dest_runs.p;
+  a.phys_count = (int32_t *)g.dr_phys.p;
+  a.err = ctr + 4;
+  a.dest_start = (int32_t *)g.dr_dest_start.p;
+  a.cursor = (int32_t *)g.dr_cursor.p;
+  a.run_list = (int32_t *)g.dr_list.p;
+  a.run_off = (int64_t *)g.dr_off.p;
+  a.rhoc_new = d_rhoc_new;
+  a.cell_base_new = (const int64_t *)g.dr_cb_new.p;
+  a.xp_new = d_xp_new;
+  a.vp_new = d_vp_new;
+  a.pid_new = d_pid ? d_pid_new : nullptr;
+  launch_drift_runs(a, st);
+  launch_drift_spine(a, d_rhoc_new, (int64_t *)g.dr_rows.p, d_idx_b_r_new, (int64_t *)g.dr_total.p, st);
+  launch_cell_table(L, d_rhoc_new, d_idx_b_r_new, (int64_t *)g.dr_cb_new.p, st);
+  g.launches += 6;
+  CU(cudaGetLastError());
+  // the new sizes decide whether the outputs fit: one host synchronisation
+  int32_t h_ctr[8];
+  int64_t h_total = 0;
+  CU(cudaMemcpyAsync(h_ctr, ctr, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(&h_total, g.dr_total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  *n_used_new = h_total;
+  if (n_physical) *n_physical = h_ctr[1];
+  if (h_ctr[4] & (1 << CUBE_ERR_CAPACITY)) return fail(CUBE_ERR_CAPACITY);
+  if (h_ctr[4]) return fail(CUBE_ERR_INVALID);
+  if (h_total > cap_new || h_total >= ((int64_t)1 << 31)) return fail(CUBE_ERR_CAPACITY);
+  a.n_used_new = h_total;
+  launch_drift_place(a, h_ctr[0], (int32_t *)g.dr_scan_tmp.p, st);
+  g.launches += 7;
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(&h_ctr[4], ctr + 4, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  if (h_ctr[4]) return fail(CUBE_ERR_INVALID);
+  return CUBE_OK;
+}
+
+int cube_drift_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, const float *d_vp,
+                      const int64_t *d_pid, int64_t n_used, float dt_mid, float vz_max, int32_t *d_rhoc_new,
+                      int64_t *d_idx_b_r_new, int16_t *d_xp_new, float *d_vp_new, int64_t *d_pid_new,
+                      int64_t cap_new, int64_t *n_used_new, int64_t *n_physical, void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  CK(ensure_device());
+  return drift_device(d_rhoc, d_idx_b_r, d_xp, d_vp, d_pid, n_used, dt_mid, vz_max, d_rhoc_new, d_idx_b_r_new,
+                      d_xp_new, d_vp_new, d_pid_new, cap_new, n_used_new, n_physical,
+                      stream ? (cudaStream_t)stream : g.stream);
+}
+
+int cube_buffer_v_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, float *d_vp, int64_t n_used,
+                         void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!d_rhoc || !d_idx_b_r || (n_used > 0 && !d_vp) || n_used < 0) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  const Lay &L = g.L;
+  cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
+  CK(grow(g.dr_cb, sizeof(int64_t) * (size_t)L.ntile * L.nte * L.nte * L.nte));
+  launch_cell_table(L, d_rhoc, d_idx_b_r, (int64_t *)g.dr_cb.p, st);
+  launch_halo_velocities(L, d_rhoc, (const int64_t *)g.dr_cb.p, d_vp, n_used, g.num_sms, st);
+  g.launches += 2;
+  CU(cudaGetLastError());
+  return CUBE_OK;
+}
+
+int cube_drift(int32_t *rhoc, int64_t *idx_b_r, int16_t *xp, float *vp, int64_t *pid, int64_t n_used,
+               int64_t capacity, float dt_mid, float vz_max, int64_t *n_used_new, int64_t *n_physical) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!rhoc || !idx_b_r || !n_used_new || n_used < 0 || capacity < n_used) return fail(CUBE_ERR_INVALID);
+  if (n_used > 0 && (!xp || !vp)) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  const Lay &L = g.L;
+  const size_t ncs = (size_t)L.ntile * L.nte * L.nte * L.nte, nrows = (size_t)L.ntile * L.nte * L.nte;
+  const size_t nin = (size_t)std::max<int64_t>(n_used, 1), nout = (size_t)std::max<int64_t>(capacity, 1);
+  CK(grow(g.dh_rhoc, sizeof(int32_t) * ncs));
+  CK(grow(g.dh_idx, sizeof(int64_t) * nrows));
+  CK(grow(g.dh_xp, sizeof(int16_t) * 3 * nin));
+  CK(grow(g.dh_vp, sizeof(float) * 3 * nin));
+  CK(grow(g.dh_rhoc2, sizeof(int32_t) * ncs));
+  CK(grow(g.dh_idx2, sizeof(int64_t) * nrows));
+  CK(grow(g.dh_xp2, sizeof(int16_t) * 3 * nout));
+  CK(grow(g.dh_vp2, sizeof(float) * 3 * nout));
+  if (pid) {
+    CK(grow(g.dh_pid, sizeof(int64_t) * nin));
+    CK(grow(g.dh_pid2, sizeof(int64_t) * nout));
+  }
+  cudaStream_t st = g.stream;
+  CU(cudaMemcpyAsync(g.dh_rhoc.p, rhoc, sizeof(int32_t) * ncs, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(g.dh_idx.p, idx_b_r, sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, st));
+  if (n_used > 0) {
+    CU(cudaMemcpyAsync(g.dh_xp.p, xp, sizeof(int16_t) * 3 * n_used, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(g.dh_vp.p, vp, sizeof(float) * 3 * n_used, cudaMemcpyHostToDevice, st));
+    if (pid) CU(cudaMemcpyAsync(g.dh_pid.p, pid, sizeof(int64_t) * n_used, cudaMemcpyHostToDevice, st));
+  }
+  int64_t n_new = 0;
+  const int s = drift_device((const int32_t *)g.dh_rhoc.p, (const int64_t *)g.dh_idx.p, (const int16_t *)g.dh_xp.p,
+                             (const float *)g.dh_vp.p, pid ? (const int64_t *)g.dh_pid.p : nullptr, n_used, dt_mid,
+                             vz_max, (int32_t *)g.dh_rhoc2.p, (int64_t *)g.dh_idx2.p, (int16_t *)g.dh_xp2.p,
+                             (float *)g.dh_vp2.p, pid ? (int64_t *)g.dh_pid2.p : nullptr, capacity, &n_new,
+                             n_physical, st);
+  *n_used_new = n_new;
+  if (s != CUBE_OK) return s;  // the host arrays are untouched
+  CU(cudaMemcpyAsync(rhoc, g.dh_rhoc2.p, sizeof(int32_t) * ncs, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(idx_b_r, g.dh_idx2.p, sizeof(int64_t) * nrows, cudaMemcpyDeviceToHost, st));
+  if (n_new > 0) {
+    CU(cudaMemcpyAsync(xp, g.dh_xp2.p, sizeof(int16_t) * 3 * n_new, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(vp, g.dh_vp2.p, sizeof(float) * 3 * n_new, cudaMemcpyDeviceToHost, st));
+    if (pid) CU(cudaMemcpyAsync(pid, g.dh_pid2.p, sizeof(int64_t) * n_new, cudaMemcpyDeviceToHost, st));
+  }
+  CU(cudaStreamSynchronize(st));
+  return CUBE_OK;
 }
 
 // ---- learned PP shell ----

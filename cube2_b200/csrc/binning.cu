@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_down(const int32_t *in, i
   if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = part[nb];
 }
 
-static void scan_exclusive(const int32_t *in, int64_t n, int32_t *out, int32_t *tmp, cudaStream_t s) {
+void scan_exclusive_i32(const int32_t *in, int64_t n, int32_t *out, int32_t *tmp, cudaStream_t s) {
   const int nb = (int)((n + kScanTile - 1) / kScanTile);
   k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, n, tmp);
   k_scan_top<<<1, kScanThreads, 0, s>>>(tmp, nb);
@@ -442,7 +442,7 @@ void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
   cudaMemsetAsync(a.spill_n, 0, sizeof(int32_t), s);
   k_pp_bin<false><<<blocks, kWarps * 32, shm, s>>>(p);
   k_spill_fix<<<1, 1024, 0, s>>>(a.spill, a.spill_rank, a.spill_n, p.spill_cap, a.count);
-  scan_exclusive(a.count, a.ncells, a.cell_start, a.scan_tmp, s);
+  scan_exclusive_i32(a.count, a.ncells, a.cell_start, a.scan_tmp, s);
   k_pp_bin<true><<<blocks, kWarps * 32, shm, s>>>(p);
   k_spill_place<<<8, 256, 0, s>>>(p);
 }

@@ -179,6 +179,50 @@ void launch_pm3_gather(const PM3Args &a, cudaStream_t s);
 void launch_green_fp64(int n, double apm_soft, double apm_range, double gridsize, int p_order, float *G,
                        cudaStream_t s);
 
+// exclusive scan of int32 counts (binning.cu): out[0..n] with out[n] = total; tmp has
+// scan_tmp_elems(n) entries
+void scan_exclusive_i32(const int32_t *in, int64_t n, int32_t *out, int32_t *tmp, cudaStream_t s);
+
+// Drift of one image and the rebuild of its buffers (drift.cu)
+struct DriftArgs {
+  const Lay *L;
+  int nlayer;            // drift.f90:26
+  float dt_mid;
+  int64_t n_used, n_used_new;  // stored copies of the current image and of the new one
+  int num_sms;
+  const int32_t *rhoc;   // current image
+  const int64_t *cell_base;
+  const int16_t *xp;
+  const float *vp;
+  const int64_t *pid;    // may be null
+  uint32_t *runrank;     // [n_used]
+  int32_t *run_base;     // [ntile * nte^3]
+  void *runs;            // [run_cap] records of drift_run_bytes()
+  int32_t run_cap;
+  int32_t *ctr;          // [2] zeroed: runs, kept particles
+  int32_t *dest_runs;    // [nc^3] zeroed
+  int32_t *phys_count;   // [nc^3] zeroed
+  int32_t *err;
+  int32_t *dest_start;   // [nc^3 + 1]
+  int32_t *cursor;       // [nc^3] zeroed
+  int32_t *run_list;     // [run_cap]
+  int64_t *run_off;      // [run_cap]
+  const int32_t *rhoc_new;   // new image (spine from launch_drift_spine)
+  const int64_t *cell_base_new;
+  int16_t *xp_new;
+  float *vp_new;
+  int64_t *pid_new;
+};
+size_t drift_run_bytes();
+void launch_drift_runs(const DriftArgs &a, cudaStream_t s);
+// new counts of every extended cell, row sums and the spine; *total = stored copies
+void launch_drift_spine(const DriftArgs &a, int32_t *rhoc_new, int64_t *rows, int64_t *idx_b_r_new,
+                        int64_t *total, cudaStream_t s);
+void launch_drift_place(const DriftArgs &a, int32_t nruns, int32_t *scan_tmp, cudaStream_t s);
+// buffer_v: every buffer copy takes the velocity of the physical particle it mirrors
+void launch_halo_velocities(const Lay &L, const int32_t *rhoc, const int64_t *cell_base, float *vp, int64_t n_used,
+                            int num_sms, cudaStream_t s);
+
 // PP kick with all scratch in a static device array (noalloc.cu)
 int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
                      const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp,

@@ -150,6 +150,32 @@ int cube_kick_graph_create(const int32_t *isort, const int32_t *ires, const int3
 int cube_kick_graph_launch(cube_kick_graph *graph, void *stream);
 int cube_kick_graph_destroy(cube_kick_graph *graph);
 
+/* ---- drift and buffer rebuild (drift.f90, buffer_grid.f90, buffer_particle.f90) ---- */
+
+/* One drift of the configured image followed by the rebuild of its periodic buffers:
+ * drift.f90:1-161 (new offsets xp + nint(dt_mid vp / (x_resolution ratio_cs)) with int16
+ * wrap, re-binning by ceiling(x + dt_mid vp / ratio_cs), compaction; the order inside a
+ * cell is the reference's layered visiting order with nlayer = 2 ceiling(dt_mid vz_max /
+ * ratio_cs) + 2) and then buffer_grid + buffer_x + buffer_v (main.f90:27-31 without the
+ * kick): every buffer cell receives the particles of the physical cell it mirrors, in
+ * order.  With CUBE_PM3_TILE_PERIODIC each tile is its own periodic box.  Inputs and
+ * outputs are distinct device arrays; pid (one int64 per stored copy) may be NULL.  The
+ * call waits for the new sizes: *n_used_new receives the stored copies of the new image
+ * (physical + buffers) and *n_physical (may be NULL) the physical particles.  Returns
+ * CUBE_ERR_CAPACITY, with only rhoc_new and idx_b_r_new written, when *n_used_new >
+ * cap_new; CUBE_ERR_INVALID for a non-finite nlayer or nint beyond the default integer. */
+int cube_drift_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, const float *d_vp,
+                      const int64_t *d_pid, int64_t n_used, float dt_mid, float vz_max, int32_t *d_rhoc_new,
+                      int64_t *d_idx_b_r_new, int16_t *d_xp_new, float *d_vp_new, int64_t *d_pid_new,
+                      int64_t cap_new, int64_t *n_used_new, int64_t *n_physical, void *stream);
+/* Same on host arrays, in place (the reference's own arrays, `capacity` stored copies). */
+int cube_drift(int32_t *rhoc, int64_t *idx_b_r, int16_t *xp, float *vp, int64_t *pid, int64_t n_used,
+               int64_t capacity, float dt_mid, float vz_max, int64_t *n_used_new, int64_t *n_physical);
+/* buffer_v (buffer_particle.f90:14-21): every buffer copy takes the velocity of the
+ * physical particle it mirrors, in place on device arrays; enqueued on `stream`. */
+int cube_buffer_v_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, float *d_vp, int64_t n_used,
+                         void *stream);
+
 /* ---- PP kernel shape autotuner (no reference counterpart) ---- */
 
 /* The PP force kernel comes in several shapes: `chunk` i-particles per work item (a
