@@ -292,6 +292,14 @@ def run_ours(args, rank, world, local_rank):
     loop = per_box_loop(args.workload, fk, img, stream, a_mid, dt, ms_step) if batch and rank == 0 else None
     if batch:
         fk.configure()
+    drift = None
+    if rank == 0:
+        try:
+            drift = drift_leg(img, CUBE_PM3_TILE_PERIODIC if batch else CUBE_PM3_PERIODIC, stream, args.steps,
+                              args.warmup)
+        except Exception as e:  # reported beside the kick, never instead of it
+            drift = {"error": repr(e)}
+        fk.configure()
     learned = None
     if not batch and not args.no_learned and rank == 0:
         try:
@@ -325,7 +333,7 @@ def run_ours(args, rank, world, local_rank):
             "stages_ms": {"pm3": pm3_ms, "pp_binning_and_worklist": ppb_ms, "pp_force": ppf_ms,
                           "note": "the PP binning and work list run on a second stream beside PM3"},
             "roofline": roofline, "force_error": truth, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": ck, "cpu_baseline": cpu, "graph": graph, "pp_shape": pp_shape, "learned": learned}
+            "clocks": ck, "cpu_baseline": cpu, "graph": graph, "pp_shape": pp_shape, "drift": drift, "learned": learned}
     if loop is not None:
         line["per_box_loop"] = loop
     if rank == 0:
@@ -335,6 +343,57 @@ def run_ours(args, rank, world, local_rank):
 
 
 LEARNED_BOUND = 0.01  # rms force error bound of the learned shell against the FP64 truth
+
+
+def measured_hbm_peak():
+    """(GB/s, source) of the HBM copy bandwidth measured on this pool's B200s."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s (of fallback)"
+
+
+DRIFT_BYTES_PER_COPY = 26  # xp 6 + vp 12 + pid 8 bytes per stored copy, read once and written once
+
+
+def drift_leg(img, pm3_mode, stream, steps, warmup):
+    """The other half of a time step on the bench image: drift + buffer rebuild
+    (cube_drift_device) and buffer_v (cube_buffer_v_device), timed with CUDA events.  Each drift
+    moves the fastest particle by 0.1 coarse cells."""
+    import torch
+    from cube2_b200.drift import DeviceImage
+    from cube2_b200.kick import FineKick
+    dev = torch.device("cuda", torch.cuda.current_device())
+    FineKick(img.layout, pm3_mode=pm3_mode).configure()
+    di = DeviceImage(img, dev)
+    vmax = float(np.abs(img.vp).max())
+    vz = float(np.abs(img.vp[:, 2]).max())
+    dt_mid = 0.1 * img.layout.ratio_cs / max(vmax, 1e-6)
+    n_in = di.n_used
+    for _ in range(max(warmup, 1)):
+        di.drift(dt_mid, vz, stream)
+        di.buffer_v(stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        di.drift(dt_mid, vz, stream)
+        di.buffer_v(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(steps, 1)
+    moved = DRIFT_BYTES_PER_COPY * (n_in + di.n_used)
+    peak, src = measured_hbm_peak()
+    gbs = moved / (ms * 1e-3) / 1e9
+    return {"ms_per_step": ms, "value": di.n_physical / (ms * 1e-3), "unit": "particle-drifts/s",
+            "stored_copies_in": int(n_in), "stored_copies_out": int(di.n_used), "physical": int(di.n_physical),
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "peak_source": src,
+                         "bytes": f"{DRIFT_BYTES_PER_COPY} B per stored copy read + written (xp, vp, pid)"},
+            "what": "drift + buffer_grid + buffer_x + buffer_v (cube_drift_device + cube_buffer_v_device), "
+                    "two host synchronisations per drift for the new sizes"}
 
 
 def learned_variant(args, img, tables, stream, truth_plain, value_plain, ms_plain):
