@@ -402,27 +402,12 @@ def learned_variant(args, img, tables, stream, truth_plain, value_plain, ms_plai
     own kernels.  Timed like the plain kick; its error against the FP64 truth is checked on the
     same sampled particles, and above LEARNED_BOUND the kick falls back to the plain one."""
     import torch
-    from cube2_b200 import ic
     from cube2_b200 import learned as Ln
     from cube2_b200 import workloads as W
     from cube2_b200.kick import CUBE_PM3_PERIODIC, FineKick, force_truth_fp64
-    from cube2_b200.layout import RATIO_SF, Layout, apm3_table, build_image, ixyz3_table
+    from cube2_b200.layout import apm3_table
     dev = torch.device("cuda", torch.cuda.current_device())
-    t0 = time.perf_counter()
-    # training data: three lognormal boxes (sigma 0.5, 1.0, 1.5; seeds 4001..4003), ~2.6M samples
-    Lt = Layout(ng=96, nnt=1, nns=2, ratio_cs=4, ngb=4, app=0.1)
-    tt = (np.arange(1, Lt.ns3 + 1, dtype=np.int32), np.full(Lt.ns3, 2, np.int32), ixyz3_table(Lt), None, RATIO_SF)
-    boxes = [build_image(*ic.lognormal_poisson(96, sg, seed)[:2], Lt) for sg, seed in ((0.5, 4001), (1.0, 4002),
-                                                                                       (1.5, 4003))]
-    X, T, scale = Ln.training_set(boxes, [tt] * 3, dev)
-    Xs, mu, sd = Ln.standardize(X, X.shape[0])
-    net = Ln.ShellNet(batch_cap=8192, seed=1)
-    steps = 6000
-    hist = Ln.train(net, Xs, T, steps=steps, batch=8192, lr=1e-3, log_every=1000)
-    shell = Ln.ShellNet(Ln.fold(net.params(), mu, sd), batch_cap=16)
-    net.close()
-    t_train = time.perf_counter() - t0
-    del X, Xs, T
+    shell, scale, tinfo = Ln.train_shell(dev)
     # the learned kick on the bench image
     L = img.layout
     isort, ires, ix, _, rs = tables
@@ -449,9 +434,7 @@ def learned_variant(args, img, tables, stream, truth_plain, value_plain, ms_plai
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
     res = {"ms_per_step": ms, "value": img.n_particles / (ms * 1e-3), "unit": UNIT,
            "speedup_vs_plain": ms_plain / ms, "pp_cutoff_fine_cells": Ln.SHORT.cutoff,
-           "train": {"samples": int(boxes[0].active.sum() + boxes[1].active.sum() + boxes[2].active.sum()),
-                     "steps": steps, "batch": 8192, "seconds": t_train, "loss": hist,
-                     "fields": "lognormal Poisson 96^3, sigma 0.5 / 1.0 / 1.5 (seeds 4001..4003)"}}
+           "train": tinfo}
     # errors against the FP64 truth on the plain run's sampled particles
     if truth_plain is not None and not args.no_truth:
         act = np.nonzero(img.active)[0]
@@ -605,10 +588,136 @@ def _has_gpu():
         return False
 
 
+LOOP_METRIC = "particle-steps/s (drift + kick + buffer_v)"
+LOOP_UNIT = "particle-steps/s"
+
+
+def _timed_steps(loop, steps, stream):
+    """K steps of a TimeLoop timed with CUDA events on its stream; (ms per step, drift ms, kick ms)."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        loop.step(events=ev[k])
+    torch.cuda.synchronize()
+    drift = sum(e[0].elapsed_time(e[1]) for e in ev)
+    kick = sum(e[1].elapsed_time(e[2]) for e in ev)
+    return ev[0][0].elapsed_time(ev[-1][2]) / max(steps, 1), drift / max(steps, 1), kick / max(steps, 1)
+
+
+def run_loop(args, rank, world, local_rank):
+    """The kick-drift time loop (drift, buffer_grid, buffer_x, kick, buffer_v per step) on
+    Zel'dovich initial conditions built on the device.  The plain loop (cutoff 2) is timed;
+    the same start is then run with the learned shell (cutoff 1 + MLP) and with cutoff 1 alone,
+    and the final states are compared with the plain one by CIC power-spectrum ratio (k up to
+    k_Nyquist / 2 of the P(k) grid) and rms position difference."""
+    import torch
+    import torch.distributed as dist
+    from cube2_b200 import learned as Ln
+    from cube2_b200 import loop as LP
+    from cube2_b200 import workloads as W
+    from cube2_b200.layout import Layout
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev)
+    w = W.LOOP_WORKLOADS[args.workload]
+    L = Layout(**w["layout"])
+    stream = torch.cuda.Stream(dev)
+    t0 = time.perf_counter()
+    di = LP.zeldovich_start(L, w["rms"], w["seed"], 1.0, dev)
+    c = LP.growth_rate(di, w["apm3f"])
+    if not c > 0:
+        raise RuntimeError(f"no growing mode: c = {c}")
+    dt = float(np.log1p(w["growth_per_step"]) / np.sqrt(c))
+    di.vp[:di.n_used] *= float(np.sqrt(c))
+    torch.cuda.synchronize()
+    t_ic = time.perf_counter() - t0
+    N = L.ng ** 3
+    nw = w["pk_grid"]
+    pk0 = di.power_spectrum(nw)
+    start_learned, start_short = LP.clone_image(di), LP.clone_image(di)
+    plain = LP.TimeLoop(di, w["apm3f"], coef=dt, dt_mid=dt, stream=stream)
+    for _ in range(max(args.warmup, 0)):
+        plain.step()
+    torch.cuda.synchronize()
+    if plain.error_word():
+        raise RuntimeError(f"device error mask {plain.error_word()}")
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = Clocks(uuid)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ms, ms_drift, ms_kick = _timed_steps(plain, args.steps, stream)
+    ck = clocks.stop()
+    ms = max_over_ranks(ms, world, dev)
+    value = N * world / (ms * 1e-3)
+    pk_plain = di.power_spectrum(nw)
+    n_phys_ok = di.n_physical == N
+
+    def run_variant(start, apm3f, shell=None, scale=1.0):
+        lp = LP.TimeLoop(start, apm3f, coef=dt, dt_mid=dt, shell=shell, shell_scale=scale, stream=stream)
+        for _ in range(max(args.warmup, 0)):
+            lp.step()
+        m, md, mk = _timed_steps(lp, args.steps, stream)
+        pk = start.power_spectrum(nw)
+        kmax = nw // 4
+        ok = (pk_plain["modes"] > 0) & (np.arange(pk_plain["modes"].size) >= 1) & (np.arange(pk_plain["modes"].size) <= kmax)
+        ratio = pk["pk"][ok] / pk_plain["pk"][ok]
+        return {"ms_per_step": m, "drift_ms": md, "kick_ms": mk, "value": N / (m * 1e-3), "unit": LOOP_UNIT,
+                "pk_ratio_max_dev": float(np.max(np.abs(ratio - 1.0))),
+                "pk_ratio_bins": [round(float(x), 5) for x in ratio],
+                "rms_position_difference_fine_cells": LP.rms_position_difference(start, di),
+                "within_1pct": bool(np.max(np.abs(ratio - 1.0)) <= 0.01), "error_word": lp.error_word()}
+    variants = {}
+    if rank == 0 and not args.no_learned:
+        try:
+            shell, scale, tinfo = Ln.train_shell(dev)
+            variants["learned"] = run_variant(start_learned, 2.0, shell, scale)
+            variants["learned"]["train"] = tinfo
+            shell.close()
+        except Exception as e:  # reported beside the plain loop, never instead of it
+            variants["learned"] = {"error": repr(e)}
+        try:
+            variants["cutoff1_without_shell"] = run_variant(start_short, 2.0)
+        except Exception as e:
+            variants["cutoff1_without_shell"] = {"error": repr(e)}
+    growth = pk_plain["pk"][1:nw // 4 + 1] / pk0["pk"][1:nw // 4 + 1]
+    peak, src = measured_hbm_peak()
+    line = {"metric": LOOP_METRIC, "value": value, "unit": LOOP_UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32 (int16 fixed-point positions, fp64 Green table)",
+            "data": "synthetic (Zel'dovich lattice, P(k) ~ k^-2, built on the device; see cube2_b200/loop.py)",
+            "config": {"workload": args.workload, "particles": N, "layout": L.as_dict(), "pm3_mesh": L.ng * 2,
+                       "pp_cutoff_fine_cells": w["apm3f"] / 2, "growth_per_step": w["growth_per_step"],
+                       "dt": dt, "growth_rate_c": c, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (mesh 1024^3 fp32 = 4.3 GB, particle arrays > 3 GB)"},
+            "stages_ms": {"drift_and_buffers": ms_drift, "kick_and_buffer_v": ms_kick},
+            "initial_conditions_seconds": t_ic, "particles_conserved": bool(n_phys_ok),
+            "pk_growth_plain": [round(float(x), 4) for x in growth[:8]],
+            "pk_grid": nw, "variants": variants, "clocks": ck, "hbm_peak_gbs": peak,
+            "e2e": {"unavailable": "the loop keeps the image on the device between steps; the host-array "
+                                   "entry points (cube_kick_fine, cube_drift) are timed on the single-kick workloads"},
+            "cpu_baseline": {"unavailable": "the reference loop is the Fortran driver (no Fortran compiler here)"}}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
     from cube2_b200 import workloads as W
+    if args.workload in W.LOOP_WORKLOADS:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's time loop is the Fortran driver "
+                          "(main.f90); no Fortran compiler here"}))
+        return
     if W.WORKLOADS[args.workload]["kind"] == "batch":
         print(json.dumps({"impl": "reference", "unavailable": "the reference CPU path is timed on the single-image "
                           "workloads; batch workloads compare against a per-box launch loop instead"}))
@@ -638,8 +747,11 @@ def run_reference(args, rank, world):
 def main():
     args = parse()
     rank, world, local_rank = dist_env()
+    from cube2_b200 import workloads as W
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload in W.LOOP_WORKLOADS:
+        run_loop(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 

@@ -92,6 +92,7 @@ struct Ctx {
   Buf dr_cb, dr_cb_new, dr_runrank, dr_run_base, dr_runs, dr_ctr, dr_dest_runs, dr_dest_start, dr_scan_tmp,
       dr_cursor, dr_phys, dr_list, dr_off, dr_rows, dr_total;
   Buf dh_rhoc, dh_idx, dh_xp, dh_vp, dh_pid, dh_rhoc2, dh_idx2, dh_xp2, dh_vp2, dh_pid2;  // host-array drift
+  Buf pw_grid, pw_k, pw_bins;  // power spectrum
   cudaEvent_t tune_ev[2 * kMaxPPShapes] = {};
   void *h_stage = nullptr;  // pinned staging for small tables
   size_t h_stage_cap = 0;
@@ -1374,6 +1375,56 @@ int cube_drift(int32_t *rhoc, int64_t *idx_b_r, int16_t *xp, float *vp, int64_t 
   }
   CU(cudaStreamSynchronize(st));
   return CUBE_OK;
+}
+
+// ---- CIC power spectrum (utilities/cicpower.f90, utilities/powerspectrum.f90) ----
+
+int cube_power_spectrum(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
+                        int64_t n_physical, int32_t nw, int32_t nbin, double *bins, void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!d_rhoc || !d_idx_b_r || !bins || (n_used > 0 && !d_xp) || n_physical <= 0) return fail(CUBE_ERR_INVALID);
+  if (nw < 2 || nw > 2048 || (nw & 1)) return fail(CUBE_ERR_INVALID);
+  if (nbin <= 0) nbin = (int)std::lround((nw / 2) * std::sqrt(3.0));
+  if (nbin > 4096) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  const Lay &L = g.L;
+  const int64_t n3 = (int64_t)nw * nw * nw, nk = (int64_t)nw * nw * (nw / 2 + 1);
+  CK(grow(g.dr_cb, sizeof(int64_t) * (size_t)L.ntile * L.nte * L.nte * L.nte));
+  CK(grow(g.pw_grid, sizeof(float) * n3));
+  CK(grow(g.pw_k, sizeof(cufftComplex) * nk));
+  CK(grow(g.pw_bins, sizeof(double) * 4 * (nbin + 1)));
+  cudaStream_t own = g.stream;
+  if (stream) g.stream = (cudaStream_t)stream;
+  cudaStream_t st = g.stream;
+  int s = CUBE_OK;
+  do {
+    if (cudaMemsetAsync(g.pw_grid.p, 0, sizeof(float) * n3, st) != cudaSuccess ||
+        cudaMemsetAsync(g.pw_bins.p, 0, sizeof(double) * 4 * (nbin + 1), st) != cudaSuccess) {
+      s = fail(CUBE_ERR_CUDA);
+      break;
+    }
+    launch_cell_table(L, d_rhoc, d_idx_b_r, (int64_t *)g.dr_cb.p, st);
+    launch_cic_grid(L, nw, d_rhoc, (const int64_t *)g.dr_cb.p, d_xp, n_used, (float *)g.pw_grid.p, g.num_sms, st);
+    launch_density_contrast((float *)g.pw_grid.p, n3, (float)((double)n3 / (double)n_physical), st);
+    cufftHandle fw;
+    s = get_plan(nw, 1, CUFFT_R2C, &fw);
+    if (s != CUBE_OK) break;
+    if (cufftExecR2C(fw, (cufftReal *)g.pw_grid.p, (cufftComplex *)g.pw_k.p) != CUFFT_SUCCESS) {
+      s = fail(CUBE_ERR_CUFFT);
+      break;
+    }
+    launch_pk_bins((const cufftComplex *)g.pw_k.p, nw, nbin, (double *)g.pw_bins.p, g.num_sms, st);
+    g.launches += 4;
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(bins, g.pw_bins.p, sizeof(double) * 4 * (nbin + 1), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      s = fail(CUBE_ERR_CUDA);
+  } while (0);
+  g.stream = own;
+  return s;
 }
 
 // ---- learned PP shell ----

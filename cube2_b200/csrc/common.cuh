@@ -223,6 +223,15 @@ void launch_drift_place(const DriftArgs &a, int32_t nruns, int32_t *scan_tmp, cu
 void launch_halo_velocities(const Lay &L, const int32_t *rhoc, const int64_t *cell_base, float *vp, int64_t n_used,
                             int num_sms, cudaStream_t s);
 
+// CIC power spectrum (power.cu): deposit of the physical particles on an nw^3 grid, density
+// contrast, and the binning of the R2C transform into [4][nbin + 1] doubles (modes, sum |k|,
+// sum |delta_k|^2 / sinc^4, sum 4 pi k^3 |delta_k|^2 / sinc^4)
+void launch_cic_grid(const Lay &L, int nw, const int32_t *rhoc, const int64_t *cell_base, const int16_t *xp,
+                     int64_t n_used, float *grid, int num_sms, cudaStream_t s);
+void launch_density_contrast(float *grid, int64_t n, float scale, cudaStream_t s);
+size_t pk_bins_smem(int nbin);
+void launch_pk_bins(const cufftComplex *ck, int nw, int nbin, double *bins, int num_sms, cudaStream_t s);
+
 // PP kick with all scratch in a static device array (noalloc.cu)
 int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
                      const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp,

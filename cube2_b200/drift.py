@@ -125,6 +125,12 @@ class DeviceImage:
         _check(lib().cube_buffer_v_device(_dp(self.rhoc), _dp(self.idx), _dp(self.vp), ctypes.c_int64(self.n_used),
                                           _sp(stream)), "cube_buffer_v_device")
 
+    def power_spectrum(self, nw: int, nbin: int = 0, stream=None) -> dict:
+        """CIC power spectrum of the physical particles (cube_power_spectrum): per linear
+        |k| bin (grid units) the mode count, mean |k|, mean |delta_k|^2 / sinc^4 and the
+        dimensionless mean 4 pi k^3 |delta_k|^2 / sinc^4."""
+        return power_spectrum(self.rhoc, self.idx, self.xp, self.n_used, self.n_physical, nw, nbin, stream)
+
     def to_host(self) -> Image:
         import torch
         torch.cuda.synchronize()
@@ -137,4 +143,17 @@ class DeviceImage:
                      interior_mask(L, rhoc), n_particles=self.n_physical)
 
 
-__all__ = ["DeviceImage", "drift_host", "interior_mask", "CubeError"]
+def power_spectrum(d_rhoc, d_idx, d_xp, n_used: int, n_physical: int, nw: int, nbin: int = 0, stream=None) -> dict:
+    """cube_power_spectrum on device arrays; see DeviceImage.power_spectrum."""
+    nb = nbin if nbin > 0 else int(round((nw // 2) * np.sqrt(3.0)))
+    bins = np.zeros(4 * (nb + 1), np.float64)
+    _check(lib().cube_power_spectrum(_dp(d_rhoc), _dp(d_idx), _dp(d_xp), ctypes.c_int64(n_used),
+                                     ctypes.c_int64(n_physical), ctypes.c_int32(nw), ctypes.c_int32(nb), _p(bins),
+                                     _sp(stream)), "cube_power_spectrum")
+    b = bins.reshape(4, nb + 1)
+    modes = b[0]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return {"modes": modes, "k": b[1] / modes, "pk": b[2] / modes, "delta2": b[3] / modes}
+
+
+__all__ = ["DeviceImage", "drift_host", "interior_mask", "power_spectrum", "CubeError"]

@@ -16,6 +16,11 @@
   lognormal count (median 32^3, sigma 1, clipped to 2048 .. 200000; seed
   3000), so the boxes are uneven.  ``batch8`` is the same with 8 boxes.
 
+* ``loop512``       the kick-drift time loop: 512^3 particles on a 512^3-fine-cell box
+  (PM3 mesh 1024^3), Zel'dovich initial conditions (P(k) ~ k^-2, rms displacement 0.5
+  cell, seed 5000) built on the device (cube2_b200/loop.py), 2^3 tiles.  ``loop128``
+  is the same at 128^3 (tests and quick runs).
+
 All use ratio_cs = 4, a one coarse-cell tile buffer (ngb = 4), TSC, equal
 particle mass 1, PM3 softening apm3f = 4 mesh cells on a ratio_sf = 2 mesh
 (so the PP range apm3f / ratio_sf is 2 fine cells) and the full periodic
@@ -44,6 +49,14 @@ WORKLOADS = {
     # the same with 8 boxes and smaller counts (tests)
     "batch8": dict(layout=dict(ng=64, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1), kind="batch", box=32,
                    median=4096, sigma=1.0, clip=(512, 20000), seed=3100, rsf=2, apm3f=4.0),
+}
+
+# time loops: initial conditions built on the device (loop.zeldovich_start)
+LOOP_WORKLOADS = {
+    "loop512": dict(layout=dict(ng=512, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1), rms=0.5, seed=5000, apm3f=4.0,
+                    growth_per_step=0.05, pk_grid=512),
+    "loop128": dict(layout=dict(ng=128, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1), rms=0.5, seed=5100, apm3f=4.0,
+                    growth_per_step=0.05, pk_grid=128),
 }
 
 

@@ -176,6 +176,17 @@ int cube_drift(int32_t *rhoc, int64_t *idx_b_r, int16_t *xp, float *vp, int64_t 
 int cube_buffer_v_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, float *d_vp, int64_t n_used,
                          void *stream);
 
+/* ---- CIC power spectrum (utilities/cicpower.f90, utilities/powerspectrum.f90) ---- */
+
+/* CIC deposit of the image's physical particles on a cell-centred nw^3 grid
+ * (cicpower.f90:55-70), delta = rho nw^3 / n_physical - 1, one R2C transform, and the
+ * linear-k binning of powerspectrum.f90:52-94: for bins b = 0..nbin (nbin <= 0: nint(nw/2
+ * sqrt 3)), bins[b] = modes, bins[nbin+1+b] = sum |k|, bins[2(nbin+1)+b] = sum |delta_k|^2 /
+ * sinc^4 and bins[3(nbin+1)+b] = sum 4 pi |k|^3 |delta_k|^2 / sinc^4 (delta_k = FFT / nw^3,
+ * |k| in grid units).  nw even, 2..2048.  Waits for the result (host array). */
+int cube_power_spectrum(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
+                        int64_t n_physical, int32_t nw, int32_t nbin, double *bins, void *stream);
+
 /* ---- PP kernel shape autotuner (no reference counterpart) ---- */
 
 /* The PP force kernel comes in several shapes: `chunk` i-particles per work item (a

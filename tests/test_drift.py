@@ -57,3 +57,22 @@ def test_fixed_point_offset_wraps_and_rounds_half_away():
     counts, x, v, _ = D.drift_physical(L, rhoc, xp, vp, None, 1.0, 1.0)
     assert x.tolist() == [[-32766, -32768, 97]]  # 32767 + 3 wraps; 100 + nint(-2.5) = 97
     assert counts.sum() == 1
+
+
+def test_power_oracle_lattice_and_shot_noise():
+    """A lattice at the grid's own cell centres has no power; a Poisson sample has about
+    the shot noise 1/N per mode (CIC-deconvolved, so a little above at high k)."""
+    from oracle import power_oracle as P
+    nw, nc = 16, 16
+    g = (np.arange(nw) + 0.5) * nc / nw
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    lat = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    pk = P.power_spectrum(lat, nc, nw)["pk"]
+    assert np.nanmax(np.abs(pk[1:])) < 1e-20
+    rng = np.random.default_rng(2)
+    n = 200000
+    pois = rng.random((n, 3)) * nc
+    r = P.power_spectrum(pois, nc, nw)
+    m = r["modes"][2:8]
+    ratio = np.sum(r["pk"][2:8] * m) / np.sum(m) * n  # mode-weighted mean over bins 2..7
+    assert 0.9 < ratio < 1.15, ratio

@@ -139,3 +139,24 @@ def test_kick_drift_loop_matches_oracle_each_step(gpu):
         got = di.to_host()
         _compare((got.rhoc, got.idx_b_r, got.xp, got.vp, got.pid), want[:5])
         np.testing.assert_array_equal(np.sort(got.pid[got.active]), np.arange(img.n_particles))
+
+
+@pytest.mark.parametrize("nw", [32, 64])
+def test_power_spectrum_matches_oracle(gpu, nw):
+    import torch
+    from cube2_b200 import workloads as W
+    from cube2_b200.drift import DeviceImage
+    from cube2_b200.kick import CUBE_PM3_PERIODIC, FineKick
+    from oracle import power_oracle as P
+    img = W.make("zeldovich64")
+    L = img.layout
+    FineKick(L, pm3_mode=CUBE_PM3_PERIODIC).configure()
+    di = DeviceImage(img, torch.device("cuda:0"))
+    got = di.power_spectrum(nw)
+    pos = W.physical_positions(img) / L.ratio_cs  # coarse-cell units
+    want = P.power_spectrum(pos, L.nc, nw)
+    np.testing.assert_array_equal(got["modes"], want["modes"])
+    ok = want["modes"] > 0
+    np.testing.assert_allclose(got["k"][ok], want["k"][ok], rtol=1e-12)
+    np.testing.assert_allclose(got["pk"][ok], want["pk"][ok], rtol=2e-3, atol=1e-12)
+    np.testing.assert_allclose(got["delta2"][ok], want["delta2"][ok], rtol=2e-3, atol=1e-9)
