@@ -625,12 +625,7 @@ def run_loop(args, rank, world, local_rank):
     L = Layout(**w["layout"])
     stream = torch.cuda.Stream(dev)
     t0 = time.perf_counter()
-    di = LP.zeldovich_start(L, w["rms"], w["seed"], 1.0, dev)
-    c = LP.growth_rate(di, w["apm3f"])
-    if not c > 0:
-        raise RuntimeError(f"no growing mode: c = {c}")
-    dt = float(np.log1p(w["growth_per_step"]) / np.sqrt(c))
-    di.vp[:di.n_used] *= float(np.sqrt(c))
+    di, dt, c = LP.start_with_growth(L, w["rms"], w["seed"], w["growth_per_step"], w["apm3f"], dev)
     torch.cuda.synchronize()
     t_ic = time.perf_counter() - t0
     N = L.ng ** 3
@@ -676,13 +671,29 @@ def run_loop(args, rank, world, local_rank):
                 "within_1pct": bool(np.max(np.abs(ratio - 1.0)) <= 0.01), "error_word": lp.error_word()}
     variants = {}
     if rank == 0 and not args.no_learned:
+        start_lognormal = LP.clone_image(start_learned)
         try:
-            shell, scale, tinfo = Ln.train_shell(dev)
+            # the method's own snapshots: a 128^3 companion box of the same statistics (another seed),
+            # every 5 steps of a plain loop as long as this one
+            sl = dict(w["layout"], ng=128)
+            snaps = LP.snapshots(Layout(**sl), w["rms"], w["seed"] + 7, w["growth_per_step"], w["apm3f"],
+                                 args.warmup + args.steps, 2, dev)
+            shell, scale, tinfo = Ln.train_shell_on(snaps, dev, steps=12000,
+                                                    fields="snapshots 0, 2, 4, ... of a plain 128^3 loop of the "
+                                                    f"same statistics (seed {w['seed'] + 7})")
+            del snaps
             variants["learned"] = run_variant(start_learned, 2.0, shell, scale)
             variants["learned"]["train"] = tinfo
             shell.close()
         except Exception as e:  # reported beside the plain loop, never instead of it
             variants["learned"] = {"error": repr(e)}
+        try:
+            shell, scale, tinfo = Ln.train_shell(dev)
+            variants["learned_lognormal_boxes"] = run_variant(start_lognormal, 2.0, shell, scale)
+            variants["learned_lognormal_boxes"]["train"] = tinfo
+            shell.close()
+        except Exception as e:
+            variants["learned_lognormal_boxes"] = {"error": repr(e)}
         try:
             variants["cutoff1_without_shell"] = run_variant(start_short, 2.0)
         except Exception as e:

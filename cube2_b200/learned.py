@@ -238,26 +238,35 @@ def unexplained(net: ShellNet, X, T, rows) -> float:
     return float((r * r).sum() / (Tr.double() ** 2).sum())
 
 
-def train_shell(device, steps: int = 6000, batch: int = 8192, seed: int = 1):
-    """The shell used by the benchmarks: trained on three lognormal Poisson boxes of 96^3 fine
-    cells (sigma 0.5, 1.0, 1.5; seeds 4001..4003, about 2.6M samples) with Adam on standardized
-    inputs, then folded for raw inputs.  Returns (ShellNet, target scale, info)."""
+def train_shell_on(images, device, steps: int = 6000, batch: int = 8192, seed: int = 1, fields: str = ""):
+    """A shell trained on the method's own forces on `images` (host Images in the periodic
+    layout): targets from the cutoff-2 and cutoff-1 kicks of each image, Adam on standardized
+    inputs, folded for raw inputs.  Returns (ShellNet, target scale, info)."""
     import time
 
-    from . import ic
-    from .layout import RATIO_SF, build_image, ixyz3_table
+    from .layout import RATIO_SF, ixyz3_table
     t0 = time.perf_counter()
-    Lt = Layout(ng=96, nnt=1, nns=2, ratio_cs=4, ngb=4, app=0.1)
-    tt = (np.arange(1, Lt.ns3 + 1, dtype=np.int32), np.full(Lt.ns3, 2, np.int32), ixyz3_table(Lt), None, RATIO_SF)
-    boxes = [build_image(*ic.lognormal_poisson(96, sg, sd)[:2], Lt) for sg, sd in ((0.5, 4001), (1.0, 4002),
-                                                                                   (1.5, 4003))]
-    X, T, scale = training_set(boxes, [tt] * 3, device)
+    tabs = [(np.arange(1, im.layout.ns3 + 1, dtype=np.int32), np.full(im.layout.ns3, 2, np.int32),
+             ixyz3_table(im.layout), None, RATIO_SF) for im in images]
+    X, T, scale = training_set(images, tabs, device)
     Xs, mu, sd = standardize(X, X.shape[0])
     net = ShellNet(batch_cap=batch, seed=seed)
     hist = train(net, Xs, T, steps=steps, batch=batch, lr=1e-3, log_every=1000)
     shell = ShellNet(fold(net.params(), mu, sd), batch_cap=16)
     net.close()
-    info = {"samples": int(sum(int(b.active.sum()) for b in boxes)), "steps": steps, "batch": batch,
-            "seconds": time.perf_counter() - t0, "loss": hist,
-            "fields": "lognormal Poisson 96^3, sigma 0.5 / 1.0 / 1.5 (seeds 4001..4003)"}
+    info = {"samples": int(X.shape[0]), "steps": steps, "batch": batch, "seconds": time.perf_counter() - t0,
+            "loss": hist, "fields": fields}
+    del X, Xs, T
     return shell, scale, info
+
+
+def train_shell(device, steps: int = 6000, batch: int = 8192, seed: int = 1):
+    """The shell of the single-kick benchmark: trained on three lognormal Poisson boxes of 96^3
+    fine cells (sigma 0.5, 1.0, 1.5; seeds 4001..4003, about 2.6M samples)."""
+    from . import ic
+    from .layout import build_image
+    Lt = Layout(ng=96, nnt=1, nns=2, ratio_cs=4, ngb=4, app=0.1)
+    boxes = [build_image(*ic.lognormal_poisson(96, sg, sd)[:2], Lt) for sg, sd in ((0.5, 4001), (1.0, 4002),
+                                                                                   (1.5, 4003))]
+    return train_shell_on(boxes, device, steps, batch, seed,
+                          fields="lognormal Poisson 96^3, sigma 0.5 / 1.0 / 1.5 (seeds 4001..4003)")

@@ -215,8 +215,11 @@ class TimeLoop:
         di.buffer_v(self.stream)
         if events:
             events[2].record(st) if st is not None else events[2].record()
+        import torch
         if st is not None:
             st.synchronize()  # out is read on the host below
+        else:
+            torch.cuda.synchronize()  # the library's own stream
         self.vz = float(self.out[4].item())  # vmax_z after the kick: nlayer of the next drift
 
     def error_word(self) -> int:
@@ -235,3 +238,28 @@ def clone_image(di: DeviceImage) -> DeviceImage:
     c._spare = None
     c.n_used = n
     return c
+
+
+def start_with_growth(L: Layout, rms_disp: float, seed: int, growth_per_step: float, apm3f: float, device):
+    """Zel'dovich start in the linear growing mode: (image with vp = sqrt(c) Psi, step dt, c)."""
+    di = zeldovich_start(L, rms_disp, seed, 1.0, device)
+    c = growth_rate(di, apm3f)
+    if not c > 0:
+        raise RuntimeError(f"no growing mode: c = {c}")
+    dt = float(np.log1p(growth_per_step) / np.sqrt(c))
+    di.vp[:di.n_used] *= float(np.sqrt(c))
+    return di, dt, c
+
+
+def snapshots(L: Layout, rms_disp: float, seed: int, growth_per_step: float, apm3f: float, steps: int,
+              every: int, device):
+    """Host images of a plain loop on layout L taken every `every` steps (step 0 included): the
+    method's own snapshots, for training the learned shell."""
+    di, dt, _ = start_with_growth(L, rms_disp, seed, growth_per_step, apm3f, device)
+    loop = TimeLoop(di, apm3f, coef=dt, dt_mid=dt)
+    out = [di.to_host()]
+    for k in range(1, steps + 1):
+        loop.step()
+        if k % every == 0:
+            out.append(di.to_host())
+    return out

@@ -19,7 +19,7 @@
 * ``loop512``       the kick-drift time loop: 512^3 particles on a 512^3-fine-cell box
   (PM3 mesh 1024^3), Zel'dovich initial conditions (P(k) ~ k^-2, rms displacement 0.5
   cell, seed 5000) built on the device (cube2_b200/loop.py), 2^3 tiles.  ``loop128``
-  is the same at 128^3 (tests and quick runs).
+  and ``loop256`` are the same at 128^3 (tests and quick runs) and 256^3 (profiling).
 
 All use ratio_cs = 4, a one coarse-cell tile buffer (ngb = 4), TSC, equal
 particle mass 1, PM3 softening apm3f = 4 mesh cells on a ratio_sf = 2 mesh
@@ -57,6 +57,9 @@ LOOP_WORKLOADS = {
                     growth_per_step=0.05, pk_grid=512),
     "loop128": dict(layout=dict(ng=128, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1), rms=0.5, seed=5100, apm3f=4.0,
                     growth_per_step=0.05, pk_grid=128),
+    # profiling size: particle arrays (16.8M x 26 B) larger than L2, a few GB on the device
+    "loop256": dict(layout=dict(ng=256, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1), rms=0.5, seed=5200, apm3f=4.0,
+                    growth_per_step=0.05, pk_grid=256),
 }
 
 
