@@ -1377,6 +1377,26 @@ int cube_drift(int32_t *rhoc, int64_t *idx_b_r, int16_t *xp, float *vp, int64_t 
   return CUBE_OK;
 }
 
+// ---- checkpoint files ----
+
+int cube_snapshot_write(const char *prefix, const char *suffix, const cube_sim_header *header, const int32_t *rhoc,
+                        const int64_t *idx_b_r, const int16_t *xp, const float *vp, const int64_t *pid) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  const int s = snapshot_write(g.L, prefix, suffix, header, rhoc, idx_b_r, xp, vp, pid);
+  return s == CUBE_OK ? s : fail(s);
+}
+
+int cube_snapshot_read(const char *prefix, const char *suffix, cube_sim_header *header, int32_t *rhoc_phys,
+                       int16_t *xp, float *vp, int64_t *pid, int64_t capacity) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  const int s = snapshot_read(g.L, prefix, suffix, header, rhoc_phys, xp, vp, pid, capacity);
+  return s == CUBE_OK ? s : fail(s);
+}
+
 // ---- CIC power spectrum (utilities/cicpower.f90, utilities/powerspectrum.f90) ----
 
 int cube_power_spectrum(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,

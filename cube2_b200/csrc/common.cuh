@@ -232,6 +232,14 @@ void launch_density_contrast(float *grid, int64_t n, float scale, cudaStream_t s
 size_t pk_bins_smem(int nbin);
 void launch_pk_bins(const cufftComplex *ck, int nw, int nbin, double *bins, int num_sms, cudaStream_t s);
 
+// checkpoint files (snapshot.cu)
+constexpr size_t kSimHeaderBytes = 13 * 8 + 19 * 4;
+int snapshot_write(const Lay &L, const char *prefix, const char *suffix, const cube_sim_header *h,
+                   const int32_t *rhoc, const int64_t *idx_b_r, const int16_t *xp, const float *vp,
+                   const int64_t *pid);
+int snapshot_read(const Lay &L, const char *prefix, const char *suffix, cube_sim_header *h, int32_t *rhoc_phys,
+                  int16_t *xp, float *vp, int64_t *pid, int64_t capacity);
+
 // PP kick with all scratch in a static device array (noalloc.cu)
 int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
                      const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp,

@@ -33,18 +33,24 @@ def drift_host(img: Image, dt_mid: float, vz_max: float, pm3_mode: int = CUBE_PM
     L = img.layout
     FineKick(L, pm3_mode=pm3_mode).configure()
     cap = int(capacity if capacity is not None else max(2 * img.n_used, 1024))
-    rhoc = np.ascontiguousarray(img.rhoc, np.int32).copy()
-    idx = np.ascontiguousarray(img.idx_b_r, np.int64).copy()
-    xp = np.zeros((cap, 3), np.int16)
-    vp = np.zeros((cap, 3), np.float32)
-    pid = np.zeros(cap, np.int64)
-    xp[:img.n_used] = img.xp
-    vp[:img.n_used] = img.vp
-    pid[:img.n_used] = img.pid
     n_new, n_phys = ctypes.c_int64(), ctypes.c_int64()
-    _check(lib().cube_drift(_p(rhoc), _p(idx), _p(xp), _p(vp), _p(pid), ctypes.c_int64(img.n_used),
-                            ctypes.c_int64(cap), ctypes.c_float(dt_mid), ctypes.c_float(vz_max), ctypes.byref(n_new),
-                            ctypes.byref(n_phys)), "cube_drift")
+    for attempt in range(2):  # on a capacity error the call reports the size it needs
+        rhoc = np.ascontiguousarray(img.rhoc, np.int32).copy()
+        idx = np.ascontiguousarray(img.idx_b_r, np.int64).copy()
+        xp = np.zeros((cap, 3), np.int16)
+        vp = np.zeros((cap, 3), np.float32)
+        pid = np.zeros(cap, np.int64)
+        xp[:img.n_used] = img.xp
+        vp[:img.n_used] = img.vp
+        pid[:img.n_used] = img.pid
+        st = lib().cube_drift(_p(rhoc), _p(idx), _p(xp), _p(vp), _p(pid), ctypes.c_int64(img.n_used),
+                              ctypes.c_int64(cap), ctypes.c_float(dt_mid), ctypes.c_float(vz_max),
+                              ctypes.byref(n_new), ctypes.byref(n_phys))
+        if st == CUBE_ERR_CAPACITY and attempt == 0 and capacity is None and n_new.value > cap:
+            cap = int(n_new.value)
+            continue
+        _check(st, "cube_drift")
+        break
     n = n_new.value
     return Image(L, xp[:n].copy(), vp[:n].copy(), rhoc, idx, pid[:n].copy(), interior_mask(L, rhoc),
                  n_particles=int(n_phys.value))

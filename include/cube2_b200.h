@@ -176,6 +176,34 @@ int cube_drift(int32_t *rhoc, int64_t *idx_b_r, int16_t *xp, float *vp, int64_t 
 int cube_buffer_v_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, float *d_vp, int64_t n_used,
                          void *stream);
 
+/* ---- checkpoint files (checkpoint.f90, particle_initialization.f90) ---- */
+
+/* sim_header of parameters.f90:141-164.  In the info file it is 13 int64 followed by 19
+ * real(4), 180 bytes, no padding (a Fortran stream write of the derived type). */
+typedef struct cube_sim_header {
+  int64_t nplocal, npglobal, izipx, izipv, image, nn, nnt, nt, ncell, ncb, timestep, cur_checkpoint,
+      cur_halofind;
+  float a, t, tau, dt_pp, dt_pm3, dt_pm2, dt_pm1, dt_vmax, mass_p_cdm, box, h0, omega_m, omega_l, s8, vsim2phys,
+      sigma_vres, sigma_vi, z_i, vz_max;
+} cube_sim_header;
+
+/* Write the checkpoint of the configured image (checkpoint.f90:11-38): files
+ * prefix + {info, xp, vp, np, id} + suffix, as the reference names them
+ * (basic_functions.f08:60-86: prefix "<opath>image<i>/<z>_", suffix "_<i>.bin").  The image
+ * is given with its buffers; its physical particles are written tile by tile, row by row, the
+ * order the reference's arrays hold right after a drift.  header->nplocal is set from the
+ * image; pid NULL writes no id file.  Host arrays; needs no GPU. */
+int cube_snapshot_write(const char *prefix, const char *suffix, const cube_sim_header *header, const int32_t *rhoc,
+                        const int64_t *idx_b_r, const int16_t *xp, const float *vp, const int64_t *pid);
+/* Read one (particle_initialization.f90:19-60): the header, the physical counts rhoc_phys
+ * (C view [nnt^3][nt][nt][nt] of rhoc(1:nt,1:nt,1:nt,:,:,:); NULL skips them) and nplocal
+ * particles into xp / vp / pid (pid NULL skips the id file).  CUBE_ERR_INVALID when the
+ * stored formats (izipx, izipv = 2) or nnt / nt differ from the configured layout;
+ * CUBE_ERR_CAPACITY, with the header filled, when nplocal > capacity.  The buffers are rebuilt
+ * by a drift with dt_mid = 0 on the image of physical cells (cube_drift). */
+int cube_snapshot_read(const char *prefix, const char *suffix, cube_sim_header *header, int32_t *rhoc_phys,
+                       int16_t *xp, float *vp, int64_t *pid, int64_t capacity);
+
 /* ---- CIC power spectrum (utilities/cicpower.f90, utilities/powerspectrum.f90) ---- */
 
 /* CIC deposit of the image's physical particles on a cell-centred nw^3 grid
