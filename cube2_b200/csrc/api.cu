@@ -1456,7 +1456,7 @@ struct cube_mlp {
 static void mlp_free(cube_mlp *h) {
   MlpParams &p = h->p;
   void *bufs[] = {p.master, p.grad, p.mom, p.vel, p.wb, p.wt, p.xb, p.a[0], p.a[1], p.a[2], p.dyb, p.dzb, p.dzt,
-                  p.at, p.tb, p.z[0], p.z[1], p.z[2], p.y, p.dy, p.dz, p.da, p.b4pad};
+                  p.at, p.tb, p.z[0], p.z[1], p.z[2], p.y, p.dy, p.dz, p.da, p.b4pad, p.err};
   for (void *b : bufs)
     if (b) cudaFree(b);
   delete h;
@@ -1498,6 +1498,8 @@ int cube_mlp_create(const float *params, int32_t batch_cap, cube_mlp **out) {
   al(&p.dz, sizeof(float) * B * W);
   al(&p.da, sizeof(float) * B * W);
   al(&p.b4pad, sizeof(float) * kMlpOutPad);
+  al(&p.err, sizeof(int32_t));
+  if (ok) ok = cudaMemset(p.err, 0, sizeof(int32_t)) == cudaSuccess;
   if (ok) ok = cudaMemcpy(p.master, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice) == cudaSuccess;
   if (ok) ok = cudaMemset(p.mom, 0, sizeof(float) * kMlpParams) == cudaSuccess &&
                cudaMemset(p.vel, 0, sizeof(float) * kMlpParams) == cudaSuccess &&
@@ -1602,6 +1604,11 @@ int cube_mlp_kick(cube_mlp *h, const int32_t *d_rhoc, const int64_t *d_idx_b_r, 
                    kick * scale, g.num_sms, s);
   g.launches += 1;
   CU(cudaGetLastError());
+  // the inference kernel's bounded waits report through a status word: read it once the kick is done
+  int32_t e = 0;
+  CU(cudaMemcpyAsync(&e, h->p.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (e) return fail(CUBE_ERR_TIMEOUT);
   return CUBE_OK;
 }
 

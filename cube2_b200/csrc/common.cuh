@@ -270,6 +270,7 @@ struct MlpParams {
   __nv_bfloat16 *xb = nullptr, *a[3] = {}, *dyb = nullptr, *dzb = nullptr, *dzt = nullptr, *at = nullptr;
   float *tb = nullptr, *z[3] = {}, *y = nullptr, *dy = nullptr, *dz = nullptr, *da = nullptr, *b4pad = nullptr;
   int device = -1;
+  int32_t *err = nullptr;  // device status word of the inference kernel (bit CUBE_ERR_TIMEOUT)
 };
 void launch_mlp_pos(const Lay &L, const int16_t *xp, const int32_t *rhoc, const int64_t *cell_base, float4 *pos,
                     cudaStream_t s);

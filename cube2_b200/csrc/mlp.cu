@@ -16,6 +16,7 @@
 // all four layers with the weights resident in shared memory and adds the predicted force
 // times the kick coefficient to vp of the interior particles.
 #include <algorithm>
+#include <cstdlib>
 
 #include "common.cuh"
 
@@ -467,6 +468,331 @@ __global__ void __launch_bounds__(kApplyWarps * 32, 1) k_mlp_apply(MlpApplyK p) 
 }
 
 // ---------------------------------------------------------------------------------------------
+// fused inference + kick on the 5th-generation tensor cores (tcgen05): 128 particles per tile,
+// accumulators in tensor memory
+//
+// Two warpgroups per CTA, one CTA per SM, each warpgroup with its own tile: while one runs its
+// epilogue (features, or bias + GELU + BF16 of a layer), the other's MMAs run.  A thread owns
+// one particle (row m = thread index in the warpgroup = TMEM lane).  The operands sit in shared
+// memory in the K-major layout without swizzle that the UMMA descriptors read: core matrices
+// of 8 rows x 16 bytes, stored chunk-major, element (r, k) of an R-row matrix at byte
+//   ((k / 8) * (R / 8) + r / 8) * 128 + (r % 8) * 16 + (k % 8) * 2,
+// so one MMA step of K = 16 covers two 8-element chunks (leading-byte offset (R / 8) * 128 between
+// them, stride-byte offset 128 between 8-row groups).  Layer l: D[128][N] = A[128][K] W_l^T with
+// A the warpgroup's activation buffer and W_l [N][K] (N = 128, or 16 for the output layer), issued
+// by one thread as K / 16 tcgen05.mma and one tcgen05.commit to the warpgroup's mbarrier.
+
+constexpr int kTcRows = 128;                // particles per tile (UMMA M)
+constexpr int kTcGroups = 4;                // warpgroups per CTA, each with its own tile
+constexpr int kTcThreads = kTcGroups * kTcRows;
+constexpr size_t kTcW1 = (size_t)kMlpW * kMlpK1 * 2, kTcW = (size_t)kMlpW * kMlpW * 2,
+                 kTcW4 = (size_t)kMlpOutPad * kMlpW * 2;
+constexpr size_t kTcAct = (size_t)kTcRows * kMlpW * 2;  // one warpgroup's activations
+constexpr size_t kTcOffW2 = kTcW1, kTcOffW3 = kTcOffW2 + kTcW, kTcOffW4 = kTcOffW3 + kTcW,
+                 kTcOffAct = kTcOffW4 + kTcW4, kTcOffBias = kTcOffAct + kTcGroups * kTcAct,
+                 kTcOffBar = kTcOffBias + sizeof(float) * (3 * kMlpW + kMlpOutPad),
+                 kTcSmem = kTcOffBar + 8 * kTcGroups + 16;
+constexpr uint32_t kTcCols = 128 * kTcGroups;  // TMEM columns: 128 per warpgroup
+constexpr unsigned long long kTcWaitNs = 1000000000ull;  // bound of one mbarrier wait: 1 s
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// byte offset of element (r, k) of an R-row operand in the chunk-major core-matrix layout
+__device__ __forceinline__ uint32_t umma_off(int r, int k, int R) {
+  return (uint32_t)(((k >> 3) * (R >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle; start, leading and stride byte
+// offsets in 16-byte units, version 1 (bits 46-47)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: BF16 A and B (K-major), FP32 accumulator, M = 128, N
+__host__ __device__ constexpr uint32_t umma_idesc(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void wg_sync(int wg) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + wg), "r"(kTcRows) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// wait for the phase of an mbarrier to complete, for at most kTcWaitNs; false on a timeout
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+    if (global_ns() - t0 > kTcWaitNs) return false;
+  }
+}
+
+// every thread of the warpgroup gets the AND of v over the warpgroup (also a warpgroup barrier)
+__device__ __forceinline__ bool wg_all(int wg, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(1 + wg), "r"(kTcRows)
+      : "memory");
+  return r != 0;
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float v[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float v[4]) {
+  uint32_t r[4];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int j = 0; j < 4; j++) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
+}
+
+// the inputs of mlp_inputs written straight into row m of the activation buffer, one 8-value
+// chunk at a time: chunk 2 dz + h holds the stencil rows dy = 2h - 1, 2h of plane dz (x fastest),
+// chunk 8 the offsets, chunk 9 zeros
+__device__ __forceinline__ void tc_inputs(float4 q, bool live, const float *__restrict__ rho, int ng,
+                                          unsigned char *act, int m) {
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  if (!live) {
+#pragma unroll
+    for (int c = 0; c < kMlpK1 / 8; c++) *reinterpret_cast<uint4 *>(act + umma_off(m, 8 * c, kTcRows)) = zero;
+    return;
+  }
+  const float xs[3] = {q.x - 0.5f, q.y - 0.5f, q.z - 0.5f};
+  int i0[3];
+  float f[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const float fl = floorf(xs[d]);
+    i0[d] = (int)fl;
+    f[d] = xs[d] - fl;
+  }
+  int X[4];
+#pragma unroll
+  for (int dx = 0; dx < 4; dx++) X[dx] = wrap_cell(i0[0] + dx - 1, ng);
+#pragma unroll 1
+  for (int c = 0; c < 8; c++) {
+    const int dz = c >> 1, h = c & 1;
+    const int64_t Z = wrap_cell(wrap_cell(i0[2] + dz - 1, ng), ng);
+    __align__(16) __nv_bfloat162 v[4];
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+      const int64_t Y = wrap_cell(wrap_cell(i0[1] + 2 * h + r - 1, ng), ng);
+      const float *row = rho + (Z * ng + Y) * ng;
+      v[2 * r] = __floats2bfloat162_rn(__ldg(row + X[0]), __ldg(row + X[1]));
+      v[2 * r + 1] = __floats2bfloat162_rn(__ldg(row + X[2]), __ldg(row + X[3]));
+    }
+    *reinterpret_cast<uint4 *>(act + umma_off(m, 8 * c, kTcRows)) = *reinterpret_cast<const uint4 *>(v);
+  }
+  __align__(16) __nv_bfloat162 o[4];
+  o[0] = __floats2bfloat162_rn(f[0], f[1]);
+  o[1] = __floats2bfloat162_rn(f[2], 0.f);
+  o[2] = o[3] = __floats2bfloat162_rn(0.f, 0.f);
+  *reinterpret_cast<uint4 *>(act + umma_off(m, 64, kTcRows)) = *reinterpret_cast<const uint4 *>(o);
+  *reinterpret_cast<uint4 *>(act + umma_off(m, 72, kTcRows)) = zero;
+}
+
+// copy layer l ([R][K] row-major in global) into the chunk-major layout
+__device__ __forceinline__ void tc_load_layer(unsigned char *dst, const bf16 *src, int R, int K) {
+  for (int i = threadIdx.x; i < R * (K / 8); i += blockDim.x) {
+    const int r = i / (K / 8), c = i % (K / 8);
+    *reinterpret_cast<uint4 *>(dst + umma_off(r, 8 * c, R)) = *reinterpret_cast<const uint4 *>(src + r * K + 8 * c);
+  }
+}
+
+// issue one layer: D (TMEM) = A W^T over K / 16 steps, then commit to the mbarrier
+__device__ __forceinline__ void tc_issue(uint32_t tmem_d, uint32_t a_base, uint32_t w_base, int K, int N,
+                                         uint32_t bar) {
+  const uint32_t lbo_a = (kTcRows / 8) * 128, lbo_w = (uint32_t)(N / 8) * 128;
+  const uint32_t idesc = umma_idesc(N);
+  for (int s = 0; s < K / 16; s++) {
+    const uint64_t ad = umma_desc(a_base + 2 * s * lbo_a, lbo_a, 128);
+    const uint64_t bd = umma_desc(w_base + 2 * s * lbo_w, lbo_w, 128);
+    umma_bf16(tmem_d, ad, bd, idesc, s > 0 ? 1u : 0u);
+  }
+  umma_commit(bar);
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_mlp_apply_tc(MlpApplyK p, int32_t *err) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  unsigned char *w1 = tc_smem, *w2 = tc_smem + kTcOffW2, *w3 = tc_smem + kTcOffW3, *w4 = tc_smem + kTcOffW4;
+  float *bias = reinterpret_cast<float *>(tc_smem + kTcOffBias);  // b1 b2 b3 [128] each, b4 [16]
+  uint64_t *bars = reinterpret_cast<uint64_t *>(tc_smem + kTcOffBar);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tc_smem + kTcOffBar + 8 * kTcGroups);
+  const int tid = threadIdx.x, wg = tid / kTcRows, m = tid % kTcRows, warp = tid >> 5;
+  unsigned char *act = tc_smem + kTcOffAct + wg * kTcAct;
+
+  tc_load_layer(w1, p.wb + mlp_wboff(0), kMlpW, kMlpK1);
+  tc_load_layer(w2, p.wb + mlp_wboff(1), kMlpW, kMlpW);
+  tc_load_layer(w3, p.wb + mlp_wboff(2), kMlpW, kMlpW);
+  tc_load_layer(w4, p.wb + mlp_wboff(3), kMlpOutPad, kMlpW);
+  for (int i = tid; i < 3 * kMlpW + kMlpOutPad; i += blockDim.x) {
+    float v = 0.f;
+    if (i < 3 * kMlpW) v = p.master[mlp_boff(i / kMlpW) + i % kMlpW];
+    else if (i - 3 * kMlpW < kMlpOut) v = p.master[mlp_boff(3) + i - 3 * kMlpW];
+    bias[i] = v;
+  }
+  if (tid == 0) {
+    for (int b = 0; b < kTcGroups; b++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTcCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_async_smem();  // the weights were written by ordinary stores; the tensor cores read them
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot + (uint32_t)(wg * kMlpW);  // this warpgroup's 128 columns
+  const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;  // TMEM lanes of this warp
+  const uint32_t bar = smem_u32(&bars[wg]);
+  const uint32_t a_s = smem_u32(act), w1_s = smem_u32(w1), w2_s = smem_u32(w2), w3_s = smem_u32(w3),
+                 w4_s = smem_u32(w4);
+  uint32_t phase = 0;
+  bool ok = true;
+
+  const int64_t ntiles = (p.n + kTcRows - 1) / kTcRows;
+  for (int64_t tile = (int64_t)blockIdx.x * kTcGroups + wg; tile < ntiles && ok;
+       tile += (int64_t)gridDim.x * kTcGroups) {
+    const int64_t i = tile * kTcRows + m;
+    const float4 q = i < p.n ? p.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool live = i < p.n && q.w != 0.f;
+    tc_inputs(q, live, p.rho, p.ng, act, m);  // layer-1 input row of this particle
+    // layers 1-3 (N = 128): MMA, then bias + GELU + BF16 back into the activation buffer
+#pragma unroll 1
+    for (int l = 0; l < 3 && ok; l++) {
+      fence_async_smem();
+      tc_fence_before();
+      wg_sync(wg);
+      if (m == 0) {
+        tc_fence_after();
+        tc_issue(tmem, a_s, l == 0 ? w1_s : (l == 1 ? w2_s : w3_s), l == 0 ? kMlpK1 : kMlpW, kMlpW, bar);
+      }
+      ok = wg_all(wg, mbar_wait(bar, phase));
+      phase ^= 1u;
+      tc_fence_after();
+      if (!ok) break;
+      const float *b = bias + l * kMlpW;
+#pragma unroll 1
+      for (int c0 = 0; c0 < kMlpW; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + lane_base + (uint32_t)c0, v);
+        __align__(16) __nv_bfloat162 h[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+          h[j] = __floats2bfloat162_rn(gelu_f(v[2 * j] + b[c0 + 2 * j]), gelu_f(v[2 * j + 1] + b[c0 + 2 * j + 1]));
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+          *reinterpret_cast<uint4 *>(act + umma_off(m, c0 + 8 * c, kTcRows)) = reinterpret_cast<const uint4 *>(h)[c];
+      }
+    }
+    if (!ok) break;
+    // output layer (N = 16, outputs 0..2 used) and the kick
+    fence_async_smem();
+    tc_fence_before();
+    wg_sync(wg);
+    if (m == 0) {
+      tc_fence_after();
+      tc_issue(tmem, a_s, w4_s, kMlpW, kMlpOutPad, bar);
+    }
+    ok = wg_all(wg, mbar_wait(bar, phase));
+    phase ^= 1u;
+    tc_fence_after();
+    if (!ok) break;
+    float y[4];
+    tmem_ld4(tmem + lane_base, y);
+    if (live) {
+      float *v = p.vp + 3 * i;
+      v[0] += p.coef * (y[0] + bias[3 * kMlpW + 0]);
+      v[1] += p.coef * (y[1] + bias[3 * kMlpW + 1]);
+      v[2] += p.coef * (y[2] + bias[3 * kMlpW + 2]);
+    }
+    tc_fence_before();  // the next tile's MMA overwrites these columns
+  }
+  if (!ok && m == 0) atomicOr(err, 1 << CUBE_ERR_TIMEOUT);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kTcCols));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // host side
 
 void launch_mlp_pos(const Lay &L, const int16_t *xp, const int32_t *rhoc, const int64_t *cell_base, float4 *pos,
@@ -513,10 +839,15 @@ void launch_mlp_apply(const MlpParams &m, const float4 *pos, const float *rho, i
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_mlp_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplySmem);
+    cudaFuncSetAttribute(k_mlp_apply_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
     attr = true;
   }
   MlpApplyK p{m.wb, m.master, pos, rho, ng, n, vp, coef};
-  k_mlp_apply<<<num_sms, kApplyWarps * 32, kApplySmem, s>>>(p);
+  if (getenv("CUBE_MLP_MMA_SYNC")) {
+    k_mlp_apply<<<num_sms, kApplyWarps * 32, kApplySmem, s>>>(p);
+  } else {
+    k_mlp_apply_tc<<<num_sms, kTcThreads, kTcSmem, s>>>(p, m.err);
+  }
 }
 
 // Forward + backward + Adam on one batch of `batch` rows picked by `rows` from X / T.

@@ -131,3 +131,29 @@ def test_trained_shell_gains_over_cutoff_one(gpu):
     assert abs(u_raw - u) < 0.02, (u, u_raw)
     net.close()
     raw.close()
+
+
+def test_tensor_memory_kernel_matches_mma_sync_kernel(gpu, monkeypatch):
+    """The inference kernel on tcgen05 (accumulators in tensor memory) against the mma.sync one,
+    on the same features and weights: both round the activations to BF16, so they agree to the
+    accumulation order."""
+    import torch
+    from cube2_b200 import learned as Ln
+    img, rho, idx, xp, vp = _zeld()
+    rng = np.random.default_rng(8)
+    p = Ln.unflatten(Ln.init_params(9))
+    for k in ("b1", "b2", "b3", "b4"):
+        p[k] = (0.1 * rng.standard_normal(p[k].shape)).astype(np.float32)
+    net = Ln.ShellNet(Ln.flatten(p), batch_cap=256)
+    out = []
+    for mma_sync in (False, True):
+        if mma_sync:
+            monkeypatch.setenv("CUBE_MLP_MMA_SYNC", "1")
+        v = vp.clone()
+        net.kick(rho, idx, xp, img.n_used, v, 1.0, 6 * np.pi, 1.0)
+        torch.cuda.synchronize()
+        out.append((v - vp).cpu().numpy().reshape(-1, 3))
+    monkeypatch.delenv("CUBE_MLP_MMA_SYNC")
+    assert np.all(out[0][~img.active] == 0)
+    assert _rel_rms(out[0][img.active], out[1][img.active]) < 2e-3
+    net.close()
