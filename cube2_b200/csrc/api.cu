@@ -408,6 +408,23 @@ static int get_green_periodic(int n, int rsf, float **out) {
   return CUBE_OK;
 }
 
+// Green table of any mesh, tabulated on the device in FP64 and kept by its parameters
+static int get_green_params(int n, float apm_soft, float apm_range, float gridsize, float **out) {
+  for (auto &e : g.greens)
+    if (e.n == n && e.apm_soft == apm_soft && e.apm_range == apm_range && e.gridsize == gridsize &&
+        e.p == g.L.p_order) {
+      *out = e.d;
+      return CUBE_OK;
+    }
+  GreenEntry e{n, apm_soft, apm_range, gridsize, g.L.p_order, nullptr};
+  CU(cudaMalloc(&e.d, sizeof(float) * (size_t)n * n * (n / 2 + 1)));
+  launch_green_fp64(n, apm_soft, apm_range, gridsize, g.L.p_order, e.d, g.stream);
+  CU(cudaGetLastError());
+  g.greens.push_back(e);
+  *out = e.d;
+  return CUBE_OK;
+}
+
 static int get_green_host(const float *host, int n, float **out) {
   const size_t count = (size_t)n * n * (n / 2 + 1);
   for (auto &e : g.hgreens)
@@ -1191,6 +1208,139 @@ int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32
   }
   g.stream = own;
   return s;
+}
+
+// ---- PM1 and PM2, the long-range layers (kick.f90:61-105, particle_mesh.f90, pm_thread) ----
+
+// PM1: one periodic mesh of nc^3 coarse cells over the image (gridsize = ratio_cs, so the mesh
+// coordinate is the global coarse coordinate), Green_3D(nc, apm_soft, 0, ratio_cs)
+// (initialize.f90:129).  PM2: per parent tile the fine mesh of the tile with its buffers,
+// ngt = (nt + 2 ncb) ratio_cs points per side (gridsize 1), all stored cells deposited
+// (nloop = ncb), the physical ones kicked, Green_3D(ngt, apm_soft, apm_range, 1)
+// (initialize.f90:135, kick.f90:82-88); the tiles' meshes go through one batched transform.
+// Both kick vp of the physical particles by a_mid dt / (6 pi) times the TSC-gathered force.
+static int run_pm_layer(int layer, const Dev &d, float mass, float kick, float apm_soft, float apm_range,
+                        float out[5]) {
+  const Lay &L = g.L;
+  const bool pm1 = layer == 1;
+  const int n = pm1 ? L.nc : L.nte * L.rcs;
+  const int nslots = pm1 ? 1 : L.ntile;
+  const int64_t n3 = (int64_t)n * n * n, nk = (int64_t)n * n * (n / 2 + 1);
+  CK(stage_begin((size_t)1 << 20));
+  CK(grow(g.cell_base, sizeof(int64_t) * (size_t)L.ntile * L.nte * L.nte * L.nte));
+  CK(grow(g.out, sizeof(float) * 8));
+  CK(grow(g.rho, sizeof(float) * n3 * nslots));
+  CK(grow(g.rhok, sizeof(cufftComplex) * nk * nslots));
+  CK(grow(g.force, sizeof(float) * n3 * 3 * nslots));
+  float *G = nullptr;
+  CK(get_green_params(n, apm_soft, pm1 ? 0.0f : apm_range, pm1 ? (float)L.rcs : 1.0f, &G));
+  // mesh coordinate = stored coordinate * ratio_cs / gridsize (kick.f90:438, particle_mesh.f90:31)
+  const double scale = pm1 ? 1.0 : (double)L.rcs;
+  std::vector<MeshJob> jobs(L.ntile);
+  for (int t = 0; t < L.ntile; t++) {
+    const int tc[3] = {t % L.nnt, (t / L.nnt) % L.nnt, t / (L.nnt * L.nnt)};
+    MeshJob &J = jobs[t];
+    J.t = t;
+    J.slot = pm1 ? 0 : t;
+    J.range = 0.f;
+    for (int q = 0; q < 3; q++) {
+      J.lo[q] = pm1 ? L.ncb : 0;  // PM2 deposits the buffer cells too (nloop = ncb)
+      J.alo[q] = L.ncb;
+      J.off[q] = pm1 ? -(double)tc[q] * L.nt : 0.0;
+    }
+  }
+  size_t soff = 0;
+  CK(upload(g.jobs, jobs.data(), jobs.size(), soff));
+  CU(cudaMemsetAsync(g.out.p, 0, sizeof(float) * 8, g.stream));
+  launch_cell_table(L, d.rhoc, d.idx, (int64_t *)g.cell_base.p, g.stream);
+  PM3Args a{};
+  a.L = &g.L;
+  a.rsf = 1;
+  a.n = n;
+  a.nslots = nslots;
+  a.jobs = (const MeshJob *)g.jobs.p;
+  a.njobs = L.ntile;
+  for (int q = 0; q < 3; q++) {
+    a.rdep[q] = pm1 ? L.nt : L.nte;
+    a.ract[q] = L.nt;
+  }
+  a.wrap = pm1 ? 1 : 0;
+  a.shift = pm1 ? 0 : L.ncb * L.rcs;  // array index = Fortran index - (1 - ngb)
+  a.fphys_lo = pm1 ? 0 : L.ncb * L.rcs;
+  a.fphys_n = pm1 ? n : L.nt * L.rcs;
+  a.scale = scale;
+  a.xp = d.xp;
+  a.rhoc = d.rhoc;
+  a.cell_base = (const int64_t *)g.cell_base.p;
+  a.rho = (float *)g.rho.p;
+  a.rhok = (cufftComplex *)g.rhok.p;
+  a.force = (float *)g.force.p;
+  a.green = G;
+  a.mass = mass;
+  a.kick = kick;
+  a.vp = d.vp;
+  a.out = (float *)g.out.p;
+  a.want_vmax = 1;
+  cufftHandle fw, bw;
+  CK(get_plan(n, nslots, CUFFT_R2C, &fw));
+  CK(get_plan(n, nslots, CUFFT_C2R, &bw));
+  CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3 * nslots, g.stream));
+  launch_pm3_deposit(a, g.stream);
+  CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
+  launch_pm3_kspace(a, g.stream);
+  CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)g.rho.p));
+  launch_pm3_force(a, g.stream);
+  launch_pm3_gather(a, g.stream);
+  g.launches += 5;
+  CU(cudaGetLastError());
+  CK(stage_end());
+  CU(cudaMemcpyAsync(out, g.out.p, sizeof(float) * 5, cudaMemcpyDeviceToHost, g.stream));
+  CU(cudaStreamSynchronize(g.stream));
+  return CUBE_OK;
+}
+
+static int pm_layer_entry(int layer, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp,
+                          int64_t n_used, float *d_vp, float mass, float a_mid, float dt, float apm_soft,
+                          float apm_range, float *f2max, float vmax[3], void *stream) {
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!d_rhoc || !d_idx_b_r || (n_used > 0 && (!d_xp || !d_vp)) || n_used < 0) return fail(CUBE_ERR_INVALID);
+  if (!(apm_soft > 0.f) || apm_range < 0.f) return fail(CUBE_ERR_INVALID);
+  const Lay &L = g.L;
+  if (layer == 2 && L.pm3_mode == CUBE_PM3_TILE_PERIODIC) return fail(CUBE_ERR_INVALID);
+  if (layer == 1 && (L.nc % 4 || L.nc < 8)) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  cudaStream_t own = g.stream;
+  if (stream) g.stream = (cudaStream_t)stream;
+  const float kick = (float)((double)(a_mid * dt / 6.0f) / 3.14159265358979323846);
+  Dev d{d_xp, d_rhoc, d_idx_b_r, d_vp, n_used};
+  float out[5] = {0, 0, 0, 0, 0};
+  const int s = run_pm_layer(layer, d, mass, kick, apm_soft, apm_range, out);
+  g.stream = own;
+  if (s != CUBE_OK) return s;
+  if (f2max) *f2max = out[0];
+  if (vmax) {
+    vmax[0] = out[2];
+    vmax[1] = out[3];
+    vmax[2] = out[4];
+  }
+  return CUBE_OK;
+}
+
+int cube_pm1_force_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
+                          float *d_vp, float mass, float a_mid, float dt, float apm1c, float *f2max, float vmax[3],
+                          void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  return pm_layer_entry(1, d_rhoc, d_idx_b_r, d_xp, n_used, d_vp, mass, a_mid, dt, apm1c, 0.f, f2max, vmax,
+                        stream);
+}
+
+int cube_pm2_force_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
+                          float *d_vp, float mass, float a_mid, float dt, float apm2, float apm1, float *f2max,
+                          float vmax[3], void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  return pm_layer_entry(2, d_rhoc, d_idx_b_r, d_xp, n_used, d_vp, mass, a_mid, dt, apm2, apm1, f2max, vmax, stream);
 }
 
 // ---- drift and buffer rebuild ----

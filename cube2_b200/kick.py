@@ -57,7 +57,8 @@ EXPORTS = ("cube_set_layout", "cube_get_layout", "cube_last_error", "cube_error_
            "cube_kick_graph_launch", "cube_kick_graph_destroy", "cube_mlp_create", "cube_mlp_destroy",
            "cube_mlp_get_params", "cube_mlp_features", "cube_mlp_train_step", "cube_mlp_forward", "cube_mlp_kick",
            "cube_pp_set_shape", "cube_pp_shapes", "cube_drift_device", "cube_drift", "cube_buffer_v_device",
-           "cube_power_spectrum", "cube_snapshot_write", "cube_snapshot_read")
+           "cube_power_spectrum", "cube_snapshot_write", "cube_snapshot_read", "cube_pm1_force_device",
+           "cube_pm2_force_device")
 
 
 def lib() -> ctypes.CDLL:

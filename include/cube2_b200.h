@@ -150,6 +150,26 @@ int cube_kick_graph_create(const int32_t *isort, const int32_t *ires, const int3
 int cube_kick_graph_launch(cube_kick_graph *graph, void *stream);
 int cube_kick_graph_destroy(cube_kick_graph *graph);
 
+/* ---- PM1 and PM2, the long-range layers of the reference's force split ---- */
+
+/* PM1 (kick.f90:61-73 with particle_mesh.f90, pm_layer 1): TSC deposit of the physical
+ * particles on one periodic mesh of nc^3 coarse cells over the image (gridsize = ratio_cs),
+ * the Green table Green_3D(nc, apm1c, 0, ratio_cs) of initialize.f90:129 (tabulated here in
+ * FP64), the 4-point difference, and the TSC gather and kick of vp by a_mid dt / (6 pi) for the
+ * physical particles.  Device arrays; the call waits for f2max and vmax.  nc a multiple of 4. */
+int cube_pm1_force_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
+                          float *d_vp, float mass, float a_mid, float dt, float apm1c, float *f2max, float vmax[3],
+                          void *stream);
+/* PM2 (kick.f90:77-105, pm_thread of kick.f90:403-568 with pm_layer 2): per parent tile, the fine
+ * mesh of the tile with its buffers (ngt = ngp + 2 ngb points per side, gridsize 1), every stored
+ * copy of the tile deposited (nloop = ncb), Green_3D(ngt, apm2, apm1, 1) of initialize.f90:135,
+ * and the kick of the tile's physical particles.  The tiles' meshes are transformed as one batch.
+ * Same conventions as cube_pm1_force_device.  The range apm1 should not exceed the buffer depth
+ * ngb, as in the reference (apm1 = 14, ngb = 16). */
+int cube_pm2_force_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
+                          float *d_vp, float mass, float a_mid, float dt, float apm2, float apm1, float *f2max,
+                          float vmax[3], void *stream);
+
 /* ---- drift and buffer rebuild (drift.f90, buffer_grid.f90, buffer_particle.f90) ---- */
 
 /* One drift of the configured image followed by the rebuild of its periodic buffers:

@@ -261,6 +261,57 @@ def pm3_subtile(img, ires, ixyz3, ratio_sf, greens: dict, mass: float, a_mid: fl
     return dict(vp=vp, f2max=f2max, vmax=vmax, dv=dv)
 
 
+def pm1(img, apm1c: float, mass: float, a_mid: float, dt: float):
+    """PM1 (particle_mesh.f90, pm_layer 1) on the periodic coarse mesh nc^3 with
+    Green_3D(nc, apm1c, 0, ratio_cs).  Returns dict(vp, f2max, vmax, dv)."""
+    L = img.layout
+    n = L.nc
+    ol = _olay(L)
+    G = green(n, apm1c, 0.0, float(L.ratio_cs))
+    rho = np.empty((n, n, n), dtype=np.float64)
+    lib().pm1o_deposit(ctypes.byref(ol), _ptr(img.xp), _ptr(img.rhoc), _ptr(img.idx_b_r), _ptr(rho))
+    rho *= mass
+    phi = _solve(rho, G)
+    force = np.empty((3, n, n, n), dtype=np.float64)
+    lib().pm3o_force_periodic(_c_i64(n), _ptr(phi), _c_d(float(n) ** 3), _ptr(force))
+    f2max = float(lib().pm3o_f2max(_c_i64(n ** 3), _ptr(force)))
+    vp = img.vp.copy()
+    dv = np.zeros((img.n_used, 3), dtype=np.float64)
+    vmax = np.zeros(3, dtype=np.float32)
+    kick = float(np.float32(a_mid) * np.float32(dt) / np.float32(6.0)) / np.pi
+    lib().pm1o_gather(ctypes.byref(ol), _ptr(img.xp), _ptr(img.rhoc), _ptr(img.idx_b_r), _ptr(force), _c_d(kick),
+                      _ptr(vp), _ptr(dv), _ptr(vmax))
+    return dict(vp=vp, f2max=f2max, vmax=vmax, dv=dv)
+
+
+def pm2(img, apm2: float, apm1: float, mass: float, a_mid: float, dt: float):
+    """PM2 (pm_thread with the parameters of kick.f90:82-88) on every tile's buffered fine mesh,
+    ngt = (nt + 2 ncb) ratio_cs, with Green_3D(ngt, apm2, apm1, 1).  Returns dict(vp, f2max, vmax, dv)."""
+    L = img.layout
+    nft = L.nte * L.ratio_cs
+    nfp, nfb = L.nt * L.ratio_cs, L.ncb * L.ratio_cs
+    ol = _olay(L)
+    G = green(nft, apm2, apm1, 1.0)
+    vp = img.vp.copy()
+    dv = np.zeros((img.n_used, 3), dtype=np.float64)
+    f2max = 0.0
+    vmax = np.zeros(3, dtype=np.float32)
+    kick = float(np.float32(a_mid) * np.float32(dt) / np.float32(6.0)) / np.pi
+    for t in range(L.nnt ** 3):
+        rho = np.empty((nft, nft, nft), dtype=np.float64)
+        lib().pm2o_deposit(ctypes.byref(ol), _ptr(img.xp), _ptr(img.rhoc), _ptr(img.idx_b_r), _c_i(t), _ptr(rho))
+        rho *= mass
+        phi = _solve(rho, G)
+        force = np.empty((3, nft, nft, nft), dtype=np.float64)
+        lib().pm3o_force_periodic(_c_i64(nft), _ptr(phi), _c_d(float(nft) ** 3), _ptr(force))
+        f2max = max(f2max, float(lib().pm3o_f2max_subtile(_c_i64(nft), _c_i64(nfp), _c_i64(nfb), _ptr(force))))
+        vm = np.zeros(3, dtype=np.float32)
+        lib().pm2o_gather(ctypes.byref(ol), _ptr(img.xp), _ptr(img.rhoc), _ptr(img.idx_b_r), _c_i(t), _ptr(force),
+                          _c_d(kick), _ptr(vp), _ptr(dv), _ptr(vm))
+        vmax = np.maximum(vmax, vm)
+    return dict(vp=vp, f2max=f2max, vmax=vmax, dv=dv)
+
+
 # ----------------------------------------------------------------------------------------------
 # FP64 truth
 

@@ -10,6 +10,8 @@
  *   f2max    : kick.f90:494
  *   gather   : kick.f90:497-540   (TSC gather + kick dv*a_mid*dt/6/pi)
  *   Green    : Green/Green.f90:1-80 (Green_3D, FP64, alias sum n_int=2)
+ *   PM1, PM2 : particle_mesh.f90 (pm_layer 1) and pm_thread with the PM2 parameters of
+ *              kick.f90:82-88, the same deposit / force / gather on other meshes
  *
  * The FFT between deposit and force is done by the Python driver
  * (scipy.fft), the stand-in for FFTW/MKL which is not available here.
@@ -87,11 +89,9 @@ static inline double mesh_scale(const olay_t *L, int rsf) {
 /* Deposit every interior particle of every tile into rho[n][n][n] (unit mass).
  * Threads take whole z-planes of coarse cells; planes `stride` apart never touch
  * the same mesh points (the z-layer striping of kick.f90:425-429). */
-void pm3o_deposit_periodic(const olay_t *L, const int16_t *xp, const int32_t *rhoc, const int64_t *idx_b_r,
-                           int rsf, double *rho) {
+static void deposit_periodic(const olay_t *L, const int16_t *xp, const int32_t *rhoc, const int64_t *idx_b_r,
+                             int64_t n, double sc, double *rho) {
   const int nnt = L->nnt, nt = NT(L), ncb = NCB(L), nc = NC(L);
-  const int64_t n = (int64_t)L->ng * rsf;
-  const double sc = mesh_scale(L, rsf);
   int stride = 3;
   while (nc % stride) stride++;
   memset(rho, 0, sizeof(double) * n * n * n);
@@ -126,6 +126,20 @@ void pm3o_deposit_periodic(const olay_t *L, const int16_t *xp, const int32_t *rh
         }
     }
   }
+}
+
+void pm3o_deposit_periodic(const olay_t *L, const int16_t *xp, const int32_t *rhoc, const int64_t *idx_b_r,
+                           int rsf, double *rho) {
+  deposit_periodic(L, xp, rhoc, idx_b_r, (int64_t)L->ng * rsf, mesh_scale(L, rsf), rho);
+}
+
+/* PM1 (particle_mesh.f90:18-60 with pm_layer 1): the periodic coarse mesh n = nc over the image,
+ * mesh coordinate xpos * ratio_cs / gridsize with gridsize = real(ratio_cs), i.e. the global
+ * coarse coordinate.  The reference deposits each tile with its nloop = 1 buffer cells and keeps
+ * the tile's own mesh points, which places every physical particle's weights once, as here. */
+void pm1o_deposit(const olay_t *L, const int16_t *xp, const int32_t *rhoc, const int64_t *idx_b_r, double *rho) {
+  const float gs = (float)L->ratio_cs;
+  deposit_periodic(L, xp, rhoc, idx_b_r, NC(L), (double)L->ratio_cs / (double)gs, rho);
 }
 
 /* potential_to_force on a periodic mesh: F_d(x) = sum_o w_o phi(x+o e_d) / n^3 * scale
@@ -168,11 +182,11 @@ double pm3o_f2max(int64_t npts, const double *force) {
 /* Gather + kick for every interior particle (kick.f90:497-540):
  * dv = sum w F; vp[ip] += dv * kick; writes the applied dv (before kick) into acc[ip]
  * when acc != NULL; returns max |vp| per axis of the updated particles in vmax. */
-void pm3o_gather_periodic(const olay_t *L, const int16_t *xp, const int32_t *rhoc, const int64_t *idx_b_r,
-                          int rsf, const double *force, double kick, float *vp, double *acc, float vmax[3]) {
+static void gather_periodic(const olay_t *L, const int16_t *xp, const int32_t *rhoc, const int64_t *idx_b_r,
+                            int64_t n, double sc, const double *force, double kick, float *vp, double *acc,
+                            float vmax[3]) {
   const int nnt = L->nnt, nt = NT(L), ncb = NCB(L);
-  const int64_t n = (int64_t)L->ng * rsf, n3 = n * n * n;
-  const double sc = mesh_scale(L, rsf);
+  const int64_t n3 = n * n * n;
   float vm0 = 0, vm1 = 0, vm2 = 0;
   const int64_t ncell = (int64_t)nnt * nnt * nnt * nt * nt * nt;
 #pragma omp parallel for schedule(dynamic, 64) reduction(max : vm0, vm1, vm2)
@@ -220,6 +234,88 @@ void pm3o_gather_periodic(const olay_t *L, const int16_t *xp, const int32_t *rho
   vmax[0] = vm0;
   vmax[1] = vm1;
   vmax[2] = vm2;
+}
+
+void pm3o_gather_periodic(const olay_t *L, const int16_t *xp, const int32_t *rhoc, const int64_t *idx_b_r,
+                          int rsf, const double *force, double kick, float *vp, double *acc, float vmax[3]) {
+  gather_periodic(L, xp, rhoc, idx_b_r, (int64_t)L->ng * rsf, mesh_scale(L, rsf), force, kick, vp, acc, vmax);
+}
+
+/* PM1 gather and kick (particle_mesh.f90:100-148) */
+void pm1o_gather(const olay_t *L, const int16_t *xp, const int32_t *rhoc, const int64_t *idx_b_r,
+                 const double *force, double kick, float *vp, double *acc, float vmax[3]) {
+  const float gs = (float)L->ratio_cs;
+  gather_periodic(L, xp, rhoc, idx_b_r, NC(L), (double)L->ratio_cs / (double)gs, force, kick, vp, acc, vmax);
+}
+
+/* ---------------- PM2: per-tile buffered fine mesh (kick.f90:77-105, pm_thread :403-568) ---------------- */
+/* Tile t (0-based), mesh side ngt = (nt + 2 ncb) ratio_cs, gridsize 1 (mesh coordinate = tile-local
+ * fine coordinate), array index = Fortran index - (1 - ngb).  The deposit takes every stored cell
+ * of the tile (nc1 - nloop .. nc2 + nloop with nloop = ncb), dropping weights outside the mesh;
+ * the gather takes the physical cells. */
+void pm2o_deposit(const olay_t *L, const int16_t *xp, const int32_t *rhoc, const int64_t *idx_b_r, int t,
+                  double *rho) {
+  const int ncb = NCB(L), nte = NTE(L);
+  const int64_t nft = (int64_t)nte * L->ratio_cs, nfb = (int64_t)ncb * L->ratio_cs;
+  const double sc = (double)L->ratio_cs / (double)1.0f;
+  memset(rho, 0, sizeof(double) * nft * nft * nft);
+  for (int k = 0; k < nte; k++)
+    for (int j = 0; j < nte; j++)
+      for (int i = 0; i < nte; i++) {
+        int64_t np = rhoc_at(L, rhoc, t, k, j, i);
+        int64_t base = cell_base(L, rhoc, idx_b_r, t, k, j, i);
+        int cidx[3] = {i, j, k};
+        for (int64_t l = 0; l < np; l++) {
+          const int16_t *q = xp + 3 * (base + l);
+          int64_t c[3];
+          float w[3][3];
+          for (int d = 0; d < 3; d++) tsc_w(decode(cidx[d] - ncb, q[d]) * sc, &c[d], w[d]);
+          for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+              for (int e = 0; e < 3; e++) {
+                int64_t X = c[0] + e - 1 + nfb, Y = c[1] + b - 1 + nfb, Z = c[2] + a - 1 + nfb;
+                if (X < 0 || X >= nft || Y < 0 || Y >= nft || Z < 0 || Z >= nft) continue;
+                rho[(Z * nft + Y) * nft + X] += (double)(w[0][e] * w[1][b] * w[2][a]);
+              }
+        }
+      }
+}
+
+void pm2o_gather(const olay_t *L, const int16_t *xp, const int32_t *rhoc, const int64_t *idx_b_r, int t,
+                 const double *force, double kick, float *vp, double *acc, float vmax[3]) {
+  const int ncb = NCB(L), nt = NT(L), nte = NTE(L);
+  const int64_t nft = (int64_t)nte * L->ratio_cs, nfb = (int64_t)ncb * L->ratio_cs, n3 = nft * nft * nft;
+  const double sc = (double)L->ratio_cs / (double)1.0f;
+  for (int k = ncb; k < ncb + nt; k++)
+    for (int j = ncb; j < ncb + nt; j++)
+      for (int i = ncb; i < ncb + nt; i++) {
+        int64_t np = rhoc_at(L, rhoc, t, k, j, i);
+        int64_t base = cell_base(L, rhoc, idx_b_r, t, k, j, i);
+        int cidx[3] = {i, j, k};
+        for (int64_t l = 0; l < np; l++) {
+          int64_t ip = base + l;
+          const int16_t *q = xp + 3 * ip;
+          int64_t c[3];
+          float w[3][3];
+          for (int d = 0; d < 3; d++) tsc_w(decode(cidx[d] - ncb, q[d]) * sc, &c[d], w[d]);
+          double dv[3] = {0, 0, 0};
+          for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+              for (int e = 0; e < 3; e++) {
+                int64_t m = ((c[2] + a - 1 + nfb) * nft + (c[1] + b - 1 + nfb)) * nft + (c[0] + e - 1 + nfb);
+                double ww = (double)(w[0][e] * w[1][b] * w[2][a]);
+                dv[0] += force[m] * ww;
+                dv[1] += force[n3 + m] * ww;
+                dv[2] += force[2 * n3 + m] * ww;
+              }
+          for (int d = 0; d < 3; d++) {
+            if (acc) acc[3 * ip + d] = dv[d];
+            vp[3 * ip + d] = (float)((double)vp[3 * ip + d] + dv[d] * kick);
+            float av = fabsf(vp[3 * ip + d]);
+            if (av > vmax[d]) vmax[d] = av;
+          }
+        }
+      }
 }
 
 /* ---------------- mode 0: per-subtile buffered mesh ---------------- */

@@ -91,3 +91,28 @@ def test_pm3_linear_in_mass(gpu):
     a = fk.c_pm3_force_kernel(img, isort, ires, ixyz3_table(L), RATIO_SF, 1.0, SIXPI, 1.0, vp=z.copy())[0]
     b = fk.c_pm3_force_kernel(img, isort, ires, ixyz3_table(L), RATIO_SF, 3.0, SIXPI, 1.0, vp=z.copy())[0]
     assert _rel_rms(b.astype(np.float64), 3.0 * a.astype(np.float64)) < 1e-6
+
+
+@pytest.mark.parametrize("layer", [1, 2])
+@pytest.mark.parametrize("ngb", [4, 16])
+def test_pm1_pm2_match_restatement(gpu, layer, ngb):
+    """PM1 (periodic coarse mesh) and PM2 (per-tile buffered fine mesh) on the GPU against the
+    restatement of particle_mesh.f90 / pm_thread with the PM1 and PM2 parameters."""
+    from cube2_b200 import ic
+    from cube2_b200 import longrange as LR
+    from cube2_b200.layout import Layout, build_image
+    from oracle import oracle as O
+    L = Layout(ng=32, nnt=2, nns=2, ratio_cs=4, ngb=ngb, app=0.1)
+    pos, vel = ic.uniform_random(3000, 32.0, 13)
+    img = build_image(pos, vel, L)
+    if layer == 1:
+        vp, f2, vmax = LR.pm1_force(img, 3.5, 1.0, SIXPI, 1.0)
+        ref = O.pm1(img, 3.5, 1.0, SIXPI, 1.0)
+    else:
+        vp, f2, vmax = LR.pm2_force(img, 3.5, 14.0, 1.0, SIXPI, 1.0)
+        ref = O.pm2(img, 3.5, 14.0, 1.0, SIXPI, 1.0)
+    act = img.active
+    assert _rel_rms((vp - img.vp)[act].astype(np.float64), (ref["vp"] - img.vp)[act].astype(np.float64)) < TOL
+    assert np.all(vp[~act] == img.vp[~act])
+    assert abs(f2 - ref["f2max"]) <= 1e-5 * ref["f2max"]
+    np.testing.assert_allclose(vmax, ref["vmax"], rtol=1e-5)
