@@ -104,15 +104,23 @@ __global__ void __launch_bounds__(kDriftWarps * 32) k_drift_runs(DriftK p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int32_t *td = s_dest[warp], *tc = s_cnt[warp];
   const unsigned lt = (1u << lane) - 1u;
-  for (int64_t S = (int64_t)blockIdx.x * kDriftWarps + warp; S < p.ncells_src;
-       S += (int64_t)gridDim.x * kDriftWarps) {
-    const int n = p.rhoc[S];
+  const int64_t stride = (int64_t)gridDim.x * kDriftWarps;
+  int64_t S = (int64_t)blockIdx.x * kDriftWarps + warp;
+  // the count and first slot of the next cell are loaded one cell ahead
+  int n_next = S < p.ncells_src ? p.rhoc[S] : 0;
+  int64_t base_next = S < p.ncells_src ? p.cell_base[S] : 0;
+  for (; S < p.ncells_src; S += stride) {
+    const int n = n_next;
+    const int64_t base = base_next;
+    if (S + stride < p.ncells_src) {
+      n_next = p.rhoc[S + stride];
+      base_next = p.cell_base[S + stride];
+    }
     if (n <= 0) continue;
     if (n >= (1 << kRankBits) - 1) {  // the rank field holds ranks below 2^26 - 1
       if (lane == 0) atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
       continue;
     }
-    const int64_t base = p.cell_base[S];
     if (base < 0 || base + n > p.n_used) {  // the spine does not match the counts
       if (lane == 0) atomicOr(p.err, 1 << CUBE_ERR_INVALID);
       continue;
@@ -299,11 +307,18 @@ __device__ __forceinline__ int16_t drift_offset(const DriftK &p, int16_t x, floa
 
 __global__ void __launch_bounds__(kDriftWarps * 32) k_drift_write(DriftK p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int64_t S = (int64_t)blockIdx.x * kDriftWarps + warp; S < p.ncells_src;
-       S += (int64_t)gridDim.x * kDriftWarps) {
-    const int n = p.rhoc[S];
+  const int64_t stride = (int64_t)gridDim.x * kDriftWarps;
+  int64_t S = (int64_t)blockIdx.x * kDriftWarps + warp;
+  int n_next = S < p.ncells_src ? p.rhoc[S] : 0;
+  int64_t base_next = S < p.ncells_src ? p.cell_base[S] : 0;
+  for (; S < p.ncells_src; S += stride) {
+    const int n = n_next;
+    const int64_t base = base_next;
+    if (S + stride < p.ncells_src) {
+      n_next = p.rhoc[S + stride];
+      base_next = p.cell_base[S + stride];
+    }
     if (n <= 0 || n >= (1 << kRankBits) - 1) continue;
-    const int64_t base = p.cell_base[S];
     if (base < 0 || base + n > p.n_used) continue;
     const int rb = p.run_base[S];
     for (int l = lane; l < n; l += 32) {
