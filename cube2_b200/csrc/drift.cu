@@ -128,9 +128,14 @@ __global__ void __launch_bounds__(kDriftWarps * 32) k_drift_runs(DriftK p) {
     int t, cx, cy, cz;
     cell_of(p, S, t, cx, cy, cz);
     int nent = 0;  // warp-uniform
-    for (int c0 = 0; c0 < n; c0 += 32) {
+    // 64 copies per step: the loads of both halves are in flight together
+    for (int c64 = 0; c64 < n; c64 += 64) {
+    const int32_t D2[2] = {c64 + lane < n ? drift_dest(p, base + c64 + lane, cx, cy, cz, t) : -1,
+                           c64 + 32 + lane < n ? drift_dest(p, base + c64 + 32 + lane, cx, cy, cz, t) : -1};
+    for (int h = 0; h < 2 && c64 + 32 * h < n; h++) {
+      const int c0 = c64 + 32 * h;
       const int l = c0 + lane;
-      const int32_t D = l < n ? drift_dest(p, base + l, cx, cy, cz, t) : -1;
+      const int32_t D = D2[h];
       uint32_t word = kDropped;
       unsigned pending = __ballot_sync(0xffffffffu, D >= 0);
       while (pending) {
@@ -159,6 +164,7 @@ __global__ void __launch_bounds__(kDriftWarps * 32) k_drift_runs(DriftK p) {
         pending &= ~grp;
       }
       if (l < n) p.runrank[base + l] = word;
+    }
     }
     if (nent) {
       int rb = 0;
@@ -324,15 +330,23 @@ __global__ void __launch_bounds__(kDriftWarps * 32) k_drift_write(DriftK p) {
     for (int l = lane; l < n; l += 32) {
       const int64_t ip = base + l;
       const uint32_t w = p.runrank[ip];
+      // the copy's own data does not depend on its slot: loaded beside the slot lookup
+      float v[3];
+      int16_t x[3];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        v[d] = p.vp[3 * ip + d];
+        x[d] = p.xp[3 * ip + d];
+      }
+      const int64_t id = p.pid ? p.pid[ip] : 0;
       if (w == kDropped) continue;
       const int64_t pos = p.run_off[rb + (int)(w >> kRankBits)] + (int64_t)(w & ((1u << kRankBits) - 1u));
 #pragma unroll
       for (int d = 0; d < 3; d++) {
-        const float v = p.vp[3 * ip + d];
-        p.xp_new[3 * pos + d] = drift_offset(p, p.xp[3 * ip + d], v, p.err);
-        p.vp_new[3 * pos + d] = v;
+        p.xp_new[3 * pos + d] = drift_offset(p, x[d], v[d], p.err);
+        p.vp_new[3 * pos + d] = v[d];
       }
-      if (p.pid) p.pid_new[pos] = p.pid[ip];
+      if (p.pid) p.pid_new[pos] = id;
     }
   }
 }
