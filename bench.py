@@ -94,6 +94,10 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            # wait for the first sample, so that the sampler is running when the timed region starts
+            first = self.proc.stdout.readline()
+            if first:
+                self.lines.append(first)
         except (OSError, FileNotFoundError):
             self.proc = None
 
@@ -107,7 +111,7 @@ class Clocks:
             self.proc.kill()
             out, _ = self.proc.communicate()
         rows = []
-        for ln in out.splitlines():
+        for ln in self.lines[1:] + out.splitlines():  # the first sample predates the timed region
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
