@@ -32,10 +32,21 @@ def test_kick_fine_equals_pm3_then_pp(gpu):
     np.testing.assert_allclose(out[2:], vmax, rtol=1e-5)
 
 
-def test_device_api_equals_host_api(gpu):
+def _many_tiles():
+    """125 parent tiles: more than the host kick's per-tile events, so it takes the one-piece
+    path (whole-array copies, one PP launch)."""
+    from cube2_b200 import ic
+    from cube2_b200.layout import Layout, build_image
+    L = Layout(ng=80, nnt=5, nns=2, ratio_cs=4, ngb=4, app=0.1)
+    pos, vel = ic.uniform_random(20000, 80.0, 17)
+    return build_image(pos, vel, L)
+
+
+@pytest.mark.parametrize("case", ["t32", "many_tiles"])
+def test_device_api_equals_host_api(gpu, case):
     import torch
     from cube2_b200.kick import FineKick
-    img, _ = load_golden("t32")
+    img = load_golden("t32")[0] if case == "t32" else _many_tiles()
     L = img.layout
     fk = FineKick(L)
     isort, ires, ix, apm3, rs = _tables(L)
