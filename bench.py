@@ -207,7 +207,7 @@ def run_ours(args, rank, world, local_rank):
     # the PP kernel shape the autotuner picked during the warm-up (cube_pp_shapes)
     from cube2_b200.kick import pp_shapes
     table, cur = pp_shapes()
-    pp_shape = {**{k: table[cur][k] for k in ("chunk", "jtile", "unroll", "blocks")}, "index": cur,
+    pp_shape = {**{k: table[cur][k] for k in ("chunk", "jtile", "unroll", "blocks", "packed")}, "index": cur,
                 "tuning_ms": [round(float(t["ms"]), 3) for t in table],
                 "what": "autotuned on the first kick: work list + PP force kernel timed per shape"}
 

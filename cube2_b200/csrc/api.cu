@@ -85,8 +85,11 @@ struct Ctx {
   // pp_shape_key; pp_ms holds the last tuning's times, pp_last the shape of the last PP kick
   int pp_fixed = -1;
   std::unordered_map<uint64_t, int> pp_tuned;
-  float pp_ms[kMaxPPShapes] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+  float pp_ms[kMaxPPShapes];
   int pp_last = 0;
+  Ctx() {
+    for (float &m : pp_ms) m = -1.0f;
+  }
   Buf pp_scratch;  // tuning runs kick these velocities, not the caller's
   // drift and buffer rebuild scratch
   Buf dr_cb, dr_cb_new, dr_runrank, dr_run_base, dr_runs, dr_ctr, dr_dest_runs, dr_dest_start, dr_scan_tmp,
@@ -734,7 +737,7 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   int64_t interior = 0;
   for (auto &t : m.tiles) interior += (int64_t)L.nt * t.rcp * L.nt * t.rcp * L.nt * t.rcp;
   const int64_t item_cap = interior + d.n_used / pp_min_chunk() + 16;
-  CK(grow(g.items, sizeof(int4) * (size_t)item_cap));
+  CK(grow(g.items, sizeof(PPItem) * (size_t)item_cap));
   CK(grow(g.sched, sizeof(int32_t) * sched_ints(L.ntile)));
   int32_t *ctr = (int32_t *)g.counters.p;  // [0] spill_n [2] err
   BinArgs b{};
@@ -769,7 +772,7 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   p.cell_start = (const int32_t *)g.cell_start.p;
   p.spos = (const float4 *)g.spos.p;
   p.range_loc = (const float *)g.range_loc.p;
-  p.items = (int4 *)g.items.p;
+  p.items = (PPItem *)g.items.p;
   p.sched = (int32_t *)g.sched.p;
   p.item_cap = item_cap;
   p.vp = d.vp;
@@ -1090,6 +1093,7 @@ int cube_pp_shapes(cube_pp_shape_info *out, int32_t cap, int32_t *n_shapes, int3
     out[k].jtile = d.jtile;
     out[k].unroll = d.unroll;
     out[k].blocks = d.blocks;
+    out[k].packed = d.packed;
     out[k].ms = g.pp_ms[k];
   }
   return CUBE_OK;

@@ -49,11 +49,12 @@ constexpr int kWarps = 8;  // warps per block in warp-per-cell kernels
 constexpr int kPPChunk = 16;  // i-particles per PP work item of the default shape (a crowded PP cell is split into chunks)
 
 // PP force kernel shape (pp.cu): i-particles per work item, staged candidates per warp, pair-loop
-// unroll, resident blocks per SM the registers are budgeted for
+// unroll, resident blocks per SM the registers are budgeted for, pair law on packed f32x2
+// arithmetic (two candidates per lane and instruction) or on scalar FP32
 struct PPShapeDesc {
-  int chunk, jtile, unroll, blocks;
+  int chunk, jtile, unroll, blocks, packed;
 };
-constexpr int kMaxPPShapes = 16;
+constexpr int kMaxPPShapes = 32;
 
 // ---------------------------------------------------------------------------------------------
 // device helpers
@@ -116,6 +117,16 @@ size_t bin_smem_bytes(int max_rcp);
 size_t scan_tmp_elems(int64_t n);
 
 // PP work list + force
+// One PP work item (pp.cu): a chunk of at most `chunk` particles of one interior PP cell, with
+// what its warp needs up front; k_pp_items fills it once per kick
+struct __align__(16) PPItem {
+  uint32_t cell;  // global PP cell index
+  int32_t i0;     // first particle of the chunk in the cell-sorted order
+  int32_t dims;   // ni | rcp << 8 | R << 16: particles, PP cells per coarse cell, stencil radius
+  float rc;       // PP range of the cell
+  float cep, k35, h, rc2;  // 2 / rc, 1 / (35 rc^2), ratio_cs / rcp, rc^2
+};
+
 struct PPArgs {
   const Lay *L;
   const TilePP *d_tiles;
@@ -124,7 +135,7 @@ struct PPArgs {
   const int32_t *cell_start;
   const float4 *spos;
   const float *range_loc;   // [ns3] PP range by subtile location
-  int4 *items;              // [item_cap]
+  PPItem *items;            // [item_cap]
   int32_t *sched;           // [sched_ints(ntile)], zeroed by launch_pp_items: bucket counts and
                             // cursors per tile, tile bases, work-queue heads
   int64_t item_cap;

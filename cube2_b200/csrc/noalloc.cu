@@ -37,9 +37,9 @@ constexpr size_t kOffCount = kOffCellBase + na_align(sizeof(int64_t) * kNaCells)
 constexpr size_t kOffStart = kOffCount + na_align(sizeof(int32_t) * kNaCells);         // int32 [cells + 1]
 constexpr size_t kOffScan = kOffStart + na_align(sizeof(int32_t) * (kNaCells + 1));    // int32 scan scratch
 constexpr size_t kOffSpos = kOffScan + na_align(sizeof(int32_t) * (kNaCells / 4096 + 2));
-constexpr size_t kOffItems = kOffSpos + na_align(sizeof(float4) * kNaParticles);       // int4 work list
+constexpr size_t kOffItems = kOffSpos + na_align(sizeof(float4) * kNaParticles);       // PPItem work list
 constexpr size_t kItemCap = kNaCells + kNaParticles / kPPChunk + 16;
-constexpr size_t kOffSpill = kOffItems + na_align(sizeof(int4) * kItemCap);
+constexpr size_t kOffSpill = kOffItems + na_align(sizeof(PPItem) * kItemCap);
 constexpr size_t kOffSpillRank = kOffSpill + na_align(sizeof(Spill) * kNaSpill);
 constexpr size_t kOffTiles = kOffSpillRank + na_align(sizeof(int32_t) * kNaSpill);
 constexpr size_t kOffRange = kOffTiles + na_align(sizeof(TilePP) * kNaTiles);
@@ -118,7 +118,7 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
   int32_t *cell_start = (int32_t *)(base + kOffStart);
   int32_t *scan_tmp = (int32_t *)(base + kOffScan);
   float4 *spos = (float4 *)(base + kOffSpos);
-  int4 *items = (int4 *)(base + kOffItems);
+  PPItem *items = (PPItem *)(base + kOffItems);
   Spill *spill = (Spill *)(base + kOffSpill);
   int32_t *spill_rank = (int32_t *)(base + kOffSpillRank);
   TilePP *d_tiles = (TilePP *)(base + kOffTiles);

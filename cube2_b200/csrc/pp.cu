@@ -26,6 +26,15 @@
 // Kahan-compensated sums updated once per flush of the staging buffer; the
 // groups of a particle are merged with warp shuffles (TwoSum), and the owning
 // lane applies af*mass^2, the kick, f2max and vmax.
+//
+// Packed shapes evaluate the pair law on sm_100's f32x2 arithmetic (FFMA2, FMUL2, FADD2):
+// a lane takes two staged candidates per round, which halves the issue slots of the law;
+// every operation rounds as its scalar form, so each pair's force is bit for bit the scalar
+// one and only the summation order differs.  The kernel is issue-bound, so the per-lane state
+// that is touched once per flush or item (Kahan sums, maxima, the owned particle's velocity,
+// which a cp.async brings in while the item runs) lives in shared memory, and a warp pops
+// its work items four at a time, each carrying its first particle, count, stencil radius
+// and pair-law constants (k_pp_items computes them once per kick).
 #include <type_traits>
 #include <utility>
 
@@ -43,10 +52,14 @@ constexpr int kBuckets = 32;
 // warps; jtile = candidates a warp stages in shared memory between two flushes; unroll = unroll
 // factor of the pair loop; blocks = resident blocks per SM the registers are budgeted for
 // (4: 64 registers a thread, 3: 80).  Shape 0 is the default and the one the pair-count mode uses.
-constexpr PPShapeDesc kShapes[] = {{16, 64, 2, 4},  {8, 128, 1, 4},  {8, 128, 4, 4},  {4, 128, 2, 4},
-                                   {4, 256, 2, 4},  {8, 256, 2, 4},  {8, 128, 2, 4},  {16, 128, 2, 4},
-                                   {16, 128, 4, 4}, {8, 128, 2, 3},  {16, 128, 2, 3}, {16, 64, 1, 4},
-                                   {16, 64, 4, 4},  {16, 64, 2, 3},  {32, 64, 2, 4},  {32, 32, 2, 4}};
+constexpr PPShapeDesc kShapes[] = {
+    {16, 64, 2, 4, 0},  {8, 128, 1, 4, 0},  {8, 128, 4, 4, 0},  {4, 128, 2, 4, 0},  {4, 256, 2, 4, 0},
+    {8, 256, 2, 4, 0},  {8, 128, 2, 4, 0},  {16, 128, 2, 4, 0}, {16, 128, 4, 4, 0}, {8, 128, 2, 3, 0},
+    {16, 128, 2, 3, 0}, {16, 64, 1, 4, 0},  {16, 64, 4, 4, 0},  {16, 64, 2, 3, 0},  {32, 64, 2, 4, 0},
+    {32, 32, 2, 4, 0},  {16, 64, 1, 4, 1},  {8, 128, 1, 4, 1},  {8, 128, 2, 4, 1},  {4, 128, 1, 4, 1},
+    {4, 256, 1, 4, 1},  {8, 256, 1, 4, 1},  {16, 128, 1, 4, 1}, {16, 128, 2, 4, 1}, {8, 128, 1, 3, 1},
+    {16, 128, 1, 3, 1}, {16, 64, 2, 4, 1},  {16, 64, 1, 3, 1},  {32, 64, 1, 4, 1},  {32, 32, 1, 4, 1},
+    {32, 64, 2, 4, 1},  {8, 64, 1, 4, 1}};
 constexpr int kNumShapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
 static_assert(kNumShapes <= kMaxPPShapes, "shape table");
 constexpr int min_shape_chunk() {
@@ -56,8 +69,29 @@ constexpr int min_shape_chunk() {
 }
 constexpr int kMinChunk = min_shape_chunk();  // the work list capacity is sized for it
 static_assert(kShapes[0].chunk == kPPChunk, "shape 0 is the default shape");
-constexpr size_t pp_smem_warp(int jtile) { return sizeof(float4) * (jtile + 32) + sizeof(int2) * kMaxRows; }
-constexpr size_t pp_smem_block(int jtile) { return pp_smem_warp(jtile) * kPPWarps; }
+// per-warp shared memory: the staged candidates (scalar: float4 [jtile + 32]; packed: x, y and z
+// planes of jtile + 64 floats each), then the row table
+constexpr size_t pp_stage_bytes(int jtile, bool packed) {
+  return packed ? 3 * sizeof(float) * (jtile + 64) : sizeof(float4) * (jtile + 32);
+}
+// per-lane state kept in shared memory rather than registers (it is touched once per flush or
+// item): Kahan sums and compensations of x, y, z, f2 and |v| maxima, the owned particle's
+// velocity (copied in asynchronously when the item starts); then the item's bounding box, then
+// the batch of work items the warp popped
+constexpr int kLaneFields = 13;
+constexpr int kPop = 4;  // work items a warp takes from the queue at a time
+constexpr size_t pp_state_bytes() { return sizeof(float) * (kLaneFields * 32 + 8) + sizeof(PPItem) * kPop; }
+constexpr size_t pp_smem_warp(int jtile, bool packed) {
+  return pp_stage_bytes(jtile, packed) + sizeof(int2) * kMaxRows + pp_state_bytes();
+}
+constexpr size_t pp_smem_block(int jtile, bool packed) { return pp_smem_warp(jtile, packed) * kPPWarps; }
+constexpr bool pp_smem_aligned() {
+  for (int jt = 32; jt <= 256; jt += 32)
+    if (pp_smem_warp(jt, false) % 16 || pp_smem_warp(jt, true) % 16 || pp_stage_bytes(jt, true) % 16) return false;
+  return true;
+}
+static_assert(pp_smem_aligned() && (sizeof(int2) * kMaxRows + sizeof(float) * 32 * kLaneFields) % 16 == 0,
+              "16-byte aligned warp areas, bounding box and item batch");
 
 // basic_functions.f08:95-109 / pp_force_kernel.c:45-74 in FP32, same operation order
 __device__ __forceinline__ float F_ra(float r, float apm) {
@@ -76,6 +110,13 @@ __device__ __forceinline__ float F_ra(float r, float apm) {
   return 0.0f;
 }
 
+// packed f32x2 arithmetic (sm_100: one instruction updates both halves, each rounded as the
+// scalar operation)
+__device__ __forceinline__ float2 dup(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
 // s(r^2) = (F_ra(r,app) - F_ra(r,rc)) / r for 0 <= r < rc, so that the pair force is s * (dx, dy, dz).
 // With ep = 2r/rc and k = 1/(35 rc^2), for r > app:
 //   outer (ep > 1): 1/r^2 - F_ra(r,rc) = (32/35)/r^2 - k P(ep),  P = -224 + 896ep - 840ep^2 + 224ep^3
@@ -87,13 +128,13 @@ __device__ __forceinline__ float F_ra(float r, float apm) {
 // per item (2/rc and 1/(35 rc^2)).  Inside the softening length (rare, soft()) the reference's own
 // expression is evaluated.
 struct PairLaw {
-  float cep, k35, app2, app, rc;
-  __device__ __forceinline__ void init(float rc_, float app_) {
-    rc = rc_;
-    app = app_;
-    app2 = app_ * app_;
-    k35 = 1.0f / (35.0f * rc_ * rc_);
-    cep = 2.0f / rc_;
+  float cep, k35;
+  // the constants of range rc, as k_pp_items stores them in the work item
+  __device__ __forceinline__ static float k35_of(float rc_) { return 1.0f / (35.0f * rc_ * rc_); }
+  __device__ __forceinline__ static float cep_of(float rc_) { return 2.0f / rc_; }
+  __device__ __forceinline__ void init(const PPItem &it) {
+    k35 = it.k35;
+    cep = it.cep;
   }
   __device__ __forceinline__ float scale(float r2) const {
     const float invr = rsqrtf(r2);
@@ -112,8 +153,28 @@ struct PairLaw {
     const float br = fmaf(u6, w, 32.0f / 35.0f);
     return fmaf(br, ir2, -q * k35) * invr;
   }
+  // scale() of two squared distances on packed f32x2 arithmetic: every operation is the scalar
+  // one, rounded the same way, so each half equals scale() of that half bit for bit
+  __device__ __forceinline__ float2 scale2(float2 r2) const {
+    const float2 invr = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 ir2 = mul2(invr, invr);
+    const float2 ep = mul2(mul2(r2, invr), dup(cep));
+    float2 q = fma2(dup(7.0f), ep, dup(-48.0f));
+    q = fma2(q, ep, dup(70.0f));
+    q = fma2(q, ep, dup(224.0f));
+    q = fma2(q, ep, dup(-840.0f));
+    q = fma2(q, ep, dup(896.0f));
+    q = fma2(q, ep, dup(-224.0f));
+    float2 u = fma2(ep, dup(-1.0f), dup(1.0f));
+    u = make_float2(fmaxf(u.x, 0.0f), fmaxf(u.y, 0.0f));
+    const float2 u2 = mul2(u, u);
+    const float2 u6 = mul2(mul2(u2, u2), u2);
+    const float2 w = fma2(fma2(dup(7.0f / 35.0f), ep, dup(18.0f / 35.0f)), ep, dup(3.0f / 35.0f));
+    const float2 br = fma2(u6, w, dup(32.0f / 35.0f));
+    return mul2(fma2(br, ir2, mul2(q, dup(-k35))), invr);
+  }
   // 0 < r <= app: the reference's expression
-  __device__ __forceinline__ float soft(float r2) const {
+  __device__ __forceinline__ static float soft(float r2, float app, float rc) {
     const float invr = rsqrtf(r2);
     const float r = r2 * invr;
     return (F_ra(r, app) - F_ra(r, rc)) * invr;
@@ -147,6 +208,14 @@ __device__ __forceinline__ int div_small(int n, int d) { return (n * c_div.m[d])
 __device__ __forceinline__ int lowest_bit(unsigned m) { return __ffs(m) - 1; }
 __device__ __forceinline__ int lowest_bit(unsigned long long m) { return __ffsll(m) - 1; }
 
+// 4-byte asynchronous global -> shared copy (cp.async, sm_80+), its commit and wait
+__device__ __forceinline__ void cp_async4(float *smem, const float *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
   float y = x - c;
   float t = s + y;
@@ -169,12 +238,12 @@ struct PPK {
   const int32_t *cs;
   const float4 *spos;
   const float *range_loc;
-  int4 *items;      // (global cell, chunk, tile, PP range bits), tile-major, heaviest bucket first
+  PPItem *items;    // tile-major, heaviest bucket first
   int32_t *sched;   // schedule words, layout in sched_ints()
   int64_t item_cap;
   int t_lo, t_hi;   // tiles of this force launch; its queue head is sched_head(t_lo, t_hi)
   float *vp;
-  float mass2, kick, app;
+  float mass2, kick, app, app2;
   float *out;
   int want_vmax;
   int32_t *err;
@@ -232,19 +301,27 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
   const int rcp = tp.rcp, S = tp.S, npg = p.nt * rcp;
   const int64_t ncell = (int64_t)npg * npg * npg;
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int nfull = 0, bfull = 0, brem = -1, rcbits = 0;
+  int nfull = 0, bfull = 0, brem = -1, ni = 0, i0 = 0;
   int64_t g = 0;
+  PPItem it{};
   if (c < ncell) {
     const int x = (int)(c % npg) + rcp, y = (int)((c / npg) % npg) + rcp, z = (int)(c / ((int64_t)npg * npg)) + rcp;
     g = tp.cell0 + ((int64_t)z * S + y) * S + x;
-    const int ni = p.cs[g + 1] - p.cs[g];
+    i0 = p.cs[g];
+    ni = p.cs[g + 1] - i0;
     if (ni > 0) {
       const float rc = cell_range(p, t, x, y, z, rcp);
-      rcbits = __float_as_int(rc);
       const int R = stencil_radius(rc, rcp, p.rcs);
       if (R > rcp) atomicOr(p.err, 1 << CUBE_ERR_INVALID);  // beyond the one coarse-cell halo
       const float h = (float)p.rcs / (float)rcp;
       const int Rc = min(R, rcp);
+      it.cell = (uint32_t)g;
+      it.dims = (rcp << 8) | (Rc << 16);
+      it.rc = rc;
+      it.cep = PairLaw::cep_of(rc);
+      it.k35 = PairLaw::k35_of(rc);
+      it.h = h;
+      it.rc2 = rc * rc;
       int64_t nj = 0;
       for (int dz = -Rc; dz <= Rc; dz++)
         for (int dy = -Rc; dy <= Rc; dy++) {
@@ -272,13 +349,18 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
   if (PASS == 1) {
     __syncthreads();
     const int64_t f0 = (int64_t)sbase[bfull] + rfull;
+    const int dims = it.dims;
     for (int k = 0; k < nfull; k++) {
-      if (f0 + k < p.item_cap) p.items[f0 + k] = make_int4((int)g, k, t, rcbits);
+      it.i0 = i0 + k * C;
+      it.dims = dims | C;
+      if (f0 + k < p.item_cap) p.items[f0 + k] = it;
       else atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
     }
     if (brem >= 0) {
       const int64_t slot = (int64_t)sbase[brem] + rrem;
-      if (slot < p.item_cap) p.items[slot] = make_int4((int)g, nfull, t, rcbits);
+      it.i0 = i0 + nfull * C;
+      it.dims = dims | (ni - nfull * C);
+      if (slot < p.item_cap) p.items[slot] = it;
       else atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
     }
   }
@@ -307,54 +389,61 @@ __global__ void k_pp_offsets(int32_t *sched, int ntile) {
 // COUNT = false: forces and kick.  COUNT = true: only count the accepted ordered
 // pairs 0 < r^2 < rc^2 (the algorithmic work of the kick, for the roofline).
 // Shape: C i-particles per item, J staged candidates per flush, pair loop unrolled U times,
-// registers budgeted for B resident blocks per SM.
-template <bool COUNT, int C, int J, int U, int B>
+// registers budgeted for B resident blocks per SM, pair law on packed f32x2 arithmetic (PK).
+template <bool COUNT, int C, int J, int U, int B, bool PK>
 __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
-  // a flush has at most J / floor(32 / C) rounds, one bit each in the soft-pair mask
-  constexpr int kRounds = J / (32 / C);
-  static_assert(kRounds <= 64, "at most 64 rounds per flush");
-  using Mask = typename std::conditional<(kRounds > 32), unsigned long long, unsigned>::type;
+  // a flush has at most ceil(J / floor(32 / C)) rounds (packed: pair rounds, two candidates
+  // each), one bit per round and lane in the soft-pair mask
+  constexpr int kNg = 32 / C;
+  constexpr int kBits = PK ? (J + 2 * kNg - 1) / (2 * kNg) : (J + kNg - 1) / kNg;
+  static_assert(kBits <= 64, "at most 64 soft-pair bits per flush");
+  static_assert(!(COUNT && PK), "the pair count runs the scalar loop");
+  using Mask = typename std::conditional<(kBits > 32), unsigned long long, unsigned>::type;
   extern __shared__ float4 pp_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float4 *buf = reinterpret_cast<float4 *>(reinterpret_cast<char *>(pp_smem) + warp * pp_smem_warp(J));
-  int2 *rows = reinterpret_cast<int2 *>(buf + J + 32);  // (end of the row in the walk, start - walk offset)
-  // items [first, last) of tiles [t_lo, t_hi), popped through this launch's own queue head
-  const int32_t *tbase = p.sched + sched_base(p.ntile);
-  const int first = tbase[p.t_lo];
-  const int last = (int)min((int64_t)tbase[p.t_hi], p.item_cap);
-  int32_t *head = p.sched + sched_head(p.ntile, p.t_lo, p.t_hi);
-  float f2w = 0.f, vm0 = 0.f, vm1 = 0.f, vm2 = 0.f;
+  char *wbase = reinterpret_cast<char *>(pp_smem) + warp * pp_smem_warp(J, PK);
+  float4 *buf = reinterpret_cast<float4 *>(wbase);  // scalar staging: float4 [J + 32]
+  float *X = reinterpret_cast<float *>(wbase);      // packed staging: planes of J + 64 floats
+  float *Y = X + (J + 64), *Z = Y + (J + 64);
+  // (end of the row in the walk, start - walk offset)
+  int2 *rows = reinterpret_cast<int2 *>(wbase + pp_stage_bytes(J, PK));
+  float *const ks = reinterpret_cast<float *>(rows + kMaxRows) + lane;  // field f at ks[32 f]
+  float *const bbox = reinterpret_cast<float *>(rows + kMaxRows) + 32 * kLaneFields;
+  PPItem *const batch = reinterpret_cast<PPItem *>(bbox + 8);
+  for (int f = 6; f < 10; f++) ks[32 * f] = 0.f;  // f2, |v| maxima
   unsigned long long npairs = 0;
-  for (;;) {
-    int it = 0;
-    if (lane == 0) it = first + atomicAdd(head, 1);
-    it = __shfl_sync(0xffffffffu, it, 0);
-    if (it >= last) break;
-    const int4 item = p.items[it];
-    const int64_t g = (int64_t)(unsigned)item.x;
-    const int t = item.z;
-    const TilePP tp = p.tiles[t];
-    const int S = tp.S, rcp = tp.rcp;
-    const float rc = __int_as_float(item.w);
-    const float rc2 = rc * rc;
-    const int R = min(stencil_radius(rc, rcp, p.rcs), rcp);
-    const float h = (float)p.rcs / (float)rcp;
+  // The warp takes kPop consecutive items per queue pop (one atomic and one load for all of
+  // them); the items of a bucket cost about the same, and the lightest come last.
+  for (int nb = 0, b = 0;; b++) {
+    if (b == nb) {
+      // items [first, last) of tiles [t_lo, t_hi), popped through this launch's own queue head
+      const int32_t *tbase = p.sched + sched_base(p.ntile);
+      const int first = tbase[p.t_lo];
+      const int last = (int)min((int64_t)tbase[p.t_hi], p.item_cap);
+      int it = 0;
+      if (lane == 0) it = first + atomicAdd(p.sched + sched_head(p.ntile, p.t_lo, p.t_hi), kPop);
+      it = __shfl_sync(0xffffffffu, it, 0);
+      if (it >= last) break;
+      nb = min(kPop, last - it);
+      b = 0;
+      __syncwarp();
+      if (lane < 2 * nb) reinterpret_cast<int4 *>(batch)[lane] = reinterpret_cast<const int4 *>(p.items + it)[lane];
+      __syncwarp();
+    }
+    const PPItem &item = batch[b];  // read from shared memory where used
+    const int64_t g = (int64_t)item.cell;
+    const int ni = item.dims & 0xff, R = item.dims >> 16;
+    const int S = ((item.dims >> 8) & 0xff) * (p.nt + 2);
+    const float rc2 = item.rc2;
     PairLaw law;
-    law.init(rc, p.app);
-
-    const int i0 = p.cs[g] + item.y * C;
-    const int ni = min(C, p.cs[g + 1] - i0);
+    law.init(item);
     // lanes = ngrp groups of ni lanes; group `grp` walks every ngrp-th candidate
     const int ngrp = 32 / ni;
     const int grp = div_small(lane, ni), il = lane - grp * ni;
     const bool has_i = grp < ngrp;  // the 32 mod ni leftover lanes idle
-    const float4 pi = p.spos[i0 + il];
-
-    // bounding box of the item's particles: candidates farther than rc from it are dropped
-    // while staging, so the pair loop below only sees possibly-interacting candidates
-    const float blx = warp_min_redux(pi.x), bhx = warp_max_redux(pi.x), bly = warp_min_redux(pi.y),
-                bhy = warp_max_redux(pi.y), blz = warp_min_redux(pi.z), bhz = warp_max_redux(pi.z);
-    float sx_ = 0.f, cx_ = 0.f, sy_ = 0.f, cy_ = 0.f, sz_ = 0.f, cz_ = 0.f;
+    const float4 pi = p.spos[item.i0 + il];
+    bool boxed = false;  // the bounding box is taken once pi has arrived (after the first row table)
+    for (int f = 0; f < 6; f++) ks[32 * f] = 0.f;  // Kahan sums of this item
     int nbuf = 0;  // staged candidates (warp-uniform)
     // Evaluate the staged candidates: group grp takes buf[grp + k*ngrp] in round k.  The loop
     // bound is the same for every lane (no divergent loop exits): the slots past nbuf hold a
@@ -363,7 +452,66 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
     // no branch: pairs inside the softening length (r <= app, common only in dense clumps) are
     // masked out of it and their rounds recorded in a bit mask (at most 32 rounds per flush);
     // a second loop then evaluates exactly those pairs, one per lane per step.
+    // Packed: candidates 2m and 2m + 1 form pair slot m, and group grp takes slots grp + k*ngrp;
+    // its two halves are summed separately and added at the end of the flush.
+    auto flush_packed = [&]() {
+      X[nbuf + lane] = 1e18f;
+      Y[nbuf + lane] = 1e18f;
+      Z[nbuf + lane] = 1e18f;
+      X[nbuf + 32 + lane] = 1e18f;
+      Y[nbuf + 32 + lane] = 1e18f;
+      Z[nbuf + 32 + lane] = 1e18f;
+      __syncwarp();
+      float2 px = dup(0.f), py = dup(0.f), pz = dup(0.f);
+      const int nround = div_small(nbuf + 2 * ngrp - 1, 2 * ngrp);
+      Mask softmask = 0u, bit = 1u;
+      const float2 *X2 = reinterpret_cast<const float2 *>(X);
+      const float2 nx = dup(-pi.x), ny = dup(-pi.y), nz = dup(-pi.z);
+      int m = grp;
+#pragma unroll U
+      for (int k = 0; k < nround; k++, m += ngrp, bit <<= 1) {
+        const float2 dx = add2(X2[m], nx), dy_ = add2(X2[m + (J + 64) / 2], ny),
+                     dz_ = add2(X2[m + (J + 64)], nz);
+        const float2 r2 = fma2(dx, dx, fma2(dy_, dy_, mul2(dz_, dz_)));
+        float2 s = law.scale2(r2);
+        const bool fx = r2.x > p.app2, fy = r2.y > p.app2;
+        s.x = fx & (r2.x < rc2) ? s.x : 0.0f;
+        s.y = fy & (r2.y < rc2) ? s.y : 0.0f;
+        if ((!fx & (r2.x > 0.0f)) | (!fy & (r2.y > 0.0f))) softmask |= bit;
+        px = fma2(s, dx, px);
+        py = fma2(s, dy_, py);
+        pz = fma2(s, dz_, pz);
+      }
+      if (!has_i) softmask = 0u;
+      // a flagged pair round holds one or two soft pairs: both halves are tested again
+      while (__any_sync(0xffffffffu, softmask != 0u)) {
+        if (softmask) {
+          const int c = 2 * (grp + lowest_bit(softmask) * ngrp);
+          softmask &= softmask - 1u;
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            const float dx = X[c + e] - pi.x, dy_ = Y[c + e] - pi.y, dz_ = Z[c + e] - pi.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_));
+            if ((r2 <= p.app2) & (r2 > 0.0f)) {
+              const float s = PairLaw::soft(r2, p.app, item.rc);
+              px.x = fmaf(s, dx, px.x);
+              py.x = fmaf(s, dy_, py.x);
+              pz.x = fmaf(s, dz_, pz.x);
+            }
+          }
+        }
+      }
+      kahan_add(ks[0], ks[32], px.x + px.y);
+      kahan_add(ks[64], ks[96], py.x + py.y);
+      kahan_add(ks[128], ks[160], pz.x + pz.y);
+      nbuf = 0;
+      __syncwarp();
+    };
     auto flush = [&]() {
+      if constexpr (PK) {
+        flush_packed();
+        return;
+      }
       buf[nbuf + lane] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
       __syncwarp();
       float px = 0.f, py = 0.f, pz = 0.f;
@@ -381,8 +529,8 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
           // evaluated for every candidate and masked: a divergent accept branch would
           // run on nearly every round of a 32-lane warp anyway
           float s = law.scale(r2);
-          s = (r2 < rc2) & (r2 > law.app2) ? s : 0.0f;
-          softmask |= (r2 <= law.app2) & (r2 > 0.0f) & has_i ? bit : 0u;
+          s = (r2 < rc2) & (r2 > p.app2) ? s : 0.0f;
+          softmask |= (r2 <= p.app2) & (r2 > 0.0f) & has_i ? bit : 0u;
           px = fmaf(s, dx, px);
           py = fmaf(s, dy_, py);
           pz = fmaf(s, dz_, pz);
@@ -395,15 +543,15 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
             softmask &= softmask - 1u;
             const float4 pj = buf[grp + k * ngrp];
             const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
-            const float s = law.soft(fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_)));
+            const float s = PairLaw::soft(fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_)), p.app, item.rc);
             px = fmaf(s, dx, px);
             py = fmaf(s, dy_, py);
             pz = fmaf(s, dz_, pz);
           }
         }
-        kahan_add(sx_, cx_, px);
-        kahan_add(sy_, cy_, py);
-        kahan_add(sz_, cz_, pz);
+        kahan_add(ks[0], ks[32], px);
+        kahan_add(ks[64], ks[96], py);
+        kahan_add(ks[128], ks[160], pz);
       }
       nbuf = 0;
       __syncwarp();
@@ -421,7 +569,7 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
         if (ri < nr) {
           const int q = div_small(ri, side);
           const int dz = q - R, dy = ri - q * side - R;
-          need = row_needed(dy, dz, h, rc2);
+          need = row_needed(dy, dz, item.h, rc2);
           if (need) {
             const int64_t b = g + ((int64_t)dz * S + dy) * S;
             js = p.cs[b - R];
@@ -439,6 +587,26 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
         walk += __shfl_sync(0xffffffffu, incl, 31);
       }
       __syncwarp();
+      if (!boxed) {
+        // bounding box of the item's particles: candidates farther than rc from it are dropped
+        // while staging, so the pair loop below only sees possibly-interacting candidates
+        boxed = true;
+        const float blx = warp_min_redux(pi.x), bhx = warp_max_redux(pi.x), bly = warp_min_redux(pi.y),
+                    bhy = warp_max_redux(pi.y), blz = warp_min_redux(pi.z), bhz = warp_max_redux(pi.z);
+        if (lane == 0) {
+          *reinterpret_cast<float4 *>(bbox) = make_float4(blx, bly, blz, bhx);
+          *reinterpret_cast<float2 *>(bbox + 4) = make_float2(bhy, bhz);
+        }
+        // the owned particle's velocity is copied in while the item runs
+        if (!COUNT && grp == 0 && has_i) {
+          const float *v = p.vp + 3 * (int64_t)__float_as_int(pi.w);
+          cp_async4(ks + 320, v);
+          cp_async4(ks + 352, v + 1);
+          cp_async4(ks + 384, v + 2);
+        }
+        cp_async_commit();
+        __syncwarp();
+      }
       if (walk == 0) continue;
       // Walk position -> particle.  Each lane's row index only moves forward and stops at the
       // last row (rows[nrows-1].x = walk > v), and the lanes past the end load the last
@@ -453,12 +621,23 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
       for (int vb = 0; vb < walk; vb += 32) {
         const float4 pj = nxt;
         nxt = p.spos[locate(vb + 32 + lane)];  // one step ahead
-        const float ex = fmaxf(fmaxf(blx - pj.x, pj.x - bhx), 0.f);
-        const float ey = fmaxf(fmaxf(bly - pj.y, pj.y - bhy), 0.f);
-        const float ez = fmaxf(fmaxf(blz - pj.z, pj.z - bhz), 0.f);
+        const float4 bl = *reinterpret_cast<const float4 *>(bbox);  // (lo x, y, z, hi x)
+        const float2 bh = *reinterpret_cast<const float2 *>(bbox + 4);  // (hi y, z)
+        const float ex = fmaxf(fmaxf(bl.x - pj.x, pj.x - bl.w), 0.f);
+        const float ey = fmaxf(fmaxf(bl.y - pj.y, pj.y - bh.x), 0.f);
+        const float ez = fmaxf(fmaxf(bl.z - pj.z, pj.z - bh.y), 0.f);
         const bool keep = (vb + lane < walk) & (ex * ex + ey * ey + ez * ez < rc2);
         const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (keep) buf[nbuf + __popc(m & ((1u << lane) - 1u))] = pj;
+        if (keep) {
+          const int q = nbuf + __popc(m & ((1u << lane) - 1u));
+          if constexpr (PK) {
+            X[q] = pj.x;
+            Y[q] = pj.y;
+            Z[q] = pj.z;
+          } else {
+            buf[q] = pj;
+          }
+        }
         nbuf += __popc(m);
         if (nbuf > J - 32) flush();
       }
@@ -467,7 +646,7 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
     if (nbuf) flush();
     // merge the lane groups of each i-particle (tree over groups, stride s*ni lanes);
     // Kahan c is the negated low part
-    float hx = sx_, lx = -cx_, hy = sy_, ly = -cy_, hz = sz_, lz = -cz_;
+    float hx = ks[0], lx = -ks[32], hy = ks[64], ly = -ks[96], hz = ks[128], lz = -ks[160];
     for (int s = 1; s < ngrp; s <<= 1) {
       const int delta = s * ni;
       const float ohx = __shfl_down_sync(0xffffffffu, hx, delta), olx = __shfl_down_sync(0xffffffffu, lx, delta);
@@ -481,16 +660,17 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
     }
     if (!COUNT && grp == 0 && has_i) {
       const float ax = (hx + lx) * p.mass2, ay = (hy + ly) * p.mass2, az = (hz + lz) * p.mass2;
-      f2w = fmaxf(f2w, ax * ax + ay * ay + az * az);
+      ks[192] = fmaxf(ks[192], ax * ax + ay * ay + az * az);
       const int64_t ip = (int64_t)__float_as_int(pi.w);
       float *v = p.vp + 3 * ip;
-      const float v0 = v[0] + ax * p.kick, v1 = v[1] + ay * p.kick, v2 = v[2] + az * p.kick;
+      cp_async_wait_all();
+      const float v0 = ks[320] + ax * p.kick, v1 = ks[352] + ay * p.kick, v2 = ks[384] + az * p.kick;
       v[0] = v0;
       v[1] = v1;
       v[2] = v2;
-      vm0 = fmaxf(vm0, fabsf(v0));
-      vm1 = fmaxf(vm1, fabsf(v1));
-      vm2 = fmaxf(vm2, fabsf(v2));
+      ks[224] = fmaxf(ks[224], fabsf(v0));
+      ks[256] = fmaxf(ks[256], fabsf(v1));
+      ks[288] = fmaxf(ks[288], fabsf(v2));
     }
   }
   if (COUNT) {
@@ -498,12 +678,10 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
     if (lane == 0) atomicAdd(p.pairs, npairs);
     return;
   }
-  f2w = warp_max(f2w);
+  const float f2w = warp_max(ks[192]);
   if (lane == 0) atomic_max_nonneg(&p.out[1], f2w);
   if (p.want_vmax) {
-    vm0 = warp_max(vm0);
-    vm1 = warp_max(vm1);
-    vm2 = warp_max(vm2);
+    const float vm0 = warp_max(ks[224]), vm1 = warp_max(ks[256]), vm2 = warp_max(ks[288]);
     if (lane == 0) {
       atomic_max_nonneg(&p.out[2], vm0);
       atomic_max_nonneg(&p.out[3], vm1);
@@ -534,6 +712,7 @@ static PPK make_ppk(const PPArgs &a) {
   p.mass2 = a.mass2;
   p.kick = a.kick;
   p.app = L.app;
+  p.app2 = L.app * L.app;
   p.out = a.out;
   p.want_vmax = a.want_vmax;
   p.err = a.err;
@@ -576,8 +755,8 @@ void launch_pp_items(const PPArgs &a, cudaStream_t s) {
 template <bool COUNT, int S>
 static void launch_force_shape(const PPK &p, int num_sms, cudaStream_t s) {
   constexpr PPShapeDesc d = kShapes[S];
-  constexpr size_t smem = pp_smem_block(d.jtile);
-  auto fn = k_pp_force<COUNT, d.chunk, d.jtile, d.unroll, d.blocks>;
+  constexpr size_t smem = pp_smem_block(d.jtile, d.packed != 0);
+  auto fn = k_pp_force<COUNT, d.chunk, d.jtile, d.unroll, d.blocks, d.packed != 0>;
   static int per_sm = 0;
   if (!per_sm) {
     cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

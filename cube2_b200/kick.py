@@ -100,7 +100,7 @@ def _f32(a):
 
 class CPPShape(ctypes.Structure):
     _fields_ = [("chunk", ctypes.c_int32), ("jtile", ctypes.c_int32), ("unroll", ctypes.c_int32),
-                ("blocks", ctypes.c_int32), ("ms", ctypes.c_float)]
+                ("blocks", ctypes.c_int32), ("packed", ctypes.c_int32), ("ms", ctypes.c_float)]
 
 
 def pp_set_shape(shape: int = -1):
@@ -109,8 +109,8 @@ def pp_set_shape(shape: int = -1):
 
 
 def pp_shapes():
-    """(table, current): the PP kernel shapes as dicts (chunk, jtile, unroll, blocks, ms of the
-    last tuning or -1) and the index of the shape the last PP kick used."""
+    """(table, current): the PP kernel shapes as dicts (chunk, jtile, unroll, blocks, packed, ms of
+    the last tuning or -1) and the index of the shape the last PP kick used."""
     n, cur = ctypes.c_int32(), ctypes.c_int32()
     _check(lib().cube_pp_shapes(None, 0, ctypes.byref(n), ctypes.byref(cur)), "cube_pp_shapes")
     arr = (CPPShape * n.value)()

@@ -240,14 +240,16 @@ int cube_power_spectrum(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const i
 /* The PP force kernel comes in several shapes: `chunk` i-particles per work item (a
  * crowded PP cell of n particles is split into ceil(n / chunk) items, one warp each),
  * `jtile` candidates a warp stages in shared memory between flushes, the pair loop
- * unrolled `unroll` times, registers budgeted for `blocks` resident blocks per SM.  By
+ * unrolled `unroll` times, registers budgeted for `blocks` resident blocks per SM, and
+ * `packed` = 1 for the pair law on packed f32x2 arithmetic (two candidates per lane and
+ * instruction; each pair's force is the scalar one bit for bit).  By
  * default the first PP kick of each (layout, per-tile PP grids, PP ranges, octave of
  * n_used) times every shape on its own particles (work list + force kernel, into scratch
  * velocities; the host waits for it once) and that key keeps the fastest; a kick being
  * captured into a graph that meets an untimed key uses shape 0.  Results of different
  * shapes differ only by FP32 summation order. */
 typedef struct cube_pp_shape_info {
-  int32_t chunk, jtile, unroll, blocks;
+  int32_t chunk, jtile, unroll, blocks, packed;
   float ms; /* the last tuning's time of the shape (work list + force kernel), -1 if never timed */
 } cube_pp_shape_info;
 /* shape >= 0: use that shape for every PP kick; -1: autotune (default; forgets earlier picks). */
