@@ -76,8 +76,8 @@ constexpr size_t pp_stage_bytes(int jtile, bool packed) {
 }
 // per-lane state kept in shared memory rather than registers (it is touched once per flush or
 // item): Kahan sums and compensations of x, y, z, f2 and |v| maxima, the owned particle's
-// velocity (copied in asynchronously when the item starts); then the item's bounding box, then
-// the batch of work items the warp popped
+// velocity (copied in asynchronously when the item starts); then the item's bounding box and
+// the row-table cache, then the batch of work items the warp popped
 constexpr int kLaneFields = 13;
 constexpr int kPop = 4;  // work items a warp takes from the queue at a time
 constexpr size_t pp_state_bytes() { return sizeof(float) * (kLaneFields * 32 + 8) + sizeof(PPItem) * kPop; }
@@ -93,21 +93,27 @@ constexpr bool pp_smem_aligned() {
 static_assert(pp_smem_aligned() && (sizeof(int2) * kMaxRows + sizeof(float) * 32 * kLaneFields) % 16 == 0,
               "16-byte aligned warp areas, bounding box and item batch");
 
-// basic_functions.f08:95-109 / pp_force_kernel.c:45-74 in FP32, same operation order
-__device__ __forceinline__ float F_ra(float r, float apm) {
-  float ep = 2.0f * r / apm;
-  if (apm == 0.0f || ep > 2.0f) return 1.0f / (r * r);
-  if (ep > 1.0f) {
-    float ep2 = ep * ep, ep3 = ep2 * ep, ep4 = ep3 * ep, ep5 = ep4 * ep, ep6 = ep5 * ep;
-    return (1.0f / 35.0f / (apm * apm)) *
-           (12.0f / ep2 - 224.0f + 896.0f * ep - 840.0f * ep2 + 224.0f * ep3 + 70.0f * ep4 - 48.0f * ep5 +
-            7.0f * ep6);
-  }
-  if (ep > 0.0f) {
-    float ep3 = ep * ep * ep, ep4 = ep3 * ep, ep5 = ep4 * ep, ep6 = ep5 * ep;
-    return (1.0f / 35.0f / (apm * apm)) * (224.0f * ep - 224.0f * ep3 + 70.0f * ep4 + 48.0f * ep5 - 21.0f * ep6);
-  }
-  return 0.0f;
+// F_ra(r, apm) of basic_functions.f08:95-109 / pp_force_kernel.c:45-74 in FP32 without
+// divisions or branches: with ep = 2r/apm = r * ce and k = (1/35) / apm^2,
+//   ep <= 1: k (224ep - 224ep^3 + 70ep^4 + 48ep^5 - 21ep^6)
+//   ep > 1:  k (12/ep^2 - 224 + 896ep - 840ep^2 + 224ep^3 + 70ep^4 - 48ep^5 + 7ep^6)
+//            = (3/35)/r^2 + k (-224 + 896ep - ... + 7ep^6)      (k 12/ep^2 = (3/35)/r^2)
+//   ep > 2:  1/r^2
+__device__ __forceinline__ float F_ra_soft(float r, float ir2, float ce, float k) {
+  const float ep = r * ce;
+  float qo = fmaf(7.0f, ep, -48.0f);
+  qo = fmaf(qo, ep, 70.0f);
+  qo = fmaf(qo, ep, 224.0f);
+  qo = fmaf(qo, ep, -840.0f);
+  qo = fmaf(qo, ep, 896.0f);
+  qo = fmaf(qo, ep, -224.0f);
+  float qi = fmaf(-21.0f, ep, 48.0f);
+  qi = fmaf(qi, ep, 70.0f);
+  qi = fmaf(qi, ep, -224.0f);
+  qi = qi * ep;
+  qi = fmaf(qi, ep, 224.0f);
+  qi = qi * ep;
+  return ep > 2.0f ? ir2 : (ep > 1.0f ? fmaf(k, qo, (3.0f / 35.0f) * ir2) : k * qi);
 }
 
 // packed f32x2 arithmetic (sm_100: one instruction updates both halves, each rounded as the
@@ -125,8 +131,8 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 //                    = (1/r^2) (1-ep)^6 (3/35 + 18/35 ep + 7/35 ep^2)
 // (expanding the product gives back the inner polynomial 224ep - 224ep^3 + 70ep^4 + 48ep^5 - 21ep^6).
 // The polynomial coefficients are literals (instruction immediates), so a law costs two registers
-// per item (2/rc and 1/(35 rc^2)).  Inside the softening length (rare, soft()) the reference's own
-// expression is evaluated.
+// per item (2/rc and 1/(35 rc^2)).  Inside the softening length (soft(), a second pass over
+// the pairs the main loop flags) both F_ra terms are evaluated directly.
 struct PairLaw {
   float cep, k35;
   // the constants of range rc, as k_pp_items stores them in the work item
@@ -173,11 +179,11 @@ struct PairLaw {
     const float2 br = fma2(u6, w, dup(32.0f / 35.0f));
     return mul2(fma2(br, ir2, mul2(q, dup(-k35))), invr);
   }
-  // 0 < r <= app: the reference's expression
-  __device__ __forceinline__ static float soft(float r2, float app, float rc) {
+  // 0 < r <= app: (F_ra(r, app) - F_ra(r, rc)) / r; cea = 2/app, ka = (1/35)/app^2
+  __device__ __forceinline__ float soft(float r2, float cea, float ka) const {
     const float invr = rsqrtf(r2);
-    const float r = r2 * invr;
-    return (F_ra(r, app) - F_ra(r, rc)) * invr;
+    const float r = r2 * invr, ir2 = invr * invr;
+    return (F_ra_soft(r, ir2, cea, ka) - F_ra_soft(r, ir2, cep, k35)) * invr;
   }
 };
 
@@ -244,6 +250,7 @@ struct PPK {
   int t_lo, t_hi;   // tiles of this force launch; its queue head is sched_head(t_lo, t_hi)
   float *vp;
   float mass2, kick, app, app2;
+  float cea, ka;  // softening-law constants 2/app and (1/35)/app^2 (0 without softening)
   float *out;
   int want_vmax;
   int32_t *err;
@@ -410,6 +417,9 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
   float *const ks = reinterpret_cast<float *>(rows + kMaxRows) + lane;  // field f at ks[32 f]
   float *const bbox = reinterpret_cast<float *>(rows + kMaxRows) + 32 * kLaneFields;
   PPItem *const batch = reinterpret_cast<PPItem *>(bbox + 8);
+  int *const tcache = reinterpret_cast<int *>(bbox + 6);  // cell and walk of the row table
+  if (lane == 0) tcache[0] = -1;
+  __syncwarp();
   for (int f = 6; f < 10; f++) ks[32 * f] = 0.f;  // f2, |v| maxima
   unsigned long long npairs = 0;
   // The warp takes kPop consecutive items per queue pop (one atomic and one load for all of
@@ -493,7 +503,7 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
             const float dx = X[c + e] - pi.x, dy_ = Y[c + e] - pi.y, dz_ = Z[c + e] - pi.z;
             const float r2 = fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_));
             if ((r2 <= p.app2) & (r2 > 0.0f)) {
-              const float s = PairLaw::soft(r2, p.app, item.rc);
+              const float s = law.soft(r2, p.cea, p.ka);
               px.x = fmaf(s, dx, px.x);
               py.x = fmaf(s, dy_, py.x);
               pz.x = fmaf(s, dz_, pz.x);
@@ -543,7 +553,7 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
             softmask &= softmask - 1u;
             const float4 pj = buf[grp + k * ngrp];
             const float dx = pj.x - pi.x, dy_ = pj.y - pi.y, dz_ = pj.z - pi.z;
-            const float s = PairLaw::soft(fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_)), p.app, item.rc);
+            const float s = law.soft(fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_)), p.cea, p.ka);
             px = fmaf(s, dx, px);
             py = fmaf(s, dy_, py);
             pz = fmaf(s, dz_, pz);
@@ -559,9 +569,17 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
     // The needed stencil rows are laid end to end in a table of up to kMaxRows rows: row k
     // covers walk positions [rows[k-1].x, rows[k].x), and walk position v is particle
     // v + rows[k].y.  Stencils with more rows (large R) are walked in several tables.
+    // Consecutive items of one cell share their stencil: a table that holds the whole stencil is
+    // kept for the next item (tcache: its cell, or -1, and its walk length).
     const int side = 2 * R + 1, nr = side * side;
     for (int r0 = 0; r0 < nr;) {
       int nrows = 0, walk = 0;
+      const bool reuse = r0 == 0 && tcache[0] == (int)item.cell;
+      if (reuse) {
+        walk = tcache[1];
+        r0 = nr;
+      }
+      const int rstart = r0;
       for (; r0 < nr && nrows <= kMaxRows - 32; r0 += 32) {
         const int ri = r0 + lane;
         int js = 0, len = 0;
@@ -585,6 +603,10 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
         if (need) rows[nrows + __popc(m & ((1u << lane) - 1u))] = make_int2(walk + incl, js - (walk + incl - len));
         nrows += __popc(m);
         walk += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      if (!reuse && lane == 0) {
+        tcache[0] = rstart == 0 && r0 >= nr ? (int)item.cell : -1;
+        tcache[1] = walk;
       }
       __syncwarp();
       if (!boxed) {
@@ -713,6 +735,8 @@ static PPK make_ppk(const PPArgs &a) {
   p.kick = a.kick;
   p.app = L.app;
   p.app2 = L.app * L.app;
+  p.cea = L.app > 0.f ? 2.0f / L.app : 0.f;
+  p.ka = L.app > 0.f ? (1.0f / 35.0f) / (L.app * L.app) : 0.f;
   p.out = a.out;
   p.want_vmax = a.want_vmax;
   p.err = a.err;
