@@ -51,15 +51,15 @@ constexpr int kBuckets = 32;
 // chunk = i-particles per work item, so a crowded PP cell of n particles gets ceil(n / chunk)
 // warps; jtile = candidates a warp stages in shared memory between two flushes; unroll = unroll
 // factor of the pair loop; blocks = resident blocks per SM the registers are budgeted for
-// (4: 64 registers a thread, 3: 80).  Shape 0 is the default and the one the pair-count mode uses.
+// (4: 64 registers a thread, 3: 80), packed = pair law on f32x2 arithmetic.  Shape 0 is the
+// default; the last shape is the scalar form, kept for comparison.
 constexpr PPShapeDesc kShapes[] = {
-    {16, 64, 2, 4, 0},  {8, 128, 1, 4, 0},  {8, 128, 4, 4, 0},  {4, 128, 2, 4, 0},  {4, 256, 2, 4, 0},
-    {8, 256, 2, 4, 0},  {8, 128, 2, 4, 0},  {16, 128, 2, 4, 0}, {16, 128, 4, 4, 0}, {8, 128, 2, 3, 0},
-    {16, 128, 2, 3, 0}, {16, 64, 1, 4, 0},  {16, 64, 4, 4, 0},  {16, 64, 2, 3, 0},  {32, 64, 2, 4, 0},
-    {32, 32, 2, 4, 0},  {16, 64, 1, 4, 1},  {8, 128, 1, 4, 1},  {8, 128, 2, 4, 1},  {4, 128, 1, 4, 1},
-    {4, 256, 1, 4, 1},  {8, 256, 1, 4, 1},  {16, 128, 1, 4, 1}, {16, 128, 2, 4, 1}, {8, 128, 1, 3, 1},
-    {16, 128, 1, 3, 1}, {16, 64, 2, 4, 1},  {16, 64, 1, 3, 1},  {32, 64, 1, 4, 1},  {32, 32, 1, 4, 1},
-    {32, 64, 2, 4, 1},  {8, 64, 1, 4, 1}};
+    {16, 128, 2, 4, 1}, {16, 128, 1, 4, 1}, {16, 256, 2, 4, 1}, {16, 128, 4, 4, 1}, {16, 64, 2, 4, 1},
+    {16, 128, 2, 3, 1}, {16, 256, 1, 4, 1}, {8, 256, 1, 4, 1},  {8, 256, 2, 4, 1},  {8, 128, 2, 4, 1},
+    {32, 128, 2, 4, 1}, {32, 64, 2, 4, 1},  {32, 128, 1, 4, 1}, {4, 256, 1, 4, 1},  {16, 64, 1, 4, 1},
+    {16, 64, 2, 4, 0}};
+// the pair-count kernel (scalar loop, the work list of shape 0)
+constexpr PPShapeDesc kCountShape = {kShapes[0].chunk, 64, 2, 4, 0};
 constexpr int kNumShapes = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
 static_assert(kNumShapes <= kMaxPPShapes, "shape table");
 constexpr int min_shape_chunk() {
@@ -778,7 +778,7 @@ void launch_pp_items(const PPArgs &a, cudaStream_t s) {
 // pair-count kernel).
 template <bool COUNT, int S>
 static void launch_force_shape(const PPK &p, int num_sms, cudaStream_t s) {
-  constexpr PPShapeDesc d = kShapes[S];
+  constexpr PPShapeDesc d = COUNT ? kCountShape : kShapes[S];
   constexpr size_t smem = pp_smem_block(d.jtile, d.packed != 0);
   auto fn = k_pp_force<COUNT, d.chunk, d.jtile, d.unroll, d.blocks, d.packed != 0>;
   static int per_sm = 0;
@@ -802,7 +802,7 @@ void launch_pp_force(const PPArgs &a, cudaStream_t s, int t_lo, int t_hi) {
   p.t_lo = t_lo;
   p.t_hi = t_hi;
   if (a.pairs) {
-    launch_force_shape<true, 0>(p, a.num_sms, s);  // the work list was built with shape 0
+    launch_force_shape<true, 0>(p, a.num_sms, s);  // kCountShape: the work list of shape 0
   } else {
     const int shape = a.shape >= 0 && a.shape < kNumShapes ? a.shape : 0;
     launch_force_any(shape, p, a.num_sms, s, std::make_integer_sequence<int, kNumShapes>{});

@@ -66,8 +66,8 @@ def test_pp_shape_table_and_index_check(cube_lib):
     table, cur = K.pp_shapes()
     assert len(table) >= 8 and table[0]["chunk"] == 16 and 0 <= cur < len(table)
     assert all(t["chunk"] in (4, 8, 16, 32) and t["jtile"] % 32 == 0 and t["unroll"] >= 1 for t in table)
-    # both pair-law forms: scalar FP32 (shape 0, the pair count's) and packed f32x2
-    assert table[0]["packed"] == 0 and {t["packed"] for t in table} == {0, 1}
+    # both pair-law forms: packed f32x2 (the default, shape 0) and scalar FP32
+    assert table[0]["packed"] == 1 and {t["packed"] for t in table} == {0, 1}
     for bad in (-2, len(table)):
         with pytest.raises(K.CubeError):
             K.pp_set_shape(bad)
