@@ -116,6 +116,15 @@ __device__ __forceinline__ float F_ra_soft(float r, float ir2, float ce, float k
   return ep > 2.0f ? ir2 : (ep > 1.0f ? fmaf(k, qo, (3.0f / 35.0f) * ir2) : k * qi);
 }
 
+// 1/sqrt(x) on the special-function unit with subnormal inputs flushed (rsqrt.approx.ftz):
+// squared pair distances are either 0 (masked), at least (2^-16 fine cell)^2 or a far sentinel,
+// never subnormal, so only rsqrtf's handling of subnormal inputs is left out
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // packed f32x2 arithmetic (sm_100: one instruction updates both halves, each rounded as the
 // scalar operation)
 __device__ __forceinline__ float2 dup(float v) { return make_float2(v, v); }
@@ -143,7 +152,7 @@ struct PairLaw {
     cep = it.cep;
   }
   __device__ __forceinline__ float scale(float r2) const {
-    const float invr = rsqrtf(r2);
+    const float invr = rsqrt_ftz(r2);
     const float ir2 = invr * invr;
     const float ep = r2 * invr * cep;
     float q = fmaf(7.0f, ep, -48.0f);
@@ -162,7 +171,7 @@ struct PairLaw {
   // scale() of two squared distances on packed f32x2 arithmetic: every operation is the scalar
   // one, rounded the same way, so each half equals scale() of that half bit for bit
   __device__ __forceinline__ float2 scale2(float2 r2) const {
-    const float2 invr = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 invr = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
     const float2 ir2 = mul2(invr, invr);
     const float2 ep = mul2(mul2(r2, invr), dup(cep));
     float2 q = fma2(dup(7.0f), ep, dup(-48.0f));
@@ -181,7 +190,7 @@ struct PairLaw {
   }
   // 0 < r <= app: (F_ra(r, app) - F_ra(r, rc)) / r; cea = 2/app, ka = (1/35)/app^2
   __device__ __forceinline__ float soft(float r2, float cea, float ka) const {
-    const float invr = rsqrtf(r2);
+    const float invr = rsqrt_ftz(r2);
     const float r = r2 * invr, ir2 = invr * invr;
     return (F_ra_soft(r, ir2, cea, ka) - F_ra_soft(r, ir2, cep, k35)) * invr;
   }
