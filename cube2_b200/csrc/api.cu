@@ -78,7 +78,7 @@ struct Ctx {
   cudaStream_t side2 = nullptr;
   cudaEvent_t ev_pm3done = nullptr, ev_join2 = nullptr;
   Buf xp, rhoc, idx, vp, cell_base;
-  Buf tiles, count, cell_start, scan_tmp, spos, pbin, spill, spill_rank, counters, items, range_loc, sched;
+  Buf tiles, count, cell_start, scan_tmp, spos, spill, spill_rank, counters, items, range_loc, sched;
   Buf rho, rhok, force, jobs, out;
   Buf mlp_pos, mlp_rho;  // learned shell: positions of the stored copies, fine-grid CIC density
   // PP kernel shape: fixed (pp_fixed >= 0, cube_pp_set_shape) or autotuned, keyed by
@@ -731,7 +731,6 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   CK(grow(g.cell_start, sizeof(int32_t) * (size_t)(m.ncells + 1)));
   CK(grow(g.scan_tmp, sizeof(int32_t) * scan_tmp_elems(m.ncells)));
   CK(grow(g.spos, sizeof(float4) * (size_t)std::max<int64_t>(d.n_used, 1)));
-  CK(grow(g.pbin, sizeof(uint16_t) * (size_t)std::max<int64_t>(d.n_used, 1)));
   const int spill_cap = 2048;
   CK(grow(g.spill, sizeof(Spill) * spill_cap));
   CK(grow(g.spill_rank, sizeof(int32_t) * spill_cap));
@@ -752,7 +751,6 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   b.count = (int32_t *)g.count.p;
   b.cell_start = (int32_t *)g.cell_start.p;
   b.spos = (float4 *)g.spos.p;
-  b.pbin = (uint16_t *)g.pbin.p;
   b.spill = (Spill *)g.spill.p;
   b.spill_rank = (int32_t *)g.spill_rank.p;
   b.spill_n = ctr + 0;
@@ -1916,7 +1914,7 @@ void c_gpu_velocity_finalize(void) {
   cudaSetDevice(g.device);
   cudaStreamSynchronize(g.stream);
   Buf *bufs[] = {&g.xp, &g.rhoc, &g.idx, &g.vp, &g.cell_base, &g.tiles, &g.count, &g.cell_start, &g.scan_tmp,
-                 &g.spos, &g.pbin, &g.spill, &g.spill_rank, &g.counters, &g.items, &g.range_loc, &g.sched, &g.out};
+                 &g.spos, &g.spill, &g.spill_rank, &g.counters, &g.items, &g.range_loc, &g.sched, &g.out};
   for (Buf *b : bufs) release(*b);
 }
 
@@ -1954,7 +1952,6 @@ int cube_pp_bin_tile(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   CK(grow(g.cell_start, sizeof(int32_t) * (size_t)(m.ncells + 1)));
   CK(grow(g.scan_tmp, sizeof(int32_t) * scan_tmp_elems(m.ncells)));
   CK(grow(g.spos, sizeof(float4) * (size_t)std::max<int64_t>(n_used, 1)));
-  CK(grow(g.pbin, sizeof(uint16_t) * (size_t)std::max<int64_t>(n_used, 1)));
   CK(grow(g.spill, sizeof(Spill) * 2048));
   CK(grow(g.spill_rank, sizeof(int32_t) * 2048));
   int32_t *ctr = (int32_t *)g.counters.p;
@@ -1969,7 +1966,6 @@ int cube_pp_bin_tile(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   b.count = (int32_t *)g.count.p;
   b.cell_start = (int32_t *)g.cell_start.p;
   b.spos = (float4 *)g.spos.p;
-  b.pbin = (uint16_t *)g.pbin.p;
   b.spill = (Spill *)g.spill.p;
   b.spill_rank = (int32_t *)g.spill_rank.p;
   b.spill_n = ctr;

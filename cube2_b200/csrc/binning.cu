@@ -61,7 +61,6 @@ struct BinK {
   int32_t *count;
   const int32_t *cell_start;
   float4 *spos;
-  uint16_t *pbin;  // [n_used] bin of each binned particle from pass 1, kNotHome if not home
   Spill *spill;
   const int32_t *spill_rank;
   int32_t *spill_n;
@@ -97,10 +96,8 @@ __device__ __forceinline__ int morton2(int x, int y, int z) {
   return sp(x) | (sp(y) << 1) | (sp(z) << 2);
 }
 
-constexpr uint16_t kNotHome = 0xffff;  // pbin of a spilled or rejected particle
-
-// Pass 1 (SCATTER = false): per-sub-cell counts, spill collection, and each particle's bin in
-// pbin.  Pass 2 (SCATTER = true): stable placement into spos from the recorded bins.
+// Pass 1 (SCATTER = false): per-sub-cell counts, spill collection.
+// Pass 2 (SCATTER = true): stable placement into spos.
 template <bool SCATTER>
 __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
   extern __shared__ int32_t sh_hist[];
@@ -121,9 +118,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
   const int lx = cx - 1, ly = cy - 1, lz = cz - 1;
   const int nspill = SCATTER ? min(*p.spill_n, p.spill_cap) : 0;
   // spatial order: bins = (PP sub-cell b, Morton index of the 1/8-coarse-cell sub-cell inside b)
-  const bool spatial = p.spatial && (rcp == 2 || rcp == 4);
+  const bool spatial = SCATTER && p.spatial && (rcp == 2 || rcp == 4);
   const int fs = spatial ? 8 / rcp : 1, s3 = fs * fs * fs;
-  const int nbins = SCATTER ? rcp3 * s3 : rcp3;  // pass 1 counts PP sub-cells only
+  const int nbins = rcp3 * s3;
   int32_t *pre = hist + nbins;  // exclusive prefix of the bins (spatial order only)
 
   // key, spill flag and bin of particle l of this coarse cell (pp_force_kernel.c:213-236)
@@ -167,11 +164,18 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
   for (int q = lane; q < nbins; q += 32) hist[q] = 0;
   __syncwarp();
 
-  if (SCATTER && spatial) {
+  if (spatial) {
     // histogram of the bins, then an exclusive prefix per PP sub-cell
-    for (int l = lane; l < np; l += 32) {
-      const int bin = p.pbin[base + l];
-      if (bin != kNotHome) atomicAdd(&hist[bin], 1);
+    for (int l0 = 0; l0 < np; l0 += 32) {
+      const int l = l0 + lane;
+      if (l < np) {
+        float x, y, z;
+        bool spilled, bad;
+        int b, bin;
+        int64_t gkey;
+        classify(l, x, y, z, spilled, bad, b, bin, gkey);
+        if (!spilled && !bad) atomicAdd(&hist[bin], 1);
+      }
     }
     __syncwarp();
     for (int b = 0; b < rcp3; b++) {  // s3 <= 64 bins per PP sub-cell: two per lane
@@ -200,31 +204,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
     float x = 0.f, y = 0.f, z = 0.f;
     const int64_t ip = base + l;
     if (valid) {
-      if (SCATTER) {
-        // the bin recorded by pass 1; the key and position follow from it and the coordinates
-        const int rb = p.pbin[ip];
-        spilled = rb == kNotHome;
-        if (!spilled) {
-          bin = rb;
-          b = spatial ? rb / s3 : rb;
-          const int16_t *q = p.xp + 3 * ip;
-          if (p.fast) {
-            x = decode_pos_f(lx, q[0]);
-            y = decode_pos_f(ly, q[1]);
-            z = decode_pos_f(lz, q[2]);
-          } else {
-            x = __double2float_rn(decode_pos(lx, q[0]));
-            y = __double2float_rn(decode_pos(ly, q[1]));
-            z = __double2float_rn(decode_pos(lz, q[2]));
-          }
-          const int rx = b % rcp, ry = (b / rcp) % rcp, rz = b / (rcp * rcp);
-          gkey = tp.cell0 + ((int64_t)(rcp * cz + rz) * S + (rcp * cy + ry)) * S + (rcp * cx + rx);
-        }
-      } else {
-        classify(l, x, y, z, spilled, bad, b, bin, gkey);
-        if (bad) atomicOr(p.err, 1 << CUBE_ERR_INVALID);
-        p.pbin[ip] = spilled || bad ? kNotHome : (uint16_t)bin;
-      }
+      classify(l, x, y, z, spilled, bad, b, bin, gkey);
+      if (bad) atomicOr(p.err, 1 << CUBE_ERR_INVALID);
     }
     const bool home = valid && !spilled && !bad;
     if (!SCATTER) {
@@ -446,7 +427,6 @@ void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
   p.count = a.count;
   p.cell_start = a.cell_start;
   p.spos = a.spos;
-  p.pbin = a.pbin;
   p.spill = a.spill;
   p.spill_rank = a.spill_rank;
   p.spill_n = a.spill_n;

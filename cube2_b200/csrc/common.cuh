@@ -104,7 +104,6 @@ struct BinArgs {
   int32_t *count;         // [ncells]
   int32_t *cell_start;    // [ncells + 1]
   float4 *spos;           // [n_region] x,y,z (fine units, tile-local), w = ip bits
-  uint16_t *pbin;         // [n_used] scratch: each binned particle's bin, between the passes
   Spill *spill;           // [spill_cap]
   int32_t *spill_rank;    // [spill_cap]
   int32_t *spill_n;       // device counter

@@ -37,8 +37,7 @@ constexpr size_t kOffCount = kOffCellBase + na_align(sizeof(int64_t) * kNaCells)
 constexpr size_t kOffStart = kOffCount + na_align(sizeof(int32_t) * kNaCells);         // int32 [cells + 1]
 constexpr size_t kOffScan = kOffStart + na_align(sizeof(int32_t) * (kNaCells + 1));    // int32 scan scratch
 constexpr size_t kOffSpos = kOffScan + na_align(sizeof(int32_t) * (kNaCells / 4096 + 2));
-constexpr size_t kOffPbin = kOffSpos + na_align(sizeof(float4) * kNaParticles);        // uint16 [particles]
-constexpr size_t kOffItems = kOffPbin + na_align(sizeof(uint16_t) * kNaParticles);     // PPItem work list
+constexpr size_t kOffItems = kOffSpos + na_align(sizeof(float4) * kNaParticles);       // PPItem work list
 constexpr size_t kItemCap = kNaCells + kNaParticles / kPPChunk + 16;
 constexpr size_t kOffSpill = kOffItems + na_align(sizeof(PPItem) * kItemCap);
 constexpr size_t kOffSpillRank = kOffSpill + na_align(sizeof(Spill) * kNaSpill);
@@ -119,7 +118,6 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
   int32_t *cell_start = (int32_t *)(base + kOffStart);
   int32_t *scan_tmp = (int32_t *)(base + kOffScan);
   float4 *spos = (float4 *)(base + kOffSpos);
-  uint16_t *pbin = (uint16_t *)(base + kOffPbin);
   PPItem *items = (PPItem *)(base + kOffItems);
   Spill *spill = (Spill *)(base + kOffSpill);
   int32_t *spill_rank = (int32_t *)(base + kOffSpillRank);
@@ -148,7 +146,6 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
   b.count = count;
   b.cell_start = cell_start;
   b.spos = spos;
-  b.pbin = pbin;
   b.spill = spill;
   b.spill_rank = spill_rank;
   b.spill_n = ctr;
