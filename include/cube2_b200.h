@@ -295,7 +295,7 @@ int cube_mlp_kick(cube_mlp *mlp, const int32_t *d_rhoc, const int64_t *d_idx_b_r
 /* Largest input cube_pp_force_noalloc accepts: stored particles (n_used) and
  * PP cells over all tiles (also the bound on coarse cells over all extended
  * tiles).  The scratch for this size is one static device array of about
- * 17 MB that every GPU loading the library holds until the process exits. */
+ * 22 MB that every GPU loading the library holds until the process exits. */
 #define CUBE_NOALLOC_MAX_PARTICLES 524288
 #define CUBE_NOALLOC_MAX_CELLS 262144
 
