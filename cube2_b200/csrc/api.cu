@@ -757,12 +757,22 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   b.spill_cap = spill_cap;
   b.scan_tmp = (int32_t *)g.scan_tmp.p;
   b.err = ctr + 2;
-  CK(wait_xp(st));
-  if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][2], st));
   if (bin_smem_bytes(m.max_rcp) > 200 * 1024) return fail(CUBE_ERR_INVALID);  // rcp^3 histograms per warp
   b.spatial = 1;
-  launch_pp_binning(b, st);
-  g.launches += 7;  // count, spill sort, 3 scan passes, scatter, spill placement
+  if (g.xp_pending && pp_binning_spill_free(L, m.tiles.data())) {
+    // xp is arriving tile by tile: each tile is binned as soon as its own xp is in
+    if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][2], st));
+    for (int t = 0; t < L.ntile; t++) {
+      CK(wait_xp(st, t));
+      launch_pp_binning_tile(b, m.tiles.data(), t, st);
+      g.launches += 5;  // count, 3 scan passes, scatter
+    }
+  } else {
+    CK(wait_xp(st));
+    if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][2], st));
+    launch_pp_binning(b, st);
+    g.launches += 7;  // count, spill sort, 3 scan passes, scatter, spill placement
+  }
   CU(cudaGetLastError());
   p = PPArgs{};
   p.L = &g.L;

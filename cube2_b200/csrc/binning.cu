@@ -49,6 +49,7 @@ void launch_cell_table(const Lay &L, const int32_t *rhoc, const int64_t *idx_b_r
 
 struct BinK {
   int nt, ncb, nte, rcs, R, ntile;
+  int t_lo, t_n;  // the tiles this launch bins
   int64_t R3;
   int max_rcp3;
   int hist_words;  // shared ints per warp
@@ -103,9 +104,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
   extern __shared__ int32_t sh_hist[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t wid = (int64_t)blockIdx.x * kWarps + warp;
-  if (wid >= (int64_t)p.ntile * p.R3) return;
-  const int t = (int)(wid / p.R3);
-  int64_t rem = wid - (int64_t)t * p.R3;
+  if (wid >= (int64_t)p.t_n * p.R3) return;
+  const int t = p.t_lo + (int)(wid / p.R3);
+  int64_t rem = wid - (int64_t)(t - p.t_lo) * p.R3;
   const int cx = (int)(rem % p.R), cy = (int)((rem / p.R) % p.R), cz = (int)(rem / ((int64_t)p.R * p.R));
   const TilePP tp = p.tiles[t];
   const int rcp = tp.rcp, S = tp.S, rcp3 = rcp * rcp * rcp;
@@ -365,8 +366,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int32_t *in,
   if (threadIdx.x == 0) part[blockIdx.x] = tot;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_top(int32_t *part, int nb) {
-  int carry = 0;
+__global__ void __launch_bounds__(kScanThreads) k_scan_top(int32_t *part, int nb, const int32_t *base) {
+  int carry = base ? *base : 0;
   for (int c0 = 0; c0 < nb; c0 += kScanThreads) {
     int i = c0 + threadIdx.x;
     int v = i < nb ? part[i] : 0;
@@ -398,16 +399,19 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_down(const int32_t *in, i
   if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = part[nb];
 }
 
-void scan_exclusive_i32(const int32_t *in, int64_t n, int32_t *out, int32_t *tmp, cudaStream_t s) {
+void scan_exclusive_i32(const int32_t *in, int64_t n, int32_t *out, int32_t *tmp, cudaStream_t s,
+                        const int32_t *base) {
   const int nb = (int)((n + kScanTile - 1) / kScanTile);
   k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, n, tmp);
-  k_scan_top<<<1, kScanThreads, 0, s>>>(tmp, nb);
+  k_scan_top<<<1, kScanThreads, 0, s>>>(tmp, nb, base);
   k_scan_down<<<nb, kScanThreads, 0, s>>>(in, n, tmp, nb, out);
 }
 
-void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
+static BinK make_bink(const BinArgs &a) {
   const Lay &L = *a.L;
   BinK p;
+  p.t_lo = 0;
+  p.t_n = L.ntile;
   p.nt = L.nt;
   p.ncb = L.ncb;
   p.nte = L.nte;
@@ -432,19 +436,49 @@ void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
   p.spill_n = a.spill_n;
   p.spill_cap = a.spill_cap < kSpillCap ? a.spill_cap : kSpillCap;
   p.err = a.err;
-  const int64_t warps = (int64_t)p.ntile * p.R3;
-  const unsigned blocks = (unsigned)((warps + kWarps - 1) / kWarps);
   const size_t shm = sizeof(int32_t) * kWarps * p.hist_words;
   if (shm > 48 * 1024) {  // fine levels (ratio_sf up to 12 or 16) need more than the default window
     cudaFuncSetAttribute(k_pp_bin<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     cudaFuncSetAttribute(k_pp_bin<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   }
+  return p;
+}
+
+void launch_pp_binning(const BinArgs &a, cudaStream_t s) {
+  BinK p = make_bink(a);
+  const int64_t warps = (int64_t)p.ntile * p.R3;
+  const unsigned blocks = (unsigned)((warps + kWarps - 1) / kWarps);
+  const size_t shm = sizeof(int32_t) * kWarps * p.hist_words;
   cudaMemsetAsync(a.spill_n, 0, sizeof(int32_t), s);
   k_pp_bin<false><<<blocks, kWarps * 32, shm, s>>>(p);
   k_spill_fix<<<1, 1024, 0, s>>>(a.spill, a.spill_rank, a.spill_n, p.spill_cap, a.count);
   scan_exclusive_i32(a.count, a.ncells, a.cell_start, a.scan_tmp, s);
   k_pp_bin<true><<<blocks, kWarps * 32, shm, s>>>(p);
   k_spill_place<<<8, 256, 0, s>>>(p);
+}
+
+bool pp_binning_spill_free(const Lay &L, const TilePP *h_tiles) {
+  if (L.nt + 1 > 127) return false;  // the float decode of a coarse coordinate is exact up to 127
+  for (int t = 0; t < L.ntile; t++)
+    if (h_tiles[t].rcp & (h_tiles[t].rcp - 1)) return false;  // rcp * x exact for powers of two
+  return true;
+}
+
+void launch_pp_binning_tile(const BinArgs &a, const TilePP *h_tiles, int t, cudaStream_t s) {
+  BinK p = make_bink(a);
+  p.t_lo = t;
+  p.t_n = 1;
+  const unsigned blocks = (unsigned)((p.R3 + kWarps - 1) / kWarps);
+  const size_t shm = sizeof(int32_t) * kWarps * p.hist_words;
+  if (t == 0) cudaMemsetAsync(a.spill_n, 0, sizeof(int32_t), s);
+  k_pp_bin<false><<<blocks, kWarps * 32, shm, s>>>(p);
+  const TilePP &tp = h_tiles[t];
+  const int64_t nc = (int64_t)tp.S * tp.S * tp.S;
+  // the tile's cell starts continue from the previous tile's total, which that tile's scan left
+  // at cell_start[cell0]
+  scan_exclusive_i32(a.count + tp.cell0, nc, a.cell_start + tp.cell0, a.scan_tmp, s,
+                     t ? a.cell_start + tp.cell0 : nullptr);
+  k_pp_bin<true><<<blocks, kWarps * 32, shm, s>>>(p);
 }
 
 size_t bin_smem_bytes(int max_rcp) {

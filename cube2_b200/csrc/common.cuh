@@ -113,6 +113,11 @@ struct BinArgs {
   int spatial;            // 1: order inside each PP cell by Morton sub-cell (kick); 0: reference order
 };
 void launch_pp_binning(const BinArgs &a, cudaStream_t s);
+// No particle can spill into the next coarse cell's PP cells (exact float keys); then the
+// binning can run tile by tile, each tile's launches right after its own xp arrives.
+bool pp_binning_spill_free(const Lay &L, const TilePP *h_tiles);
+// count, scan and place the PP region of tile t; tiles must be binned in order on one stream
+void launch_pp_binning_tile(const BinArgs &a, const TilePP *h_tiles, int t, cudaStream_t s);
 size_t bin_smem_bytes(int max_rcp);
 size_t scan_tmp_elems(int64_t n);
 
@@ -192,7 +197,9 @@ void launch_green_fp64(int n, double apm_soft, double apm_range, double gridsize
 
 // exclusive scan of int32 counts (binning.cu): out[0..n] with out[n] = total; tmp has
 // scan_tmp_elems(n) entries
-void scan_exclusive_i32(const int32_t *in, int64_t n, int32_t *out, int32_t *tmp, cudaStream_t s);
+// out[i] = base + sum of in[0..i) for i <= n (base: a device int, or 0 when null)
+void scan_exclusive_i32(const int32_t *in, int64_t n, int32_t *out, int32_t *tmp, cudaStream_t s,
+                        const int32_t *base = nullptr);
 
 // Drift of one image and the rebuild of its buffers (drift.cu)
 struct DriftArgs {
