@@ -195,9 +195,8 @@ void launch_pm3_gather(const PM3Args &a, cudaStream_t s);
 void launch_green_fp64(int n, double apm_soft, double apm_range, double gridsize, int p_order, float *G,
                        cudaStream_t s);
 
-// exclusive scan of int32 counts (binning.cu): out[0..n] with out[n] = total; tmp has
-// scan_tmp_elems(n) entries
-// out[i] = base + sum of in[0..i) for i <= n (base: a device int, or 0 when null)
+// exclusive scan of int32 counts (binning.cu): out[i] = base + sum of in[0..i) for i <= n (base:
+// a device int, or 0 when null), so out[n] = base + total; tmp has scan_tmp_elems(n) entries
 void scan_exclusive_i32(const int32_t *in, int64_t n, int32_t *out, int32_t *tmp, cudaStream_t s,
                         const int32_t *base = nullptr);
 
