@@ -55,8 +55,8 @@ constexpr int kBuckets = 32;
 // default; the last shape is the scalar form, kept for comparison.
 constexpr PPShapeDesc kShapes[] = {
     {16, 128, 2, 4, 1}, {16, 128, 1, 4, 1}, {16, 256, 2, 4, 1}, {16, 128, 4, 4, 1}, {16, 64, 2, 4, 1},
-    {16, 128, 2, 3, 1}, {16, 256, 1, 4, 1}, {8, 256, 1, 4, 1},  {8, 256, 2, 4, 1},  {8, 128, 2, 4, 1},
-    {32, 128, 2, 4, 1}, {32, 64, 2, 4, 1},  {32, 128, 1, 4, 1}, {4, 256, 1, 4, 1},  {16, 64, 1, 4, 1},
+    {16, 128, 2, 3, 1}, {16, 256, 1, 4, 1}, {8, 256, 1, 4, 1},  {8, 256, 2, 4, 1},  {16, 128, 8, 4, 1},
+    {32, 128, 2, 4, 1}, {16, 256, 4, 4, 1}, {16, 96, 4, 4, 1},  {16, 64, 4, 4, 1},  {16, 64, 1, 4, 1},
     {16, 64, 2, 4, 0}};
 // the pair-count kernel (scalar loop, the work list of shape 0)
 constexpr PPShapeDesc kCountShape = {kShapes[0].chunk, 64, 2, 4, 0};

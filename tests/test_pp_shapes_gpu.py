@@ -33,7 +33,7 @@ def test_every_shape_gives_the_default_kick(gpu, clumpy):
     img, tabs = clumpy
     fk = K.FineKick(img.layout, pm3_mode=K.CUBE_PM3_PERIODIC)
     table, _ = K.pp_shapes()
-    assert len(table) >= 8 and {t["chunk"] for t in table} >= {4, 8, 16}
+    assert len(table) >= 8 and {t["chunk"] for t in table} >= {8, 16, 32}
     try:
         K.pp_set_shape(0)
         want, f2_want, vmax_want, _, _ = fk.c_pp_force_kernel(img, *tabs, 1.0, SIXPI, 1.0)
