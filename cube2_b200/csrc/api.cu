@@ -1385,7 +1385,8 @@ static int drift_device(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const i
   if (L.nt < L.ncb) return fail(CUBE_ERR_INVALID);  // a buffer mirrors at most one tile deep
   int nlayer = 0;
   CK(drift_nlayer(dt_mid, vz_max, L.rcs, &nlayer));
-  const int64_t run_cap = std::max<int64_t>(n_used, 1);
+  const int64_t run_cap = std::max<int64_t>(n_used, 1) + drift_run_slack(g.num_sms);
+  if (run_cap >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
   CK(grow(g.dr_cb, sizeof(int64_t) * ncs));
   CK(grow(g.dr_cb_new, sizeof(int64_t) * ncs));
   CK(grow(g.dr_runrank, sizeof(uint32_t) * run_cap));

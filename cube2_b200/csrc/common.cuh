@@ -231,6 +231,8 @@ struct DriftArgs {
   int64_t *pid_new;
 };
 size_t drift_run_bytes();
+// run-table slots beyond one per stored copy: the per-warp chunks' unused ends
+int64_t drift_run_slack(int num_sms);
 void launch_drift_runs(const DriftArgs &a, cudaStream_t s);
 // new counts of every extended cell, row sums and the spine; *total = stored copies
 void launch_drift_spine(const DriftArgs &a, int32_t *rhoc_new, int64_t *rows, int64_t *idx_b_r_new,

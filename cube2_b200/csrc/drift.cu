@@ -38,6 +38,11 @@ constexpr int kDriftMaxRuns = 64;    // destination cells of one source cell
 constexpr int kRankBits = 26;        // run slot word: entry << 26 | rank inside the run
 constexpr uint32_t kDropped = 0xffffffffu;
 constexpr int kDriftWarps = 8;
+// Run-table slots are reserved per warp kRunChunk at a time (one atomic per chunk instead of
+// one per source cell on a single counter); the unused end of a chunk holds dest = -1.
+constexpr int kRunChunk = 64;
+static_assert(kRunChunk >= kDriftMaxRuns, "a cell's runs fit one chunk");
+constexpr int kDriftGridPerSM = 16;  // blocks per SM of the warp-per-cell kernels (at most)
 
 struct DriftK {
   int nt, ncb, nte, nnt, nc, nlayer, tile_periodic;
@@ -109,6 +114,12 @@ __global__ void __launch_bounds__(kDriftWarps * 32) k_drift_runs(DriftK p) {
   // the count and first slot of the next cell are loaded one cell ahead
   int n_next = S < p.ncells_src ? p.rhoc[S] : 0;
   int64_t base_next = S < p.ncells_src ? p.cell_base[S] : 0;
+  int cur = 0, end = 0;  // this warp's reserved run slots [cur, end)
+  int kept_w = 0;        // kept copies counted by this lane
+  auto close_chunk = [&]() {
+    for (int e = cur + lane; e < end; e += 32)
+      if (e < p.run_cap) p.runs[e].dest = -1;
+  };
   for (; S < p.ncells_src; S += stride) {
     const int n = n_next;
     const int64_t base = base_next;
@@ -167,9 +178,15 @@ __global__ void __launch_bounds__(kDriftWarps * 32) k_drift_runs(DriftK p) {
     }
     }
     if (nent) {
-      int rb = 0;
-      if (lane == 0) rb = atomicAdd(&p.ctr[0], nent);
-      rb = __shfl_sync(0xffffffffu, rb, 0);
+      if (cur + nent > end) {  // a new chunk of run slots
+        close_chunk();
+        int c = 0;
+        if (lane == 0) c = atomicAdd(&p.ctr[0], kRunChunk);
+        cur = __shfl_sync(0xffffffffu, c, 0);
+        end = cur + kRunChunk;
+      }
+      const int rb = cur;
+      cur += nent;
       if (lane == 0) p.run_base[S] = rb;
       const uint64_t key = ((uint64_t)(cz % p.nlayer) << 32) | (uint64_t)S;
       int kept = 0;
@@ -187,11 +204,13 @@ __global__ void __launch_bounds__(kDriftWarps * 32) k_drift_runs(DriftK p) {
           atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
         }
       }
-      kept = __reduce_add_sync(0xffffffffu, kept);
-      if (lane == 0) atomicAdd(&p.ctr[1], kept);
+      kept_w += kept;
       __syncwarp();  // the table is reused by the next cell
     }
   }
+  close_chunk();
+  kept_w = __reduce_add_sync(0xffffffffu, kept_w);
+  if (lane == 0 && kept_w) atomicAdd(&p.ctr[1], kept_w);
 }
 
 // physical cell mirrored by extended cell (t, cx, cy, cz): the image's periodic neighbour
@@ -274,6 +293,7 @@ __global__ void k_runs_fill(DriftK p, int32_t nruns) {
   const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nruns) return;
   const int32_t D = p.runs[r].dest;
+  if (D < 0) return;  // an unused slot at the end of a warp's chunk
   const int32_t slot = atomicAdd(&p.cursor[D], 1);
   p.run_list[p.dest_start[D] + slot] = r;
 }
@@ -422,10 +442,11 @@ static DriftK make_driftk(const DriftArgs &a) {
 }
 
 size_t drift_run_bytes() { return sizeof(DriftRun); }
+int64_t drift_run_slack(int num_sms) { return (int64_t)num_sms * kDriftGridPerSM * kDriftWarps * kRunChunk; }
 
 static unsigned warp_grid(int64_t items, int num_sms) {
   const int64_t blocks = (items + kDriftWarps - 1) / kDriftWarps;
-  const int64_t cap = (int64_t)num_sms * 16;
+  const int64_t cap = (int64_t)num_sms * kDriftGridPerSM;
   return (unsigned)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
 }
 
