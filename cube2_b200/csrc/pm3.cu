@@ -313,13 +313,22 @@ __global__ void __launch_bounds__(kWarps * 32, 4) k_gather(PM3K p) {
     }
   }
   if (p.want_vmax) {
+    // one update of each maximum per block: a warp per coarse cell would put hundreds of
+    // thousands of atomics on the same three words
+    __shared__ float vmb[3][kWarps];
     vm0 = warp_max(vm0);
     vm1 = warp_max(vm1);
     vm2 = warp_max(vm2);
     if (lane == 0) {
-      atomic_max_nonneg(&p.out[2], vm0);
-      atomic_max_nonneg(&p.out[3], vm1);
-      atomic_max_nonneg(&p.out[4], vm2);
+      vmb[0][warp] = vm0;
+      vmb[1][warp] = vm1;
+      vmb[2][warp] = vm2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      float m = 0.f;
+      for (int w = 0; w < kWarps; w++) m = fmaxf(m, vmb[threadIdx.x][w]);
+      atomic_max_nonneg(&p.out[2 + threadIdx.x], m);
     }
   }
 }
