@@ -229,8 +229,15 @@ __global__ void __launch_bounds__(kFzRows * 32) k_force_zm(PM3K p) {
     c0 = cp1;
     cp1 = cp2;
   }
+  // one update of f2max per block
+  __shared__ float mb[kFzRows];
   m = warp_max(m);
-  if (lane == 0) atomic_max_nonneg(&p.out[0], m);
+  if (lane == 0) mb[wy] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kFzRows; w++) m = fmaxf(m, mb[w]);
+    atomic_max_nonneg(&p.out[0], m);
+  }
 }
 
 // the same, one point per thread, for any n
