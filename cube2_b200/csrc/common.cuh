@@ -127,7 +127,8 @@ size_t scan_tmp_elems(int64_t n);
 struct __align__(16) PPItem {
   uint32_t cell;  // global PP cell index
   int32_t i0;     // first particle of the chunk in the cell-sorted order
-  int32_t dims;   // ni | rcp << 8 | R << 16: particles, PP cells per coarse cell, stencil radius
+  int32_t dims;   // ni | rcp << 8 | R << 16 | span << 24: particles, PP cells per coarse cell,
+                  // stencil radius, 1 when the item holds two cells along x (x and x + 1)
   float rc;       // PP range of the cell
   float cep, k35, h, rc2;  // 2 / rc, 1 / (35 rc^2), ratio_cs / rcp, rc^2
 };

@@ -325,6 +325,22 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
     g = tp.cell0 + ((int64_t)z * S + y) * S + x;
     i0 = p.cs[g];
     ni = p.cs[g + 1] - i0;
+    // Two occupied neighbouring cells along x (interior x even and x + 1) whose particles fit
+    // one chunk and share the PP range form one item: its stencil rows are one cell longer,
+    // which walks fewer candidates than two items and halves the per-item work.  The odd
+    // cell of such a pair makes no item.
+    int span = 0;
+    const int lxi = x - rcp;
+    if (ni > 0 && (lxi & 1)) {
+      const int n0 = i0 - p.cs[g - 1];
+      if (n0 > 0 && n0 + ni <= C && cell_range(p, t, x - 1, y, z, rcp) == cell_range(p, t, x, y, z, rcp)) ni = 0;
+    } else if (ni > 0 && lxi + 1 < npg) {
+      const int n2 = p.cs[g + 2] - p.cs[g + 1];
+      if (n2 > 0 && ni + n2 <= C && cell_range(p, t, x + 1, y, z, rcp) == cell_range(p, t, x, y, z, rcp)) {
+        ni += n2;
+        span = 1;
+      }
+    }
     if (ni > 0) {
       const float rc = cell_range(p, t, x, y, z, rcp);
       const int R = stencil_radius(rc, rcp, p.rcs);
@@ -332,7 +348,7 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
       const float h = (float)p.rcs / (float)rcp;
       const int Rc = min(R, rcp);
       it.cell = (uint32_t)g;
-      it.dims = (rcp << 8) | (Rc << 16);
+      it.dims = (rcp << 8) | (Rc << 16) | (span << 24);
       it.rc = rc;
       it.cep = PairLaw::cep_of(rc);
       it.k35 = PairLaw::k35_of(rc);
@@ -343,7 +359,7 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
         for (int dy = -Rc; dy <= Rc; dy++) {
           if (!row_needed(dy, dz, h, rc * rc)) continue;
           const int64_t b = g + ((int64_t)dz * S + dy) * S;
-          nj += p.cs[b + Rc + 1] - p.cs[b - Rc];
+          nj += p.cs[b + Rc + 1 + span] - p.cs[b - Rc];
         }
       nfull = ni / C;
       bfull = cost_bucket(C, nj);
@@ -451,7 +467,7 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
     }
     const PPItem &item = batch[b];  // read from shared memory where used
     const int64_t g = (int64_t)item.cell;
-    const int ni = item.dims & 0xff, R = item.dims >> 16;
+    const int ni = item.dims & 0xff, R = (item.dims >> 16) & 0xff, span = item.dims >> 24;
     const int S = ((item.dims >> 8) & 0xff) * (p.nt + 2);
     const float rc2 = item.rc2;
     PairLaw law;
@@ -600,7 +616,7 @@ __global__ void __launch_bounds__(kPPThreads, B) k_pp_force(PPK p) {
           if (need) {
             const int64_t b = g + ((int64_t)dz * S + dy) * S;
             js = p.cs[b - R];
-            len = p.cs[b + R + 1] - js;
+            len = p.cs[b + R + 1 + span] - js;
           }
         }
         const unsigned m = __ballot_sync(0xffffffffu, need);
