@@ -325,20 +325,49 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
     g = tp.cell0 + ((int64_t)z * S + y) * S + x;
     i0 = p.cs[g];
     ni = p.cs[g + 1] - i0;
-    // Two occupied neighbouring cells along x (interior x even and x + 1) whose particles fit
-    // one chunk and share the PP range form one item: its stencil rows are one cell longer,
-    // which walks fewer candidates than two items and halves the per-item work.  The odd
-    // cell of such a pair makes no item.
+    // Sparse neighbouring cells along x share an item when their particles fit one chunk and
+    // they share the PP range: an aligned group of four cells (at least three occupied), else
+    // an aligned pair (both occupied).  The item's stencil rows are `span` cells longer, which
+    // walks fewer candidates than separate items and saves their per-item work; the other
+    // cells of the group make no item.  Every cell of a group decides the same way.
     int span = 0;
     const int lxi = x - rcp;
-    if (ni > 0 && (lxi & 1)) {
-      const int n0 = i0 - p.cs[g - 1];
-      if (n0 > 0 && n0 + ni <= C && cell_range(p, t, x - 1, y, z, rcp) == cell_range(p, t, x, y, z, rcp)) ni = 0;
-    } else if (ni > 0 && lxi + 1 < npg) {
-      const int n2 = p.cs[g + 2] - p.cs[g + 1];
-      if (n2 > 0 && ni + n2 <= C && cell_range(p, t, x + 1, y, z, rcp) == cell_range(p, t, x, y, z, rcp)) {
-        ni += n2;
-        span = 1;
+    {
+      auto count_at = [&](int lx) {
+        const int64_t gg = g + (lx - lxi);
+        return p.cs[gg + 1] - p.cs[gg];
+      };
+      auto same_range = [&](int lx0, int n) {
+        const float r0 = cell_range(p, t, lx0 + rcp, y, z, rcp);
+        for (int k = 1; k < n; k++)
+          if (cell_range(p, t, lx0 + k + rcp, y, z, rcp) != r0) return false;
+        return true;
+      };
+      const int h4 = lxi & ~3, h2 = lxi & ~1;
+      int tot4 = 0, occ4 = 0;
+      if (h4 + 3 < npg)
+        for (int k = 0; k < 4; k++) {
+          const int cnt = count_at(h4 + k);
+          tot4 += cnt;
+          occ4 += cnt > 0 ? 1 : 0;
+        }
+      if (h4 + 3 < npg && tot4 <= C && occ4 >= 3 && same_range(h4, 4)) {
+        if (lxi == h4) {
+          ni = tot4;
+          span = 3;
+        } else {
+          ni = 0;
+        }
+      } else if (h2 + 1 < npg) {
+        const int n0 = count_at(h2), n1 = count_at(h2 + 1);
+        if (n0 > 0 && n1 > 0 && n0 + n1 <= C && same_range(h2, 2)) {
+          if (lxi == h2) {
+            ni = n0 + n1;
+            span = 1;
+          } else {
+            ni = 0;
+          }
+        }
       }
     }
     if (ni > 0) {
