@@ -39,10 +39,10 @@ METRIC = "particle kicks/s (PM3+PP) on 1 B200, learned vs plain at equal rms for
 UNIT = "particle-kicks/s"
 PP_FLOP_PER_PAIR = 38  # 3 sub, 5 r^2, rsqrt, 1/r^2, 2 ep, 18 polynomial+reciprocal, 1 diff, 1 scale, 6 accumulate
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_pp_force launch per stored
-# particle, from an ncu capture on clustered192 (251.1 MB + 65.1 MB over 9,025,370 stored
+# particle, from an ncu capture on clustered192 (242.6 MB + 65.1 MB over 9,025,370 stored
 # particles); the kernel streams the sorted particles and vp once per launch, so the figure is
 # scaled to a full launch by the stored particle count
-PP_DRAM_BYTES_PER_STORED = (251_149_312 + 65_095_424) / 9_025_370
+PP_DRAM_BYTES_PER_STORED = (242_559_488 + 65_138_432) / 9_025_370
 
 
 def parse():
