@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
     i0 = p.cs[g];
     ni = p.cs[g + 1] - i0;
     // Sparse neighbouring cells along x share an item when their particles fit one chunk and
-    // they share the PP range: an aligned group of four cells (at least three occupied), else
+    // they lie in one subtile: an aligned group of four cells (at least three occupied), else
     // an aligned pair (both occupied).  The item's stencil rows are `span` cells longer, which
     // walks fewer candidates than separate items and saves their per-item work; the other
     // cells of the group make no item.  Every cell of a group decides the same way.
@@ -337,12 +337,9 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
         const int64_t gg = g + (lx - lxi);
         return p.cs[gg + 1] - p.cs[gg];
       };
-      auto same_range = [&](int lx0, int n) {
-        const float r0 = cell_range(p, t, lx0 + rcp, y, z, rcp);
-        for (int k = 1; k < n; k++)
-          if (cell_range(p, t, lx0 + k + rcp, y, z, rcp) != r0) return false;
-        return true;
-      };
+      // the PP range is set per subtile: a group inside one subtile shares it (groups across a
+      // subtile boundary are not formed)
+      auto same_range = [&](int lx0, int n) { return lx0 / (rcp * p.ntt) == (lx0 + n - 1) / (rcp * p.ntt); };
       const int h4 = lxi & ~3, h2 = lxi & ~1;
       int tot4 = 0, occ4 = 0;
       if (h4 + 3 < npg)
