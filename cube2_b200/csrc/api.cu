@@ -61,8 +61,12 @@ struct Ctx {
   // The PP binning and work list run on `side`, beside PM3 on the compute stream.
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // Host kicks pipeline groups of consecutive tiles (one tile per group up to kMaxTileEvents
+  // tiles): group k holds tiles [grp_lo[k], grp_lo[k + 1])
   static constexpr int kMaxTileEvents = 64;
-  cudaEvent_t ev_tile[kMaxTileEvents] = {};  // per-tile PP force done (host kicks)
+  int ngrp = 0;
+  int grp_lo[kMaxTileEvents + 1] = {};
+  cudaEvent_t ev_tile[kMaxTileEvents] = {};  // per-group PP force done (host kicks)
   cudaEvent_t ev_copied = nullptr;           // last per-tile vp copy enqueued
   bool vp_copied = false;                    // this host kick's vp is already on its way back
   // Host kicks upload xp tile by tile on `copy`; the deposit of a tile waits only for its
@@ -507,15 +511,15 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     CK(get_plan(n, nslots, CUFFT_R2C, &fw));
     CK(get_plan(n, nslots, CUFFT_C2R, &bw));
     CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3 * nslots, g.stream));
-    if (g.xp_pending) {  // deposit each tile as soon as its particles are on the device
+    if (g.xp_pending) {  // deposit each group of tiles as soon as its particles are on the device
       PM3Args at = a;
-      at.njobs = 1;
-      for (int t = 0; t < L.ntile; t++) {
-        CK(wait_xp(g.stream, t));
-        at.jobs = (const MeshJob *)g.jobs.p + t;
+      for (int k = 0; k < g.ngrp; k++) {
+        CK(wait_xp(g.stream, k));
+        at.jobs = (const MeshJob *)g.jobs.p + g.grp_lo[k];
+        at.njobs = g.grp_lo[k + 1] - g.grp_lo[k];
         launch_pm3_deposit(at, g.stream);
       }
-      g.launches += L.ntile - 1;
+      g.launches += g.ngrp - 1;
     } else {
       launch_pm3_deposit(a, g.stream);
     }
@@ -523,18 +527,18 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     launch_pm3_kspace(a, g.stream);
     CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)g.rho.p));  // potential
     launch_pm3_force(a, g.stream);
-    if (g.vp_pending && g.vp_tiles == L.ntile) {  // gather each tile as soon as its vp is on the device
+    if (g.vp_pending && g.vp_tiles == g.ngrp && g.ngrp > 0) {  // gather each group once its vp is in
       PM3Args at = a;
-      at.njobs = 1;
-      for (int t = 0; t < L.ntile; t++) {
-        CU(cudaStreamWaitEvent(g.stream, g.ev_vp[t], 0));
-        at.jobs = (const MeshJob *)g.jobs.p + t;
+      for (int k = 0; k < g.ngrp; k++) {
+        CU(cudaStreamWaitEvent(g.stream, g.ev_vp[k], 0));
+        at.jobs = (const MeshJob *)g.jobs.p + g.grp_lo[k];
+        at.njobs = g.grp_lo[k + 1] - g.grp_lo[k];
         launch_pm3_gather(at, g.stream);
-        CU(cudaEventRecord(g.ev_ready[t], g.stream));
+        CU(cudaEventRecord(g.ev_ready[k], g.stream));
       }
       g.vp_pending = false;
       g.ready_tiles = true;
-      g.launches += L.ntile - 1;
+      g.launches += g.ngrp - 1;
     } else {
       CK(wait_vp());
       launch_pm3_gather(a, g.stream);
@@ -760,11 +764,11 @@ static int run_pp_prep(const Meta &m, const Dev &d, float mass, float kick, size
   if (bin_smem_bytes(m.max_rcp) > 200 * 1024) return fail(CUBE_ERR_INVALID);  // rcp^3 histograms per warp
   b.spatial = 1;
   if (g.xp_pending && pp_binning_spill_free(L, m.tiles.data())) {
-    // xp is arriving tile by tile: each tile is binned as soon as its own xp is in
+    // xp is arriving group by group: each group of tiles is binned as soon as its xp is in
     if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][2], st));
-    for (int t = 0; t < L.ntile; t++) {
-      CK(wait_xp(st, t));
-      launch_pp_binning_tile(b, m.tiles.data(), t, st);
+    for (int k = 0; k < g.ngrp; k++) {
+      CK(wait_xp(st, k));
+      launch_pp_binning_tiles(b, m.tiles.data(), g.grp_lo[k], g.grp_lo[k + 1], st);
       g.launches += 5;  // count, 3 scan passes, scatter
     }
   } else {
@@ -813,11 +817,11 @@ static int run_pp_force(const PPArgs &p) {
   return CUBE_OK;
 }
 
-// PP force kernel tile by tile for a host kick.  The launches alternate between the side
-// streams (one launch's tail overlaps the next one's start); a tile's launch waits for the
-// binning and for that tile's PM3 gather, and its vp range (its stored particles, a contiguous
-// run of the spine) goes to the host on the copy stream as soon as the launch is done.  The
-// compute stream ends after the last copy.
+// PP force kernel group by group (consecutive tiles) for a host kick.  The launches alternate
+// between the side streams (one launch's tail overlaps the next one's start); a group's launch
+// waits for the binning and for that group's PM3 gather, and its vp range (its stored
+// particles, a contiguous run of the spine) goes to the host on the copy stream as soon as the
+// launch is done.  The compute stream ends after the last copy.
 static int run_pp_force_tiles(const PPArgs &p, const Dev &d) {
   const Lay &L = g.L;
   if (!g.ready_tiles) {  // PM3 gathered all tiles at once
@@ -827,19 +831,20 @@ static int run_pp_force_tiles(const PPArgs &p, const Dev &d) {
   CU(cudaStreamWaitEvent(g.side2, g.ev_join, 0));  // binning (on side) done
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][3], g.side));
   const int64_t rows = (int64_t)L.nte * L.nte;
-  for (int t = 0; t < L.ntile; t++) {
-    cudaStream_t st = (t & 1) ? g.side2 : g.side;
-    CU(cudaStreamWaitEvent(st, g.ready_tiles ? g.ev_ready[t] : g.ev_pm3done, 0));
-    launch_pp_force(p, st, t, t + 1);
+  for (int k = 0; k < g.ngrp; k++) {
+    cudaStream_t st = (k & 1) ? g.side2 : g.side;
+    CU(cudaStreamWaitEvent(st, g.ready_tiles ? g.ev_ready[k] : g.ev_pm3done, 0));
+    launch_pp_force(p, st, g.grp_lo[k], g.grp_lo[k + 1]);
     g.launches += 1;
     CU(cudaGetLastError());
-    CU(cudaEventRecord(g.ev_tile[t], st));
+    CU(cudaEventRecord(g.ev_tile[k], st));
   }
   // copies after all launches: a copy into pageable host memory returns only when done
-  for (int t = 0; t < L.ntile; t++) {
-    const int64_t lo = t ? d.h_idx[t * rows - 1] : 0, hi = d.h_idx[(t + 1) * rows - 1];
+  for (int k = 0; k < g.ngrp; k++) {
+    const int t0 = g.grp_lo[k], t1 = g.grp_lo[k + 1];
+    const int64_t lo = t0 ? d.h_idx[t0 * rows - 1] : 0, hi = d.h_idx[t1 * rows - 1];
     if (hi <= lo) continue;
-    CU(cudaStreamWaitEvent(g.copy, g.ev_tile[t], 0));
+    CU(cudaStreamWaitEvent(g.copy, g.ev_tile[k], 0));
     CU(cudaMemcpyAsync(d.h_vp + 3 * lo, d.vp + 3 * lo, sizeof(float) * 3 * (hi - lo), cudaMemcpyDeviceToHost,
                        g.copy));
   }
@@ -900,7 +905,7 @@ static int run_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *ra
     g.ready_tiles = false;
     CK(run_pm3(m, ires, ratio_sf, gk, d, mass, kick, false, soff));
     if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][1], g.stream));
-    if (d.h_vp && g.L.ntile <= Ctx::kMaxTileEvents) {
+    if (d.h_vp && g.ngrp > 0) {
       CK(run_pp_force_tiles(pa, d));
     } else {
       CU(cudaStreamWaitEvent(g.stream, g.ev_join, 0));
@@ -976,41 +981,36 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   CK(grow(g.idx, sizeof(int64_t) * (size_t)nrows));
   CU(cudaMemcpyAsync(g.rhoc.p, rhoc, sizeof(int32_t) * nrows * L.nte, cudaMemcpyHostToDevice, g.stream));
   CU(cudaMemcpyAsync(g.idx.p, idx_b_r, sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, g.stream));
+  g.ngrp = 0;
   if (n_used) {
     // xp tile by tile, so that the deposit of the first tiles overlaps the copy of the rest
     // (the copy stream first waits for the compute stream's earlier work on these buffers)
     CU(cudaEventRecord(g.ev_fork, g.stream));
     CU(cudaStreamWaitEvent(g.copy, g.ev_fork, 0));
     const int64_t rows = (int64_t)L.nte * L.nte;
-    const bool tiled = L.ntile <= Ctx::kMaxTileEvents;
-    for (int t = 0; tiled && t < L.ntile; t++) {
-      const int64_t lo = t ? idx_b_r[t * rows - 1] : 0, hi = idx_b_r[(t + 1) * rows - 1];
+    // groups of consecutive tiles, at most kMaxTileEvents of them
+    g.ngrp = std::min(L.ntile, Ctx::kMaxTileEvents);
+    for (int k = 0; k <= g.ngrp; k++) g.grp_lo[k] = (int)((int64_t)k * L.ntile / g.ngrp);
+    for (int k = 0; k < g.ngrp; k++) {
+      const int t0 = g.grp_lo[k], t1 = g.grp_lo[k + 1];
+      const int64_t lo = t0 ? idx_b_r[t0 * rows - 1] : 0, hi = idx_b_r[t1 * rows - 1];
       if (hi > lo)
         CU(cudaMemcpyAsync((int16_t *)g.xp.p + 3 * lo, xp + 3 * lo, sizeof(int16_t) * 3 * (hi - lo),
                            cudaMemcpyHostToDevice, g.copy));
-      CU(cudaEventRecord(g.ev_xp[t], g.copy));
+      CU(cudaEventRecord(g.ev_xp[k], g.copy));
     }
-    if (tiled) {
-      g.xp_pending = true;
-      g.xp_tiles = L.ntile;
-    } else {
-      CU(cudaMemcpyAsync(g.xp.p, xp, sizeof(int16_t) * 3 * n_used, cudaMemcpyHostToDevice, g.stream));
+    g.xp_pending = true;
+    g.xp_tiles = g.ngrp;
+    // vp travels beside the deposit and FFTs, group by group; its users wait for their part
+    for (int k = 0; k < g.ngrp; k++) {
+      const int t0 = g.grp_lo[k], t1 = g.grp_lo[k + 1];
+      const int64_t lo = t0 ? idx_b_r[t0 * rows - 1] : 0, hi = idx_b_r[t1 * rows - 1];
+      if (hi > lo)
+        CU(cudaMemcpyAsync((float *)g.vp.p + 3 * lo, vp + 3 * lo, sizeof(float) * 3 * (hi - lo),
+                           cudaMemcpyHostToDevice, g.copy));
+      CU(cudaEventRecord(g.ev_vp[k], g.copy));
     }
-    // vp travels beside the deposit and FFTs, tile by tile; its users wait for their part
-    g.vp_tiles = 0;
-    if (tiled) {
-      for (int t = 0; t < L.ntile; t++) {
-        const int64_t lo = t ? idx_b_r[t * rows - 1] : 0, hi = idx_b_r[(t + 1) * rows - 1];
-        if (hi > lo)
-          CU(cudaMemcpyAsync((float *)g.vp.p + 3 * lo, vp + 3 * lo, sizeof(float) * 3 * (hi - lo),
-                             cudaMemcpyHostToDevice, g.copy));
-        CU(cudaEventRecord(g.ev_vp[t], g.copy));
-      }
-      g.vp_tiles = L.ntile;
-    } else {
-      CU(cudaMemcpyAsync(g.vp.p, vp, sizeof(float) * 3 * n_used, cudaMemcpyHostToDevice, g.copy));
-      CU(cudaEventRecord(g.vp_ready, g.copy));
-    }
+    g.vp_tiles = g.ngrp;
     g.vp_pending = true;
   }
   Dev d{(const int16_t *)g.xp.p, (const int32_t *)g.rhoc.p, (const int64_t *)g.idx.p, (float *)g.vp.p, n_used};

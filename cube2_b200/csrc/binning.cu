@@ -464,20 +464,21 @@ bool pp_binning_spill_free(const Lay &L, const TilePP *h_tiles) {
   return true;
 }
 
-void launch_pp_binning_tile(const BinArgs &a, const TilePP *h_tiles, int t, cudaStream_t s) {
+void launch_pp_binning_tiles(const BinArgs &a, const TilePP *h_tiles, int t_lo, int t_hi, cudaStream_t s) {
   BinK p = make_bink(a);
-  p.t_lo = t;
-  p.t_n = 1;
-  const unsigned blocks = (unsigned)((p.R3 + kWarps - 1) / kWarps);
+  p.t_lo = t_lo;
+  p.t_n = t_hi - t_lo;
+  const int64_t warps = (int64_t)p.t_n * p.R3;
+  const unsigned blocks = (unsigned)((warps + kWarps - 1) / kWarps);
   const size_t shm = sizeof(int32_t) * kWarps * p.hist_words;
-  if (t == 0) cudaMemsetAsync(a.spill_n, 0, sizeof(int32_t), s);
+  if (t_lo == 0) cudaMemsetAsync(a.spill_n, 0, sizeof(int32_t), s);
   k_pp_bin<false><<<blocks, kWarps * 32, shm, s>>>(p);
-  const TilePP &tp = h_tiles[t];
-  const int64_t nc = (int64_t)tp.S * tp.S * tp.S;
-  // the tile's cell starts continue from the previous tile's total, which that tile's scan left
-  // at cell_start[cell0]
-  scan_exclusive_i32(a.count + tp.cell0, nc, a.cell_start + tp.cell0, a.scan_tmp, s,
-                     t ? a.cell_start + tp.cell0 : nullptr);
+  // the tiles' PP cells are consecutive; their cell starts continue from the previous tiles'
+  // total, which those tiles' scan left at cell_start[cell0]
+  const int64_t c0 = h_tiles[t_lo].cell0;
+  const TilePP &tl = h_tiles[t_hi - 1];
+  const int64_t nc = tl.cell0 + (int64_t)tl.S * tl.S * tl.S - c0;
+  scan_exclusive_i32(a.count + c0, nc, a.cell_start + c0, a.scan_tmp, s, t_lo ? a.cell_start + c0 : nullptr);
   k_pp_bin<true><<<blocks, kWarps * 32, shm, s>>>(p);
 }
 

@@ -116,8 +116,9 @@ void launch_pp_binning(const BinArgs &a, cudaStream_t s);
 // No particle can spill into the next coarse cell's PP cells (exact float keys); then the
 // binning can run tile by tile, each tile's launches right after its own xp arrives.
 bool pp_binning_spill_free(const Lay &L, const TilePP *h_tiles);
-// count, scan and place the PP region of tile t; tiles must be binned in order on one stream
-void launch_pp_binning_tile(const BinArgs &a, const TilePP *h_tiles, int t, cudaStream_t s);
+// count, scan and place the PP regions of tiles [t_lo, t_hi); the tiles must be binned in order
+// on one stream
+void launch_pp_binning_tiles(const BinArgs &a, const TilePP *h_tiles, int t_lo, int t_hi, cudaStream_t s);
 size_t bin_smem_bytes(int max_rcp);
 size_t scan_tmp_elems(int64_t n);
 
@@ -160,8 +161,9 @@ PPShapeDesc pp_shape_desc(int i);
 int pp_min_chunk();  // smallest chunk of any shape: the work list capacity is sized for it
 // work list for the shape a.shape (shape 0 with a.pairs)
 void launch_pp_items(const PPArgs &a, cudaStream_t s);
-// force kernel over the items of tiles [t_lo, t_hi) (t_hi < 0: all tiles); each single tile and
-// the full range have their own queue head, so per-tile launches may run on several streams
+// force kernel over the items of tiles [t_lo, t_hi) (t_hi < 0: all tiles); disjoint tile ranges
+// and the full range have their own queue heads, so launches over disjoint ranges may run on
+// several streams
 void launch_pp_force(const PPArgs &a, cudaStream_t s, int t_lo = 0, int t_hi = -1);
 
 // PM3

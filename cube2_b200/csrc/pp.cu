@@ -286,10 +286,11 @@ __device__ __forceinline__ bool row_needed(int dy, int dz, float h, float rc2) {
 // Schedule words (int32), for ntile tiles: [0, 32 ntile) item counts per (tile, bucket), turned
 // into the first item slot of each (tile, bucket) by k_pp_offsets; [32 ntile, 64 ntile) cursors;
 // then ntile + 1 tile bases (first item of each tile, and the total); then ntile + 1 queue
-// heads (one per single-tile launch, one for a launch over all tiles).
+// heads: a launch over tiles [t_lo, t_hi) uses head t_lo, one over all tiles head ntile, so
+// launches over disjoint tile ranges never share a head.
 __host__ __device__ inline int64_t sched_base(int ntile) { return 2 * (int64_t)kBuckets * ntile; }
 __host__ __device__ inline int64_t sched_head(int ntile, int t_lo, int t_hi) {
-  return sched_base(ntile) + ntile + 1 + (t_hi - t_lo == 1 ? t_lo : ntile);
+  return sched_base(ntile) + ntile + 1 + (t_hi - t_lo == ntile ? ntile : t_lo);
 }
 
 // cost bucket of a chunk with ni i-particles and nj candidates, heavy = high index:
