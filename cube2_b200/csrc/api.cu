@@ -61,9 +61,12 @@ struct Ctx {
   // The PP binning and work list run on `side`, beside PM3 on the compute stream.
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  // Host kicks pipeline groups of consecutive tiles (one tile per group up to kMaxTileEvents
-  // tiles): group k holds tiles [grp_lo[k], grp_lo[k + 1])
+  // Host kicks pipeline groups of consecutive tiles (one tile per group up to kPipeGroups
+  // tiles; more groups cost more small launches than they overlap on a 512-tile batch):
+  // group k holds tiles [grp_lo[k], grp_lo[k + 1])
   static constexpr int kMaxTileEvents = 64;
+  static constexpr int kPipeGroups = 16;
+  static_assert(kPipeGroups <= kMaxTileEvents, "one event of each kind per group");
   int ngrp = 0;
   int grp_lo[kMaxTileEvents + 1] = {};
   cudaEvent_t ev_tile[kMaxTileEvents] = {};  // per-group PP force done (host kicks)
@@ -989,7 +992,7 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
     CU(cudaStreamWaitEvent(g.copy, g.ev_fork, 0));
     const int64_t rows = (int64_t)L.nte * L.nte;
     // groups of consecutive tiles, at most kMaxTileEvents of them
-    g.ngrp = std::min(L.ntile, Ctx::kMaxTileEvents);
+    g.ngrp = std::min(L.ntile, Ctx::kPipeGroups);
     for (int k = 0; k <= g.ngrp; k++) g.grp_lo[k] = (int)((int64_t)k * L.ntile / g.ngrp);
     for (int k = 0; k < g.ngrp; k++) {
       const int t0 = g.grp_lo[k], t1 = g.grp_lo[k + 1];
