@@ -70,18 +70,19 @@ struct Ctx {
   int ngrp = 0;
   int grp_lo[kMaxTileEvents + 1] = {};
   cudaEvent_t ev_tile[kMaxTileEvents] = {};  // per-group PP force done (host kicks)
-  cudaEvent_t ev_copied = nullptr;           // last per-tile vp copy enqueued
+  cudaEvent_t ev_copied = nullptr;           // last per-group vp copy enqueued
   bool vp_copied = false;                    // this host kick's vp is already on its way back
-  // Host kicks upload xp tile by tile on `copy`; the deposit of a tile waits only for its
-  // own part, everything else that reads xp waits for all of it.
+  // Host kicks upload xp group by group on `copy`; the deposit of a group waits only for its
+  // own part (and so does the binning of a spill-free layout), everything else that reads xp
+  // waits for all of it.
   cudaEvent_t ev_xp[kMaxTileEvents] = {};
   bool xp_pending = false;
-  int xp_tiles = 0;
-  // ... and vp tile by tile too: the PM3 gather of a tile waits for its vp, and the PP force
-  // of a tile (on side or side2) waits for that tile's gather (ev_ready) and the binning.
+  int xp_tiles = 0;  // groups uploaded
+  // ... and vp group by group too: the PM3 gather of a group waits for its vp, and the PP force
+  // of a group (on side or side2) waits for that group's gather (ev_ready) and the binning.
   cudaEvent_t ev_vp[kMaxTileEvents] = {}, ev_ready[kMaxTileEvents] = {};
-  int vp_tiles = 0;          // > 0: vp was uploaded in this many tile parts
-  bool ready_tiles = false;  // ev_ready[t] recorded by this kick's PM3
+  int vp_tiles = 0;          // > 0: vp was uploaded in this many group parts
+  bool ready_tiles = false;  // ev_ready[k] recorded by this kick's PM3
   cudaStream_t side2 = nullptr;
   cudaEvent_t ev_pm3done = nullptr, ev_join2 = nullptr;
   Buf xp, rhoc, idx, vp, cell_base;
@@ -395,8 +396,8 @@ struct Dev {
   const int64_t *idx;
   float *vp;
   int64_t n_used;
-  // host kicks only: the caller's vp and spine; each tile's vp is copied back as soon as
-  // that tile's PP force kernel has finished
+  // host kicks only: the caller's vp and spine; each group's vp is copied back as soon as
+  // that group's PP force kernel has finished
   float *h_vp = nullptr;
   const int64_t *h_idx = nullptr;
 };
@@ -986,7 +987,7 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   CU(cudaMemcpyAsync(g.idx.p, idx_b_r, sizeof(int64_t) * nrows, cudaMemcpyHostToDevice, g.stream));
   g.ngrp = 0;
   if (n_used) {
-    // xp tile by tile, so that the deposit of the first tiles overlaps the copy of the rest
+    // xp group by group, so that the deposit of the first tiles overlaps the copy of the rest
     // (the copy stream first waits for the compute stream's earlier work on these buffers)
     CU(cudaEventRecord(g.ev_fork, g.stream));
     CU(cudaStreamWaitEvent(g.copy, g.ev_fork, 0));
