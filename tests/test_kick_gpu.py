@@ -95,3 +95,27 @@ def test_kick_vs_fp64_truth_zeldovich(gpu):
     F = v[samp].astype(np.float64) / kick
     rel = np.sqrt(np.sum((F - Fd) ** 2) / np.sum(Fd ** 2))
     assert rel < 0.01, rel
+
+
+def test_host_kick_rejects_an_inconsistent_spine_and_recovers(gpu):
+    """A spine row that disagrees with its rhoc row makes the host call return
+    CUBE_ERR_INVALID without kicking or writing vp, and the next valid call gives the usual
+    kick."""
+    import dataclasses
+    from cube2_b200.kick import CubeError, FineKick
+    img, _ = load_golden("t32")
+    L = img.layout
+    fk = FineKick(L)
+    isort, ires, ix, apm3, rs = _tables(L)
+    want, out_want = fk.kick_fine(img, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0)
+    bad_idx = img.idx_b_r.copy()
+    rows = L.nte * L.nte
+    bad_idx.reshape(-1)[rows // 2] += 1  # an inner row of tile 0: the tile ends stay consistent
+    bad = dataclasses.replace(img, idx_b_r=bad_idx)
+    vp = img.vp.copy()
+    with pytest.raises(CubeError):
+        fk.kick_fine(bad, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0, vp=vp)
+    np.testing.assert_array_equal(vp, img.vp)  # nothing was written back
+    got, out_got = fk.kick_fine(img, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0)
+    d_w, d_g = (want - img.vp).astype(np.float64), (got - img.vp).astype(np.float64)
+    assert np.sqrt(np.sum((d_g - d_w) ** 2) / np.sum(d_w ** 2)) < 1e-6
