@@ -1113,6 +1113,32 @@ int cube_pp_shapes(cube_pp_shape_info *out, int32_t cap, int32_t *n_shapes, int3
   return CUBE_OK;
 }
 
+int cube_pp_work_stats(int64_t out[4]) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!out) return fail(CUBE_ERR_INVALID);
+  for (int k = 0; k < 4; k++) out[k] = 0;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!g.items.p || !g.sched.p) return CUBE_OK;  // no PP kick yet
+  CU(cudaDeviceSynchronize());
+  int32_t n = 0;
+  CU(cudaMemcpy(&n, (const int32_t *)g.sched.p + sched_total_index(g.L.ntile), sizeof(int32_t),
+                cudaMemcpyDeviceToHost));
+  const size_t cap = g.items.cap / sizeof(PPItem);
+  if (n < 0 || (size_t)n > cap) return fail(CUBE_ERR_CAPACITY);
+  std::vector<PPItem> it((size_t)n);
+  if (n) CU(cudaMemcpy(it.data(), g.items.p, sizeof(PPItem) * (size_t)n, cudaMemcpyDeviceToHost));
+  std::unordered_map<uint32_t, int> per_cell;
+  for (const PPItem &x : it) per_cell[x.cell]++;
+  for (const PPItem &x : it) {
+    const int ni = x.dims & 0xff, span = (x.dims >> 24) & 0xff;
+    if (per_cell[x.cell] > 1) out[1]++;
+    if (span > 0) out[2]++;
+    out[3] = std::max<int64_t>(out[3], ni);
+  }
+  out[0] = n;
+  return CUBE_OK;
+}
+
 int cube_get_layout(cube_layout *l) {
   if (!l) return fail(CUBE_ERR_INVALID);
   if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);

@@ -156,6 +156,7 @@ struct PPArgs {
   int shape;                  // kernel shape index (pp_shape_desc); 0 with `pairs`
 };
 size_t sched_ints(int ntile);
+int64_t sched_total_index(int ntile);  // where the work list's item count lies in `sched`
 int pp_num_shapes();
 PPShapeDesc pp_shape_desc(int i);
 int pp_min_chunk();  // smallest chunk of any shape: the work list capacity is sized for it

@@ -56,6 +56,20 @@ static unsigned char *g_na_addr[kNaMaxDevices] = {};
 
 size_t noalloc_scratch_bytes() { return kNaBytes; }
 
+// The per-call tables (PP grid per tile, PP range per subtile) travel to the scratch as a
+// kernel argument, so no copy on the GPU reads this call's host stack after it returns.
+struct NaTables {
+  TilePP tiles[kNaTiles];
+  float range[kNaSub];
+  int32_t ntile, nsub;
+};
+static_assert(sizeof(NaTables) <= 32000, "kernel parameter space (32764 bytes on sm_70 and later)");
+
+__global__ void k_na_tables(const NaTables t, TilePP *tiles, float *range) {
+  for (int i = threadIdx.x; i < t.ntile; i += blockDim.x) tiles[i] = t.tiles[i];
+  for (int i = threadIdx.x; i < t.nsub; i += blockDim.x) range[i] = t.range[i];
+}
+
 int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
                      const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp,
                      int64_t n_used, float *d_vp, float mass, float a_mid, float dt, float *d_out,
@@ -71,7 +85,11 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
   // per-subtile tables by location (pp_force_kernel.cu:987-1004), on the stack
   int ires_loc[kNaSub];
   bool seen[kNaSub];
-  float range_loc[kNaSub];
+  NaTables tab;
+  float *range_loc = tab.range;
+  TilePP *tiles = tab.tiles;
+  tab.ntile = L.ntile;
+  tab.nsub = L.ns3;
   for (int q = 0; q < L.ns3; q++) seen[q] = false;
   for (int it = 0; it < L.ns3; it++) {
     const int *r = ixyz3 + 6 * it;
@@ -85,7 +103,6 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
     ires_loc[loc] = ires[it];
     range_loc[loc] = apm3[ires[it] - 1];
   }
-  TilePP tiles[kNaTiles];
   int64_t ncells = 0, interior = 0;
   int max_rcp = 1;
   const int nss = L.nns * L.nns * L.nns;
@@ -129,10 +146,7 @@ int pp_force_noalloc(const Lay &L, const int32_t *ires, const int32_t *ixyz3, co
   // the scratch keeps the previous call's contents: reset what must start at zero
   if (cudaMemsetAsync(ctr, 0, sizeof(int32_t) * 128, s) != cudaSuccess) return CUBE_ERR_CUDA;
   if (cudaMemsetAsync(d_out, 0, sizeof(float) * 6, s) != cudaSuccess) return CUBE_ERR_CUDA;
-  if (cudaMemcpyAsync(d_tiles, tiles, sizeof(TilePP) * L.ntile, cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return CUBE_ERR_CUDA;
-  if (cudaMemcpyAsync(d_range, range_loc, sizeof(float) * L.ns3, cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return CUBE_ERR_CUDA;
+  k_na_tables<<<1, 256, 0, s>>>(tab, d_tiles, d_range);
 
   launch_cell_table(L, d_rhoc, d_idx_b_r, cell_base, s);
   BinArgs b{};

@@ -801,6 +801,7 @@ static PPK make_ppk(const PPArgs &a) {
 }
 
 size_t sched_ints(int ntile) { return (size_t)sched_base(ntile) + 2 * ((size_t)ntile + 1); }
+int64_t sched_total_index(int ntile) { return sched_base(ntile) + ntile; }
 
 int pp_num_shapes() { return kNumShapes; }
 PPShapeDesc pp_shape_desc(int i) { return kShapes[i >= 0 && i < kNumShapes ? i : 0]; }
@@ -826,21 +827,27 @@ void launch_pp_items(const PPArgs &a, cudaStream_t s) {
 }
 
 // One persistent block per resident slot: blocks beyond the resident count would only start
-// once the queue is empty.  The count is looked up once per kernel (slot = shape, or the
-// pair-count kernel).
+// once the queue is empty.  The shared-memory attribute is set and the count looked up once per
+// kernel (slot = shape, or the pair-count kernel) and device: the attribute is per device.
+constexpr int kMaxDevices = 64;
 template <bool COUNT, int S>
 static void launch_force_shape(const PPK &p, int num_sms, cudaStream_t s) {
   constexpr PPShapeDesc d = COUNT ? kCountShape : kShapes[S];
   constexpr size_t smem = pp_smem_block(d.jtile, d.packed != 0);
   auto fn = k_pp_force<COUNT, d.chunk, d.jtile, d.unroll, d.blocks, d.packed != 0>;
-  static int per_sm = 0;
-  if (!per_sm) {
+  static int per_sm[kMaxDevices] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int n = 0;
+  if (dev < 0 || dev >= kMaxDevices || !per_sm[dev]) {
     cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, (const void *)fn, kPPThreads, smem);
-    per_sm = n > 0 ? n : 1;
+    n = n > 0 ? n : 1;
+    if (dev >= 0 && dev < kMaxDevices) per_sm[dev] = n;
+  } else {
+    n = per_sm[dev];
   }
-  fn<<<per_sm * num_sms, kPPThreads, smem, s>>>(p);
+  fn<<<n * num_sms, kPPThreads, smem, s>>>(p);
 }
 
 template <int... I>

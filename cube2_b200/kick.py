@@ -58,7 +58,7 @@ EXPORTS = ("cube_set_layout", "cube_get_layout", "cube_last_error", "cube_error_
            "cube_mlp_get_params", "cube_mlp_features", "cube_mlp_train_step", "cube_mlp_forward", "cube_mlp_kick",
            "cube_pp_set_shape", "cube_pp_shapes", "cube_drift_device", "cube_drift", "cube_buffer_v_device",
            "cube_power_spectrum", "cube_snapshot_write", "cube_snapshot_read", "cube_pm1_force_device",
-           "cube_pm2_force_device")
+           "cube_pm2_force_device", "cube_pp_work_stats")
 
 
 def lib() -> ctypes.CDLL:
@@ -117,6 +117,13 @@ def pp_shapes():
     _check(lib().cube_pp_shapes(arr, n.value, None, None), "cube_pp_shapes")
     table = [{k: getattr(e, k) for k, _ in CPPShape._fields_} for e in arr]
     return table, cur.value
+
+
+def pp_work_stats() -> dict:
+    """The PP work list of the last PP kick: items, items of split cells, grouped items, largest item."""
+    out = np.zeros(4, np.int64)
+    _check(lib().cube_pp_work_stats(_p(out)), "cube_pp_work_stats")
+    return dict(items=int(out[0]), split_items=int(out[1]), grouped_items=int(out[2]), max_ni=int(out[3]))
 
 
 class KickGraph:

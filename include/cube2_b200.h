@@ -19,7 +19,11 @@
  *
  * Errors never terminate the process.  The reference-named void entry points
  * record a status readable with cube_last_error(); the cube_* variants
- * return it.
+ * return it.  A call rejected on the host (bad arguments, metadata or sizes)
+ * leaves every output untouched.  A call whose failure is found on the
+ * device (CUBE_ERR_CAPACITY or CUBE_ERR_INVALID from the device status word,
+ * CUBE_ERR_TIMEOUT) has already run kernels: its outputs, vp included, are
+ * then undefined (part of vp may hold the kick).
  */
 #ifndef CUBE2_B200_H
 #define CUBE2_B200_H
@@ -256,6 +260,11 @@ typedef struct cube_pp_shape_info {
 int cube_pp_set_shape(int32_t shape);
 /* The shape table (up to `cap` entries), its size and the shape of the last PP kick. */
 int cube_pp_shapes(cube_pp_shape_info *out, int32_t cap, int32_t *n_shapes, int32_t *current);
+/* Inspection of the PP work list the last PP kick ran (waits for the device):
+ * out[0] = work items, out[1] = items that hold one chunk of a PP cell split across
+ * several items, out[2] = items that group two or four sparse PP cells along x,
+ * out[3] = the largest particle count of one item.  All zero before the first kick. */
+int cube_pp_work_stats(int64_t out[4]);
 
 /* ---- learned PP shell (no reference counterpart) ---- */
 

@@ -5,6 +5,10 @@ Python drivers for the CPU checkers:
 * :class:`RefPP`        the reference's pp_force_kernel.c, compiled per layout
                         (``oracle/_ref``), called through its own C ABI
                         (pp_force_kernel.c:134-141, :393-400);
+* :class:`RefCuda`      the reference's CUDA kick (pm3_fft_cuda.cu +
+                        pp_force_kernel.cu), compiled per layout for sm_100a,
+                        called through its own C ABI (pm3_fft_cuda.cu:516-520,
+                        pp_force_kernel.cu:960-963, :515-522);
 * :func:`pm3_periodic`  PM3 on one periodic image mesh (restatement of
                         kick.f90:403-568 with wrap-around);
 * :func:`pm3_subtile`   PM3 on the reference's per-subtile buffered meshes;
@@ -29,7 +33,7 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 _SRCS = [os.path.join(HERE, "pm3_oracle.c"), os.path.join(HERE, "ewald.c")]
 
 sys.path.insert(0, HERE)
-from layouts import LAYOUTS, ref_lib_name  # noqa: E402
+from layouts import GPU_BUILDS, LAYOUTS, ref_gpu_lib_name, ref_lib_name  # noqa: E402
 
 _c_i = ctypes.c_int
 _c_i64 = ctypes.c_int64
@@ -173,6 +177,137 @@ class RefPP:
         v = np.ascontiguousarray(vals, dtype=np.uint32).copy()
         self.lib.radix_sort_u32_pair(_ptr(k), _ptr(v), _c_i(k.shape[0]))
         return k, v
+
+
+class RefCuda:
+    """The reference's CUDA kick for one compiled layout (``GPU_BUILDS``).
+
+    PM3 (pm3_fft_cuda.cu:516-620) leaves its velocity change in the reference's
+    shared device accumulator; :meth:`kick` reads it there through
+    ``c_gpu_velocity_get`` (pp_force_kernel.cu:515-522), then runs the reference
+    PP (pp_force_kernel.cu:960-1050), which adds its own change and merges both
+    into the host velocities.
+
+    The reference ends the process (``exit``/``abort``) on any capacity or
+    metadata error, so every input is checked here first against the limits the
+    reference would enforce (pp_force_kernel.cu:45-51, :818-821, :964-1000,
+    pm3_fft_cuda.cu:392-401).
+    """
+
+    _cudart = None
+
+    def __init__(self, name: str):
+        self.params = dict(GPU_BUILDS[name])
+        self.path = os.path.join(REF_DIR, ref_gpu_lib_name(self.params))
+        if not os.path.exists(self.path):
+            raise FileNotFoundError(f"reference CUDA build missing: {self.path} (run oracle/build_ref.py)")
+        self.lib = ctypes.CDLL(self.path)
+        for f in ("c_pm3_force_kernel", "c_pp_force_kernel", "c_gpu_velocity_finalize", "c_pm3_fft_finalize"):
+            getattr(self.lib, f).restype = None
+        self.lib.c_gpu_velocity_get.restype = ctypes.c_void_p
+        self.lib.c_gpu_velocity_get.argtypes = [_c_i]
+        if RefCuda._cudart is None:
+            home = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+            RefCuda._cudart = ctypes.CDLL(os.path.join(home, "lib64", "libcudart.so.12"))
+            RefCuda._cudart.cudaMemcpy.restype = _c_i
+            RefCuda._cudart.cudaMemcpy.argtypes = [_p, _p, ctypes.c_size_t, _c_i]
+        p = self.params
+        nc = p["ng"] // p["ratio_cs"]
+        nt = nc // p["nnt"]
+        nte = nt + 2 * (p["ngb"] // p["ratio_cs"])
+        np_image = (nc * p["np_nc"]) ** 3
+        a = nte * 1.0 / nt
+        # the reference's own capacity arithmetic, in its order of operations (pp_force_kernel.cu:45-51)
+        self.np_image_max = int(np_image * a * a * a * p["image_buffer"])
+        self.np_tile_max = int(np_image // p["nnt"] ** 3 * (a * a * a) * p["tile_buffer"])
+
+    def _check(self, img, ires, ixyz3):
+        L = img.layout
+        p = self.params
+        for k in ("ng", "nnt", "nns", "ratio_cs", "ngb"):
+            if getattr(L, k) != p[k]:
+                raise ValueError(f"image layout {k}={getattr(L, k)} differs from the build's {p[k]}")
+        if p["ng"] > 512 or L.nt + 2 >= 128:
+            raise ValueError("layout outside the reference CUDA PP's exact range")
+        if not (0 <= img.n_used <= min(self.np_image_max, 2 ** 31 - 1)):
+            raise ValueError(f"{img.n_used} stored particles exceed the reference capacity {self.np_image_max}")
+        ires = np.asarray(ires)
+        if ires.min() < 2 or ires.max() > 6:
+            raise ValueError("ires outside 2..6")
+        ix = np.asarray(ixyz3)
+        if ix[:, :3].min() < 1 or ix[:, :3].max() > L.nns or ix[:, 3:].min() < 1 or ix[:, 3:].max() > L.nnt:
+            raise ValueError("ixyz3 outside the layout")
+        # particles staged per parent tile: the subtile cells plus a one coarse-cell ring
+        ncb = L.ncb
+        r = img.rhoc.reshape(L.nnt ** 3, L.nte, L.nte, L.nte)[:, ncb - 1:ncb + L.nt + 1, ncb - 1:ncb + L.nt + 1,
+                                                               ncb - 1:ncb + L.nt + 1]
+        if int(r.reshape(L.nnt ** 3, -1).sum(axis=1).max()) > self.np_tile_max:
+            raise ValueError("a parent tile exceeds the reference capacity np_tile_max")
+
+    def _d2h(self, dptr: int, n: int) -> np.ndarray:
+        out = np.empty(n, dtype=np.float32)
+        st = RefCuda._cudart.cudaMemcpy(out.ctypes.data, dptr, n * 4, 2)
+        if st != 0:
+            raise RuntimeError(f"cudaMemcpy of the reference accumulator failed ({st})")
+        return out
+
+    def kick(self, img, isort, ires, ixyz3, apm3, ratio_sf, greens: dict, mass, a_mid, dt, vp=None):
+        """PM3 then PP through the reference's CUDA path, as kick.f90:143-205 calls them.
+
+        Returns dict(dv_pm3 float32 [n_used,3] (the PM3 change alone), f2max_pm3,
+        ptotal_pm3 [ns3], vp (after both), f2max_pp, vmax [3], ptotal_pp [ns3]).
+        """
+        L = img.layout
+        isort = np.ascontiguousarray(isort, dtype=np.int32)
+        ires = np.ascontiguousarray(ires, dtype=np.int32)
+        ixyz3 = np.ascontiguousarray(ixyz3, dtype=np.int32)
+        apm3 = np.ascontiguousarray(apm3, dtype=np.float32)
+        ratio_sf = np.ascontiguousarray(ratio_sf, dtype=np.int32)
+        self._check(img, ires, ixyz3)
+        # one FFT batch per (parent tile, level) holds at most 64 subtiles (pm3_fft_cuda.cu:392-401)
+        if L.nns ** 3 > 64:
+            raise ValueError("more than 64 subtiles per parent tile")
+        gk = []
+        keep = []
+        for lev in range(2, 7):
+            g = greens.get(lev) if greens else None
+            if g is not None:
+                g = np.ascontiguousarray(g, dtype=np.float32)
+                keep.append(g)
+                gk.append(g.ctypes.data_as(_p))
+            else:
+                gk.append(None)
+        used = set(int(v) for v in ires.tolist())
+        for lev in used:
+            rsf = int(ratio_sf[lev - 1])
+            n = L.ntt * L.ratio_cs * rsf + 2 * L.ratio_cs * rsf
+            g = greens.get(lev)
+            if g is None or g.size != n * n * (n // 2 + 1):
+                raise ValueError(f"level {lev} needs a Green table of {n}^2 x {n // 2 + 1}")
+        vp = np.ascontiguousarray(img.vp.copy() if vp is None else vp, dtype=np.float32)
+        f2 = np.zeros(1, np.float32)
+        vm = np.zeros(3, np.float32)
+        pt = np.zeros(L.ns3, np.float64)
+        self.lib.c_pm3_force_kernel(_ptr(isort), _ptr(ires), _ptr(ixyz3), _ptr(ratio_sf), _ptr(img.rhoc),
+                                    _ptr(img.idx_b_r), _ptr(img.xp), *gk, _ptr(vp), _c_f(mass), _c_f(a_mid),
+                                    _c_f(dt), _ptr(f2), _ptr(vm), _ptr(pt))
+        n_used = img.n_used
+        dv = self._d2h(self.lib.c_gpu_velocity_get(_c_i(n_used)), 3 * n_used).reshape(n_used, 3)
+        out = dict(dv_pm3=dv, f2max_pm3=float(f2[0]), ptotal_pm3=pt.copy())
+        f2p = np.zeros(1, np.float32)
+        vmax = np.zeros(3, np.float32)
+        ptp = np.zeros(L.ns3, np.float64)
+        tt = np.zeros(L.ns3, np.float64)
+        self.lib.c_pp_force_kernel(_ptr(isort), _ptr(ires), _ptr(ixyz3), _ptr(apm3), _ptr(ratio_sf),
+                                   _ptr(img.rhoc), _ptr(img.idx_b_r), _ptr(img.xp), _ptr(vp), _c_f(mass),
+                                   _c_f(a_mid), _c_f(dt), _ptr(f2p), _ptr(vmax), _ptr(ptp), _ptr(tt))
+        del keep
+        out.update(vp=vp, f2max_pp=float(f2p[0]), vmax=vmax, ptotal_pp=ptp, seconds_pp=tt)
+        return out
+
+    def finalize(self):
+        self.lib.c_gpu_velocity_finalize()
+        self.lib.c_pm3_fft_finalize()
 
 
 def ref_layout_params(name: str) -> dict:

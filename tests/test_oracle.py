@@ -163,3 +163,25 @@ def test_four_layer_split_oracle_matches_fp64_truth(oracle_lib):
     # each long-range layer is needed: without it the error is several per cent
     assert err(tot - p1["dv"][act]) > 0.02
     assert err(tot - p2["dv"][act]) > 0.02
+
+
+def test_reference_cuda_builds_load_and_size_like_the_reference():
+    """The reference's CUDA path, built per layout for sm_100a (oracle/build_ref.py), loads
+    without a GPU and exports its C ABI (pm3_fft_cuda.cu:516-628, pp_force_kernel.cu:496-547,
+    :960); the capacity guard that keeps it from exit()ing uses the reference's own arithmetic
+    (pp_force_kernel.cu:45-51)."""
+    from oracle import oracle as O
+    from oracle.layouts import GPU_BUILDS
+    for name, p in GPU_BUILDS.items():
+        try:
+            r = O.RefCuda(name)
+        except FileNotFoundError:
+            pytest.skip("reference CUDA build missing (needs the reference tree)")
+        for sym in ("c_pm3_force_kernel", "c_pp_force_kernel", "c_gpu_velocity_get", "c_gpu_velocity_finalize",
+                    "c_pm3_fft_finalize", "c_select_gpu_for_image"):
+            getattr(r.lib, sym)
+        nc = p["ng"] // p["ratio_cs"]
+        nt = nc // p["nnt"]
+        nte = nt + 2 * (p["ngb"] // p["ratio_cs"])
+        assert r.np_image_max == int(p["ng"] ** 3 * (nte / nt) ** 3 * p["image_buffer"] + 1e-6)
+        assert r.np_tile_max >= p["ng"] ** 3 // p["nnt"] ** 3

@@ -21,14 +21,14 @@ def _tables(L):
             RATIO_SF.copy())
 
 
-def _noalloc(img, isort, ires, ix, apm3, rs, d_rhoc, d_idx, d_xp, d_vp, d_out, n_used=None):
+def _noalloc(img, isort, ires, ix, apm3, rs, d_rhoc, d_idx, d_xp, d_vp, d_out, n_used=None, stream=None):
     from cube2_b200.kick import _p, lib
     f = lib().cube_pp_force_noalloc
     return f(_p(isort), _p(ires), _p(ix), _p(apm3), _p(rs), ctypes.c_void_p(d_rhoc.data_ptr()),
              ctypes.c_void_p(d_idx.data_ptr()), ctypes.c_void_p(d_xp.data_ptr()),
              ctypes.c_int64(img.n_used if n_used is None else n_used), ctypes.c_void_p(d_vp.data_ptr()),
              ctypes.c_float(1.0), ctypes.c_float(SIXPI), ctypes.c_float(1.0), ctypes.c_void_p(d_out.data_ptr()),
-             None)
+             None if stream is None else ctypes.c_void_p(stream.cuda_stream))
 
 
 def _case(name):
@@ -54,11 +54,15 @@ def test_noalloc_matches_regular_entry_point_twice(gpu, name):
     d_xp = torch.from_numpy(img.xp.reshape(-1).copy()).to(dev)
     vp0 = torch.from_numpy(img.vp.reshape(-1).copy()).to(dev)
     torch.cuda.synchronize()
-    for call in range(2):  # the shared scratch keeps the previous call's contents
+    side = torch.cuda.Stream(device=dev)
+    for call in range(3):  # the shared scratch keeps the previous call's contents
         d_vp = vp0.clone()
         d_out = torch.full((8,), 7.0, dtype=torch.float32, device=dev)
         torch.cuda.synchronize()
-        assert _noalloc(img, isort, ires, ix, apm3, rs, d_rhoc, d_idx, d_xp, d_vp, d_out) == 0
+        # the third call runs on a stream of the caller's
+        st = _noalloc(img, isort, ires, ix, apm3, rs, d_rhoc, d_idx, d_xp, d_vp, d_out,
+                      stream=side if call == 2 else None)
+        assert st == 0
         torch.cuda.synchronize()
         got = d_vp.cpu().numpy().reshape(-1, 3)
         dgot = (got - img.vp).astype(np.float64)
@@ -82,4 +86,27 @@ def test_noalloc_rejects_inputs_beyond_its_scratch(gpu):
     too_many = 524288 + 1  # CUBE_NOALLOC_MAX_PARTICLES + 1
     st = _noalloc(img, isort, ires, ix, apm3, rs, t, t, t, t, t, n_used=too_many)
     assert st == 5  # CUBE_ERR_CAPACITY, nothing launched
+    assert lib().cube_last_error() == 5
+
+
+@pytest.mark.parametrize("geom", [(128, 1, 2), (80, 5, 2), (256, 2, 2)])
+def test_noalloc_rejects_layouts_beyond_its_scratch(gpu, geom):
+    """More PP cells than CUBE_NOALLOC_MAX_CELLS (a 128^3 tile: 68^3 PP cells), more than 64
+    tiles (5^3), more coarse cells over the extended tiles than CUBE_NOALLOC_MAX_CELLS
+    (8 x 34^3): rejected with CUBE_ERR_CAPACITY before anything is launched."""
+    import torch
+    from cube2_b200.kick import FineKick, lib
+    from cube2_b200.layout import Layout
+    ng, nnt, nns = geom
+    L = Layout(ng=ng, nnt=nnt, nns=nns, ratio_cs=4, ngb=4, app=0.1)
+    FineKick(L)
+    isort, ires, ix, apm3, rs = _tables(L)
+    dev = torch.device("cuda:0")
+    t = torch.zeros(16, dtype=torch.float32, device=dev)
+
+    class _Img:
+        n_used = 1
+
+    st = _noalloc(_Img, isort, ires, ix, apm3, rs, t, t, t, t, t)
+    assert st == 5
     assert lib().cube_last_error() == 5
