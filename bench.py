@@ -17,7 +17,11 @@ cutoff 2 fine cells; see cube2_b200/workloads.py).
   against the FP32 FMA peak measured in the same run.
 * ``cpu_baseline`` / ``--impl reference``: the reference's own CPU PP kernel
   (pp_force_kernel.c, built from the reference sources into oracle/_ref) plus
-  the CPU restatement of the reference PM3 on the same inputs.
+  the CPU restatement of the reference PM3 on the same inputs, a full kick of
+  the whole image per step.
+* ``batch``   the batched uneven boxes (batch512) in one kick, as a CUDA graph
+  and against one kick call per box; ``conservation`` the FP64 momentum and
+  kinetic-energy change of one kick; ``drift`` and ``learned`` the other legs.
 """
 from __future__ import annotations
 
@@ -57,6 +61,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     return ap.parse_args()
 
 
@@ -255,6 +260,28 @@ def run_ours(args, rank, world, local_rank):
         e2e = {"value": N * world * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * te / args.steps}
 
+    # FP64 momentum and kinetic-energy change of one kick, reduced on the device (outside the timed region)
+    conservation = None
+    try:
+        from cube2_b200.kick import kick_sums
+        d_vp.copy_(vp0)
+        kick()
+        torch.cuda.synchronize()
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        cs = kick_sums(d_rhoc, d_idx, img.n_used, vp0, d_vp, 1.0, stream=stream)
+        c1.record(stream)
+        torch.cuda.synchronize()
+        conservation = {"momentum_change": [float(x) for x in cs["momentum"]],
+                        "momentum_change_rel": [float(a / b) for a, b in zip(cs["momentum"], cs["momentum_scale"])],
+                        "kinetic_energy_change": cs["kinetic_energy"], "particles": cs["particles"],
+                        "ms": c0.elapsed_time(c1),
+                        "what": "cube_kick_sums over the physical particles of one kick (PM3 + PP), FP64 on the "
+                                "device; momentum_change_rel = sum m dv / sum |m dv| per axis"}
+    except Exception as e:  # reported beside the kick, never instead of it
+        conservation = {"error": repr(e)}
+
     # force error against the FP64 direct sum (outside the timed region)
     truth = None
     if not args.no_truth and rank == 0:
@@ -296,6 +323,13 @@ def run_ours(args, rank, world, local_rank):
     loop = per_box_loop(args.workload, fk, img, stream, a_mid, dt, ms_step) if batch and rank == 0 else None
     if batch:
         fk.configure()
+    batch_obj = None
+    if not batch and rank == 0 and not args.no_batch:
+        try:
+            batch_obj = batch_leg("batch512", stream, args.steps, args.warmup)
+        except Exception as e:  # reported beside the kick, never instead of it
+            batch_obj = {"error": repr(e)}
+        fk.configure()
     drift = None
     if rank == 0:
         try:
@@ -317,7 +351,7 @@ def run_ours(args, rank, world, local_rank):
         cpu = {"unavailable": "the reference CPU baseline is timed on the single-image workloads"}
     elif rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference(args.workload, img, sample=True)
+            cpu = cpu_reference(args.workload, img)
         except Exception as e:  # the baseline must not hide our number
             cpu = {"error": repr(e)}
 
@@ -337,7 +371,8 @@ def run_ours(args, rank, world, local_rank):
             "stages_ms": {"pm3": pm3_ms, "pp_binning_and_worklist": ppb_ms, "pp_force": ppf_ms,
                           "note": "the PP binning and work list run on a second stream beside PM3"},
             "roofline": roofline, "force_error": truth, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": ck, "cpu_baseline": cpu, "graph": graph, "pp_shape": pp_shape, "drift": drift, "learned": learned}
+            "clocks": ck, "cpu_baseline": cpu, "graph": graph, "pp_shape": pp_shape, "drift": drift, "learned": learned,
+            "conservation": conservation, "batch": batch_obj}
     if loop is not None:
         line["per_box_loop"] = loop
     if rank == 0:
@@ -494,6 +529,72 @@ def batch_truth(workload: str, img, samp, force_truth_fp64):
     return F
 
 
+def batch_leg(workload: str, stream, steps: int, warmup: int):
+    """Batched uneven boxes beside the main kick: every box of the batch workload in one kick
+    (one periodic mesh per box, one batched transform, one persistent PP launch over all boxes),
+    timed with CUDA events over K steps after W warm-up steps (the first one autotunes the PP
+    shape), then replayed as a captured CUDA graph, then against one kick call per box."""
+    import torch
+    from cube2_b200 import workloads as W
+    from cube2_b200.kick import CUBE_PM3_TILE_PERIODIC, FineKick
+    w = W.WORKLOADS[workload]
+    img = W.make(workload)
+    L = img.layout
+    isort, ires, ix, apm3, rs = W.tables(workload)
+    fk = FineKick(L, pm3_mode=CUBE_PM3_TILE_PERIODIC, apm3f=w["apm3f"])
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_rhoc = torch.from_numpy(img.rhoc.reshape(-1).copy()).to(dev)
+    d_idx = torch.from_numpy(img.idx_b_r.reshape(-1).copy()).to(dev)
+    d_xp = torch.from_numpy(img.xp.reshape(-1).copy()).to(dev)
+    d_vp = torch.from_numpy(img.vp.reshape(-1).copy()).to(dev)
+    d_out = torch.zeros(8, dtype=torch.float32, device=dev)
+    a_mid, dt = np.float32(6 * np.pi), np.float32(1.0)
+
+    def kick():
+        fk.kick_fine_device(d_rhoc, d_idx, d_xp, img.n_used, d_vp, d_out, isort, ires, ix, apm3, rs, 1.0, a_mid,
+                            dt, stream=stream)
+    for _ in range(max(warmup, 1)):
+        kick()
+    torch.cuda.synchronize()
+    err_word = int(d_out[5:6].cpu().view(torch.int32).item())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        kick()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(steps, 1)
+    gms = None
+    kg = fk.kick_graph(d_rhoc, d_idx, d_xp, img.n_used, d_vp, d_out, isort, ires, ix, apm3, rs, 1.0, a_mid, dt)
+    try:
+        for _ in range(max(warmup, 1)):
+            kg.launch(stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            kg.launch(stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        gms = e0.elapsed_time(e1) / max(steps, 1)
+    finally:
+        kg.close()
+    from cube2_b200.kick import pp_shapes
+    table, cur = pp_shapes()
+    loop = per_box_loop(workload, fk, img, stream, a_mid, dt, ms)
+    n_per = np.array([b ** 3 for b in W.batch_counts(workload)])
+    return {"workload": workload, "boxes": int(L.nnt ** 3), "box_fine_cells": w["box"],
+            "particles": int(img.n_particles), "stored": int(img.n_used),
+            "particles_per_box": {"min": int(n_per.min()), "median": int(np.median(n_per)), "max": int(n_per.max())},
+            "ms_per_step": ms, "value": img.n_particles / (ms * 1e-3), "unit": UNIT,
+            "graph_ms_per_step": gms, "graph_value": img.n_particles / (gms * 1e-3) if gms else None,
+            "per_box_loop": loop, "batched_speedup_vs_per_box_loop": loop["ms_per_step"] / ms,
+            "pp_shape": {k: table[cur][k] for k in ("chunk", "jtile", "unroll", "blocks", "packed")},
+            "device_error_mask": err_word,
+            "what": "all boxes in one kick (CUBE_PM3_TILE_PERIODIC: one 64^3 periodic mesh per box, one batched "
+                    "transform, one persistent PP launch over every box's work items), plain launches and as a "
+                    "replayed CUDA graph, against one cube_kick_fine_device call per box"}
+
+
 def per_box_loop(workload: str, fk_batch, img, stream, a_mid, dt, ms_batched):
     """The same boxes kicked one call per box (device-resident, one-tile layout), timed with
     CUDA events over one pass after a warm-up pass: the launch-per-tile loop the batch replaces."""
@@ -543,53 +644,57 @@ def _nnest_for_host():
     return best
 
 
-def cpu_reference(workload: str, img, sample: bool, tile: int = 0):
-    """Time the reference CPU PP kernel + the PM3 restatement on the host cores.
-
-    sample=True times the PP of one parent tile (`tile`, z-major index) and
-    scales it by that tile's share of the interior particles."""
+def reference_setup(workload: str, img):
+    """The reference CPU path for the workload's image: the reference's own PP kernel
+    (pp_force_kernel.c, compiled for this layout and nnest host threads) and the PM3 Green
+    table, tabulated in FP64 on the host by the restatement of Green.f90 (outside any timed
+    region).  Nothing of this library is loaded."""
     from cube2_b200 import workloads as W
-    from cube2_b200.kick import green_table
+    from oracle import oracle as O
+    w = W.WORKLOADS[workload]
+    L = img.layout
+    nnest = _nnest_for_host()
+    ref = O.RefPP(L, nnest=nnest)
+    n = L.ng * w["rsf"]
+    t = time.perf_counter()
+    G = O.green_mirrored(n, w["apm3f"], 0.0, 1.0 / w["rsf"])
+    return {"ref": ref, "G": G, "nnest": nnest, "green_seconds": time.perf_counter() - t, "mesh": n}
+
+
+def reference_step(workload: str, img, setup):
+    """One fine-scale kick of the whole image through the reference CPU path: the reference's
+    c_pp_force_kernel over every parent tile (pp_force_kernel.c:393-445) and the PM3
+    restatement of kick.f90 pm_thread on the full periodic mesh (float32 FFT standing in for
+    sfftw).  Returns (seconds of PP, seconds of PM3)."""
+    from cube2_b200 import workloads as W
     from oracle import oracle as O
     w = W.WORKLOADS[workload]
     L = img.layout
     isort, ires, ix, apm3, rs = W.tables(workload)
-    nnest = _nnest_for_host()
-    ref = O.RefPP(L, nnest=nnest)
     a_mid, dt = np.float32(6 * np.pi), np.float32(1.0)
-    ntile = L.nnt ** 3
     t = time.perf_counter()
-    if sample and ntile > 1:
-        # one parent tile of the image, scaled by its share of the interior particles
-        tile = tile % ntile
-        txyz = (tile % L.nnt, (tile // L.nnt) % L.nnt, tile // (L.nnt * L.nnt))
-        out = ref.tile(img, txyz, int(ires[0]), apm3, rs, 1.0, a_mid, dt)
-        t_pp = (time.perf_counter() - t) * (img.n_particles / max(out["ncount"], 1))
-        pp_sample = f"pp_force_kernel.c c_pp_force_kernel_tile on tile {tile} of {ntile} ({out['ncount']} " \
-                    f"particles), scaled by particle share"
-    else:
-        ref.kick(img, [int(ires[0])] * ntile, apm3, rs, 1.0, a_mid, dt)
-        t_pp = time.perf_counter() - t
-        pp_sample = f"pp_force_kernel.c c_pp_force_kernel over all {ntile} tiles"
-    n = L.ng * w["rsf"]
-    G = green_table(n, w["apm3f"], 0.0, 1.0 / w["rsf"]) if _has_gpu() else O.green(n, w["apm3f"], 0.0,
-                                                                                    1.0 / w["rsf"])
+    setup["ref"].kick(img, [int(ires[0])] * L.nnt ** 3, apm3, rs, 1.0, a_mid, dt)
+    t_pp = time.perf_counter() - t
     t = time.perf_counter()
-    O.pm3_periodic(img, w["rsf"], G, 1.0, a_mid, dt, fft_dtype=np.float32)
-    t_pm3 = time.perf_counter() - t
-    value = img.n_particles / (t_pp + t_pm3)
-    return {"value": value, "unit": UNIT, "cores": int(os.cpu_count() or 1), "kind": "reference",
-            "pp_threads": nnest, "pm3_kind": "port", "seconds_pp": t_pp, "seconds_pm3": t_pm3,
-            "sample": f"{pp_sample}; PM3 restatement of kick.f90 pm_thread on the full {n}^3 periodic mesh "
-                      f"(scipy pocketfft float32 standing in for sfftw)"}
+    O.pm3_periodic(img, w["rsf"], setup["G"], 1.0, a_mid, dt, fft_dtype=np.float32)
+    return t_pp, time.perf_counter() - t
 
 
-def _has_gpu():
-    try:
-        import torch
-        return torch.cuda.is_available()
-    except Exception:
-        return False
+def _reference_sample(img, setup) -> str:
+    L = img.layout
+    return (f"the whole image every step: pp_force_kernel.c c_pp_force_kernel over all {L.nnt ** 3} parent tiles "
+            f"({setup['nnest']} OpenMP threads) + the PM3 restatement of kick.f90 pm_thread on the full "
+            f"{setup['mesh']}^3 periodic mesh (scipy pocketfft float32 standing in for sfftw); Green table "
+            f"tabulated on the host in FP64 beforehand ({setup['green_seconds']:.1f} s, untimed)")
+
+
+def cpu_reference(workload: str, img):
+    """The cpu_baseline leg: one kick of the whole image through the reference CPU path."""
+    setup = reference_setup(workload, img)
+    t_pp, t_pm3 = reference_step(workload, img, setup)
+    return {"value": img.n_particles / (t_pp + t_pm3), "unit": UNIT, "cores": int(setup["nnest"]),
+            "kind": "reference", "pm3_kind": "port", "seconds_pp": t_pp, "seconds_pm3": t_pm3,
+            "host_cores": int(os.cpu_count() or 1), "sample": _reference_sample(img, setup)}
 
 
 LOOP_METRIC = "particle-steps/s (drift + kick + buffer_v)"
@@ -726,6 +831,8 @@ def run_loop(args, rank, world, local_rank):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's own CPU implementation of the path on the host
+    cores, every step a full kick of the whole image (warm-up steps untimed)."""
     if rank != 0:
         return
     from cube2_b200 import workloads as W
@@ -738,14 +845,14 @@ def run_reference(args, rank, world):
                           "workloads; batch workloads compare against a per-box launch loop instead"}))
         return
     img = W.make(args.workload)
-    times = []
-    res = None
+    setup = reference_setup(args.workload, img)
+    pp, pm3 = [], []
     for s in range(args.warmup + args.steps):
-        # each step samples the next parent tile, so K steps cover the image
-        res = cpu_reference(args.workload, img, sample=True, tile=s)
+        t_pp, t_pm3 = reference_step(args.workload, img, setup)
         if s >= args.warmup:
-            times.append(img.n_particles / res["value"])
-    sec = float(np.mean(times)) if times else float("nan")
+            pp.append(t_pp)
+            pm3.append(t_pm3)
+    sec = float(np.mean(np.array(pp) + np.array(pm3))) if pp else float("nan")
     value = img.n_particles / sec
     w = W.WORKLOADS[args.workload]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -753,8 +860,10 @@ def run_reference(args, rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
             "config": {"workload": args.workload, "particles": img.n_particles, "pm3_mesh": img.layout.ng * w["rsf"],
                        "pp_cutoff_fine_cells": w["apm3f"] / w["rsf"], "softening_fine_cells": img.layout.app},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
-                             "sample": res["sample"]},
+            "stages_ms": {"pp": 1e3 * float(np.mean(pp)), "pm3": 1e3 * float(np.mean(pm3))},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(setup["nnest"]), "kind": "reference",
+                             "pm3_kind": "port", "host_cores": int(os.cpu_count() or 1),
+                             "sample": _reference_sample(img, setup)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 

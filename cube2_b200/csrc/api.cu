@@ -104,6 +104,7 @@ struct Ctx {
       dr_cursor, dr_phys, dr_list, dr_off, dr_rows, dr_total;
   Buf dh_rhoc, dh_idx, dh_xp, dh_vp, dh_pid, dh_rhoc2, dh_idx2, dh_xp2, dh_vp2, dh_pid2;  // host-array drift
   Buf pw_grid, pw_k, pw_bins;  // power spectrum
+  Buf ks_out;                  // FP64 conservation sums
   cudaEvent_t tune_ev[2 * kMaxPPShapes] = {};
   void *h_stage = nullptr;  // pinned staging for small tables
   size_t h_stage_cap = 0;
@@ -1594,6 +1595,24 @@ int cube_snapshot_read(const char *prefix, const char *suffix, cube_sim_header *
 
 // ---- CIC power spectrum (utilities/cicpower.f90, utilities/powerspectrum.f90) ----
 
+int cube_kick_sums(const int32_t *d_rhoc, const int64_t *d_idx_b_r, int64_t n_used, const float *d_va,
+                   const float *d_vb, float mass, double out[8], void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!d_rhoc || !d_idx_b_r || !out || n_used < 0 || (n_used > 0 && (!d_va || !d_vb))) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  CK(grow(g.ks_out, sizeof(double) * kNumKickSums));
+  cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
+  CU(cudaMemsetAsync(g.ks_out.p, 0, sizeof(double) * kNumKickSums, st));
+  launch_kick_sums(g.L, d_rhoc, d_idx_b_r, d_va, d_vb, mass, (double *)g.ks_out.p, st);
+  g.launches += 1;
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(out, g.ks_out.p, sizeof(double) * kNumKickSums, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  return CUBE_OK;
+}
+
 int cube_power_spectrum(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
                         int64_t n_physical, int32_t nw, int32_t nbin, double *bins, void *stream) {
   std::lock_guard<std::mutex> lk(g_mu);
@@ -1955,7 +1974,7 @@ void c_gpu_velocity_finalize(void) {
   cudaSetDevice(g.device);
   cudaStreamSynchronize(g.stream);
   Buf *bufs[] = {&g.xp, &g.rhoc, &g.idx, &g.vp, &g.cell_base, &g.tiles, &g.count, &g.cell_start, &g.scan_tmp,
-                 &g.spos, &g.spill, &g.spill_rank, &g.counters, &g.items, &g.range_loc, &g.sched, &g.out};
+                 &g.spos, &g.spill, &g.spill_rank, &g.counters, &g.items, &g.range_loc, &g.sched, &g.out, &g.ks_out};
   for (Buf *b : bufs) release(*b);
 }
 

@@ -155,6 +155,11 @@ struct PPArgs {
   unsigned long long *pairs;  // non-null: count accepted pairs instead of kicking
   int shape;                  // kernel shape index (pp_shape_desc); 0 with `pairs`
 };
+// FP64 conservation sums of a kick over the physical particles (sums.cu): [0..2] sum m dv,
+// [3] kinetic-energy change, [4..6] sum |m dv|, [7] particles; d_out is accumulated into
+constexpr int kNumKickSums = 8;
+void launch_kick_sums(const Lay &L, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const float *d_va,
+                      const float *d_vb, float mass, double *d_out, cudaStream_t s);
 size_t sched_ints(int ntile);
 int64_t sched_total_index(int ntile);  // where the work list's item count lies in `sched`
 int pp_num_shapes();

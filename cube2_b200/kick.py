@@ -58,7 +58,7 @@ EXPORTS = ("cube_set_layout", "cube_get_layout", "cube_last_error", "cube_error_
            "cube_mlp_get_params", "cube_mlp_features", "cube_mlp_train_step", "cube_mlp_forward", "cube_mlp_kick",
            "cube_pp_set_shape", "cube_pp_shapes", "cube_drift_device", "cube_drift", "cube_buffer_v_device",
            "cube_power_spectrum", "cube_snapshot_write", "cube_snapshot_read", "cube_pm1_force_device",
-           "cube_pm2_force_device", "cube_pp_work_stats")
+           "cube_pm2_force_device", "cube_pp_work_stats", "cube_kick_sums")
 
 
 def lib() -> ctypes.CDLL:
@@ -117,6 +117,19 @@ def pp_shapes():
     _check(lib().cube_pp_shapes(arr, n.value, None, None), "cube_pp_shapes")
     table = [{k: getattr(e, k) for k, _ in CPPShape._fields_} for e in arr]
     return table, cur.value
+
+
+def kick_sums(d_rhoc, d_idx, n_used, d_va, d_vb, mass=1.0, stream=None) -> dict:
+    """FP64 momentum and kinetic-energy change of the physical particles between two device
+    velocity arrays (torch tensors or device pointers) of one image (cube_kick_sums)."""
+    def dp(x):
+        return ctypes.c_void_p(x if isinstance(x, int) else x.data_ptr())
+    out = np.zeros(8, np.float64)
+    s = None if stream is None else ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+    _check(lib().cube_kick_sums(dp(d_rhoc), dp(d_idx), ctypes.c_int64(int(n_used)), dp(d_va), dp(d_vb),
+                                ctypes.c_float(mass), _p(out), s), "cube_kick_sums")
+    return dict(momentum=out[0:3].copy(), kinetic_energy=float(out[3]), momentum_scale=out[4:7].copy(),
+                particles=int(out[7]))
 
 
 def pp_work_stats() -> dict:

@@ -239,6 +239,18 @@ int cube_snapshot_read(const char *prefix, const char *suffix, cube_sim_header *
 int cube_power_spectrum(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
                         int64_t n_physical, int32_t nw, int32_t nbin, double *bins, void *stream);
 
+/* ---- FP64 conservation sums (no reference counterpart) ---- */
+
+/* Momentum and kinetic-energy change of the physical particles (the interior coarse cells of
+ * every tile) between two velocity arrays of the same device image, typically vp before and
+ * after a kick: out[0..2] = sum m (vb - va) per axis, out[3] = sum m/2 (|vb|^2 - |va|^2),
+ * out[4..6] = sum |m (vb - va)| per axis (the scale against which out[0..2] is judged),
+ * out[7] = the number of physical particles.  Reduced in FP64 on the device; the call waits
+ * for `stream`.  The reference prints sums of the same kind as its own invariants
+ * ("sum of PM3 density", kick.f90:183; "sum of PP count", kick.f90:230). */
+int cube_kick_sums(const int32_t *d_rhoc, const int64_t *d_idx_b_r, int64_t n_used, const float *d_va,
+                   const float *d_vb, float mass, double out[8], void *stream);
+
 /* ---- PP kernel shape autotuner (no reference counterpart) ---- */
 
 /* The PP force kernel comes in several shapes: `chunk` i-particles per work item (a

@@ -486,3 +486,75 @@ void pm3o_green(int64_t n, double apm_soft, double apm_range, double gridsize, i
       for (int c = 0; c < 2; c++) G[((a * (n / 2)) * n + b * (n / 2)) * n1 + c * (n / 2)] = 0.0f;
   free(fs);
 }
+
+/* The same table from a quarter of the work: the wavenumbers of indices k and n - k along the
+ * second and third axes are m and -m, and Green_3D is even in each component, so rows k2, k3 in
+ * (n/2, n) are copies of rows n - k2, n - k3.  The alias sums of a mirrored row run in the
+ * opposite order, so the copies can differ from pm3o_green in the last bit of the FP64 sum (far
+ * below the float rounding of the result).  Used where a large table is tabulated on the host
+ * outside a timed region. */
+void pm3o_green_mirrored(int64_t n, double apm_soft, double apm_range, double gridsize, int p_order, float *G) {
+  const int64_t n1 = n / 2 + 1, h = n / 2;
+  const int64_t m = h + 1; /* rows 0 .. n/2 of each mirrored axis */
+  float *Q = (float *)malloc(sizeof(float) * (size_t)(m * m * n1));
+  /* tabulate the rows k2, k3 in 0..n/2 on an n-periodic grid: pm3o_green's loop restricted */
+  const double pi = 4.0 * atan(1.0);
+  const double alpha = (double)(4.0f / 3.0f);
+  const double c215 = (double)(2.0f / 15.0f);
+  const int n_int = 2;
+  double *fs = (double *)malloc(sizeof(double) * n);
+  const double inv_n = (double)(1.0f / (float)n);
+  for (int64_t k = 1; k <= n; k++) {
+    int64_t mm = (k + n / 2 - 1) % n - n / 2;
+    fs[k - 1] = 2.0 * pi * inv_n * (double)mm;
+  }
+  const float gs = (float)gridsize;
+  const double gpow = (double)(gs * gs);
+#pragma omp parallel for collapse(2) schedule(dynamic)
+  for (int64_t k3 = 0; k3 < m; k3++)
+    for (int64_t k2 = 0; k2 < m; k2++)
+      for (int64_t k1 = 0; k1 < n1; k1++) {
+        double kv[3] = {fs[k1], fs[k2], fs[k3]};
+        double D[3], ur[3] = {0, 0, 0}, u2n = 1;
+        for (int d = 0; d < 3; d++) {
+          D[d] = alpha * sin(kv[d]) + (1 - alpha) * sin(2 * kv[d]) / 2;
+          double s = sin(kv[d] / 2);
+          u2n *= 1 - s * s + c215 * s * s * s * s;
+        }
+        for (int i3 = -n_int; i3 <= n_int; i3++)
+          for (int i2 = -n_int; i2 <= n_int; i2++)
+            for (int i1 = -n_int; i1 <= n_int; i1++) {
+              double kn[3] = {kv[0] + 2 * pi * i1, kv[1] + 2 * pi * i2, kv[2] + 2 * pi * i3};
+              double kmag = sqrt(kn[0] * kn[0] + kn[1] * kn[1] + kn[2] * kn[2]);
+              double U = 1;
+              for (int d = 0; d < 3; d++) U *= (kn[d] == 0) ? 1.0 : sin(kn[d] / 2) / (kn[d] / 2);
+              U = pow(U, 2 * p_order + 2);
+              double y = apm_soft * kmag / 2, Ss, Sr;
+              Ss = (kmag == 0) ? 1.0 : 12 * pow(y, -4) * (2 - 2 * cos(y) - y * sin(y));
+              if (apm_range == 0)
+                Sr = 0;
+              else if (kmag == 0)
+                Sr = 1;
+              else {
+                double yr = apm_range * kmag / 2;
+                Sr = 12 * pow(yr, -4) * (2 - 2 * cos(yr) - yr * sin(yr));
+              }
+              double f = (Ss * Ss - Sr * Sr) / (kmag * kmag);
+              for (int d = 0; d < 3; d++) ur[d] += U * kn[d] * f;
+            }
+        double num = D[0] * ur[0] + D[1] * ur[1] + D[2] * ur[2];
+        double den = D[0] * D[0] + D[1] * D[1] + D[2] * D[2];
+        Q[(k3 * m + k2) * n1 + k1] = (float)(4 * pi * num / den / (u2n * u2n) / gpow);
+      }
+#pragma omp parallel for collapse(2)
+  for (int64_t k3 = 0; k3 < n; k3++)
+    for (int64_t k2 = 0; k2 < n; k2++) {
+      const int64_t q3 = k3 <= h ? k3 : n - k3, q2 = k2 <= h ? k2 : n - k2;
+      memcpy(G + (k3 * n + k2) * n1, Q + (q3 * m + q2) * n1, sizeof(float) * (size_t)n1);
+    }
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++)
+      for (int c = 0; c < 2; c++) G[((a * (n / 2)) * n + b * (n / 2)) * n1 + c * (n / 2)] = 0.0f;
+  free(fs);
+  free(Q);
+}
