@@ -470,7 +470,6 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     CK(get_green_periodic(n, rsf, &G));
     CK(grow(g.rho, sizeof(float) * n3 * nslots));
     CK(grow(g.rhok, sizeof(cufftComplex) * nk * nslots));
-    CK(grow(g.force, sizeof(float) * n3 * 3 * nslots));
     const double scale = (double)L.rcs / (double)(1.0f / (float)rsf);
     std::vector<MeshJob> jobs(L.ntile);
     for (int t = 0; t < L.ntile; t++) {
@@ -505,13 +504,20 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     a.cell_base = (const int64_t *)g.cell_base.p;
     a.rho = (float *)g.rho.p;
     a.rhok = (cufftComplex *)g.rhok.p;
-    a.force = (float *)g.force.p;
+    a.force = nullptr;
     a.green = G;
     a.mass = mass;
     a.kick = kick;
     a.vp = d.vp;
     a.out = (float *)g.out.p;
     a.want_vmax = want_vmax;
+    // the force difference is fused into the gather brick by brick where the geometry allows;
+    // otherwise the three force arrays are written and gathered from
+    const bool fused = pm3_brick_mc(a) > 0;
+    if (!fused) {
+      CK(grow(g.force, sizeof(float) * n3 * 3 * nslots));
+      a.force = (float *)g.force.p;
+    }
     cufftHandle fw, bw;
     CK(get_plan(n, nslots, CUFFT_R2C, &fw));
     CK(get_plan(n, nslots, CUFFT_C2R, &bw));
@@ -531,14 +537,18 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
     launch_pm3_kspace(a, g.stream);
     CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)g.rho.p));  // potential
-    launch_pm3_force(a, g.stream);
+    if (!fused) launch_pm3_force(a, g.stream);
+    auto gather = [&](const PM3Args &ga) {
+      if (fused) launch_pm3_force_gather(ga, g.stream);
+      else launch_pm3_gather(ga, g.stream);
+    };
     if (g.vp_pending && g.vp_tiles == g.ngrp && g.ngrp > 0) {  // gather each group once its vp is in
       PM3Args at = a;
       for (int k = 0; k < g.ngrp; k++) {
         CU(cudaStreamWaitEvent(g.stream, g.ev_vp[k], 0));
         at.jobs = (const MeshJob *)g.jobs.p + g.grp_lo[k];
         at.njobs = g.grp_lo[k + 1] - g.grp_lo[k];
-        launch_pm3_gather(at, g.stream);
+        gather(at);
         CU(cudaEventRecord(g.ev_ready[k], g.stream));
       }
       g.vp_pending = false;
@@ -546,9 +556,9 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       g.launches += g.ngrp - 1;
     } else {
       CK(wait_vp());
-      launch_pm3_gather(a, g.stream);
+      gather(a);
     }
-    g.launches += 4;
+    g.launches += fused ? 3 : 4;
     CU(cudaGetLastError());
     return CUBE_OK;
   }

@@ -201,6 +201,10 @@ void launch_pm3_deposit(const PM3Args &a, cudaStream_t s);
 void launch_pm3_kspace(const PM3Args &a, cudaStream_t s);
 void launch_pm3_force(const PM3Args &a, cudaStream_t s);  // force arrays + f2max from the potential
 void launch_pm3_gather(const PM3Args &a, cudaStream_t s);
+// periodic meshes: the force difference fused into the gather, brick by brick (no force arrays);
+// returns false (nothing launched) where the brick geometry does not apply
+int pm3_brick_mc(const PM3Args &a);
+bool launch_pm3_force_gather(const PM3Args &a, cudaStream_t s);
 void launch_green_fp64(int n, double apm_soft, double apm_range, double gridsize, int p_order, float *G,
                        cudaStream_t s);
 

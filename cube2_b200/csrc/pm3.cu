@@ -340,6 +340,186 @@ __global__ void __launch_bounds__(kWarps * 32, 4) k_gather(PM3K p) {
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Brick kernels for the periodic meshes (wrap = 1): one block per brick of kBrick^3 mesh points,
+// i.e. (kBrick / mc)^3 coarse cells of one job, mc = mesh points per coarse cell.  The bricks of
+// a job tile its active cells, and those of all jobs tile the mesh once.  A brick's particles
+// lie in (kBrick / mc)^2 rows of (kBrick / mc) coarse cells, and every row is one contiguous run
+// of storage, so the block walks them as one flat list.
+constexpr int kBrick = 16;               // owned mesh points per brick side
+constexpr int kFgThreads = 256;
+constexpr int kPotW = kBrick + 6;        // potential window: owned -3 .. +3 (4-point difference of TSC points)
+constexpr int kForW = kBrick + 2;        // force window: owned -1 .. +1 (the TSC stencil)
+constexpr int kMaxCb = 4;                // coarse cells per brick side (mc >= 4)
+constexpr int kMaxRowsPerBrick = kMaxCb * kMaxCb;
+constexpr size_t kFgSmem = sizeof(float) * ((size_t)kPotW * kPotW * kPotW + 3 * (size_t)kForW * kForW * kForW);
+
+struct BrickRows {
+  int nrows, total;
+  int cb;  // coarse cells per brick side
+};
+
+// The brick's rows of coarse cells: first particle, count and the coarse cells' first particles
+// (relative to the row), in shared memory; returns the particle total.
+__device__ __forceinline__ void brick_rows(const PM3K &p, const MeshJob &J, int cb, int ci0, int cj0, int ck0,
+                                          int64_t *rbase, int *rstart, int *rcell, BrickRows &br) {
+  const int nrows = cb * cb;
+  for (int r = threadIdx.x; r < nrows; r += blockDim.x) {
+    const int cj = cj0 + r % cb, ck = ck0 + r / cb;
+    const int64_t c0 = (((int64_t)J.t * p.nte + ck) * p.nte + cj) * p.nte + ci0;
+    int acc = 0;
+    for (int i = 0; i < cb; i++) {
+      rcell[r * (kMaxCb + 1) + i] = acc;
+      acc += p.rhoc[c0 + i];
+    }
+    rcell[r * (kMaxCb + 1) + cb] = acc;
+    rbase[r] = p.cell_base[c0];
+    rstart[r] = acc;  // count for now
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int r = 0; r < nrows; r++) {
+      const int c = rstart[r];
+      rstart[r] = acc;
+      acc += c;
+    }
+    rstart[nrows] = acc;
+  }
+  __syncthreads();
+  br.nrows = nrows;
+  br.total = rstart[nrows];
+  br.cb = cb;
+}
+
+// Flat particle index k of the brick -> (storage index, coarse cell offsets within the brick).
+__device__ __forceinline__ int64_t brick_particle(int k, const BrickRows &br, const int64_t *rbase, const int *rstart,
+                                                  const int *rcell, int &di, int &dj, int &dk) {
+  int lo = 0, hi = br.nrows - 1;  // last row with rstart <= k
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (rstart[mid] <= k) lo = mid; else hi = mid - 1;
+  }
+  const int l = k - rstart[lo];
+  int i = 0;
+  while (i + 1 < br.cb && rcell[lo * (kMaxCb + 1) + i + 1] <= l) i++;
+  di = i;
+  dj = lo % br.cb;
+  dk = lo / br.cb;
+  return rbase[lo] + l;
+}
+
+// Force and gather in one pass: the potential of the brick plus three points on every side is
+// read once (coalesced rows, periodic indices) into shared memory; the 4-point difference of
+// potential_to_force (kick.f90:545-568) gives the three force components on the brick plus one
+// point on every side, also in shared memory, and max |F|^2 of the owned points (kick.f90:494);
+// then every active particle of the brick gathers its 27 TSC points from there and is kicked
+// (kick.f90:497-540).  The force arrays never reach HBM.  The arithmetic (weights, products,
+// summation order) is the one of k_force_zm followed by k_gather.
+__global__ void __launch_bounds__(kFgThreads, 2) k_force_gather(PM3K p, int mc) {
+  extern __shared__ float fg_smem[];
+  float *pot = fg_smem;                                 // [z][y][x] kPotW^3
+  float *fw = pot + kPotW * kPotW * kPotW;              // [3][z][y][x] kForW^3
+  __shared__ int64_t rbase[kMaxRowsPerBrick];
+  __shared__ int rstart[kMaxRowsPerBrick + 1];
+  __shared__ int rcell[kMaxRowsPerBrick * (kMaxCb + 1)];
+  __shared__ float red[4][kFgThreads / 32];
+  const int cb = kBrick / mc;
+  const int nbx = p.ract[0] / cb, nby = p.ract[1] / cb, nbz = p.ract[2] / cb;
+  const int64_t per_job = (int64_t)nbx * nby * nbz;
+  const int j = (int)(blockIdx.x / per_job);
+  const int64_t b = blockIdx.x - (int64_t)j * per_job;
+  const MeshJob J = p.jobs[j];
+  const int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((int64_t)nbx * nby));
+  const int ci0 = J.alo[0] + bx * cb, cj0 = J.alo[1] + by * cb, ck0 = J.alo[2] + bz * cb;
+  const int64_t n = p.n, n3 = p.n3;
+  // first owned mesh point (exact: the offsets of periodic jobs are whole mesh points)
+  const int64_t X0 = wrapi(llrint((double)(ci0 - p.ncb) * p.scale - J.off[0]) + p.shift, n);
+  const int64_t Y0 = wrapi(llrint((double)(cj0 - p.ncb) * p.scale - J.off[1]) + p.shift, n);
+  const int64_t Z0 = wrapi(llrint((double)(ck0 - p.ncb) * p.scale - J.off[2]) + p.shift, n);
+  const float *phi = p.rho + (int64_t)J.slot * n3;
+  // potential window, owned - 3 .. owned + kBrick + 2 on every axis
+  for (int e = threadIdx.x; e < kPotW * kPotW * kPotW; e += kFgThreads) {
+    const int x = e % kPotW, y = (e / kPotW) % kPotW, z = e / (kPotW * kPotW);
+    const int64_t gx = wrap_near(X0 - 3 + x, n), gy = wrap_near(Y0 - 3 + y, n), gz = wrap_near(Z0 - 3 + z, n);
+    pot[e] = __ldg(phi + (gz * n + gy) * n + gx);
+  }
+  BrickRows br;
+  brick_rows(p, J, cb, ci0, cj0, ck0, rbase, rstart, rcell, br);  // its barriers cover the window too
+  const FDW w;
+  float m = 0.f;
+  constexpr int P2 = kPotW * kPotW;
+  for (int e = threadIdx.x; e < kForW * kForW * kForW; e += kFgThreads) {
+    const int x = e % kForW, y = (e / kForW) % kForW, z = e / (kForW * kForW);
+    const int c = (z + 2) * P2 + (y + 2) * kPotW + (x + 2);  // the point in the potential window
+    const float fx = w(pot[c - 2], pot[c - 1], pot[c + 1], pot[c + 2]);
+    const float fy = w(pot[c - 2 * kPotW], pot[c - kPotW], pot[c + kPotW], pot[c + 2 * kPotW]);
+    const float fz = w(pot[c - 2 * P2], pot[c - P2], pot[c + P2], pot[c + 2 * P2]);
+    fw[e] = fx;
+    fw[kForW * kForW * kForW + e] = fy;
+    fw[2 * kForW * kForW * kForW + e] = fz;
+    if (x >= 1 && x <= kBrick && y >= 1 && y <= kBrick && z >= 1 && z <= kBrick)
+      m = fmaxf(m, fx * fx + fy * fy + fz * fz);
+  }
+  __syncthreads();
+  // gather and kick
+  float vm0 = 0.f, vm1 = 0.f, vm2 = 0.f;
+  constexpr int F3 = kForW * kForW * kForW;
+  for (int k = threadIdx.x; k < br.total; k += kFgThreads) {
+    int di, dj, dk;
+    const int64_t ip = brick_particle(k, br, rbase, rstart, rcell, di, dj, dk);
+    const int16_t *q = p.xp + 3 * ip;
+    float wx[3], wy[3], wz[3];
+    // window coordinates: the TSC point floor(coord) lies at owned index floor(coord) - X0
+    const int64_t ix = tsc(decode_pos(ci0 + di - p.ncb, q[0]) * p.scale - J.off[0], wx) + p.shift;
+    const int64_t iy = tsc(decode_pos(cj0 + dj - p.ncb, q[1]) * p.scale - J.off[1], wy) + p.shift;
+    const int64_t iz = tsc(decode_pos(ck0 + dk - p.ncb, q[2]) * p.scale - J.off[2], wz) + p.shift;
+    const int lx = (int)wrap_near(ix - X0, n), ly = (int)wrap_near(iy - Y0, n), lz = (int)wrap_near(iz - Z0, n);
+    float d0 = 0.f, d1 = 0.f, d2 = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+#pragma unroll
+      for (int bb = 0; bb < 3; bb++) {
+        const int row = ((lz + c) * kForW + (ly + bb)) * kForW + lx;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+          const float wt = (wx[a] * wy[bb]) * wz[c];
+          d0 += fw[row + a] * wt;
+          d1 += fw[F3 + row + a] * wt;
+          d2 += fw[2 * F3 + row + a] * wt;
+        }
+      }
+    }
+    float *v = p.vp + 3 * ip;
+    const float v0 = v[0] + d0 * p.kick, v1 = v[1] + d1 * p.kick, v2 = v[2] + d2 * p.kick;
+    v[0] = v0;
+    v[1] = v1;
+    v[2] = v2;
+    vm0 = fmaxf(vm0, fabsf(v0));
+    vm1 = fmaxf(vm1, fabsf(v1));
+    vm2 = fmaxf(vm2, fabsf(v2));
+  }
+  // one update of each maximum per block
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  m = warp_max(m);
+  vm0 = warp_max(vm0);
+  vm1 = warp_max(vm1);
+  vm2 = warp_max(vm2);
+  if (lane == 0) {
+    red[0][warp] = m;
+    red[1][warp] = vm0;
+    red[2][warp] = vm1;
+    red[3][warp] = vm2;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    float r = 0.f;
+    for (int q = 0; q < kFgThreads / 32; q++) r = fmaxf(r, red[threadIdx.x][q]);
+    if (threadIdx.x == 0) atomic_max_nonneg(&p.out[0], r);
+    else if (p.want_vmax) atomic_max_nonneg(&p.out[1 + threadIdx.x], r);
+  }
+}
+
 static PM3K make_k(const PM3Args &a) {
   const Lay &L = *a.L;
   PM3K p;
@@ -376,11 +556,6 @@ static PM3K make_k(const PM3Args &a) {
   return p;
 }
 
-void launch_pm3_deposit(const PM3Args &a, cudaStream_t s) {
-  PM3K p = make_k(a);
-  const int64_t warps = (int64_t)a.rdep[0] * a.rdep[1] * a.rdep[2] * a.njobs;
-  k_deposit<<<(unsigned)((warps + kWarps - 1) / kWarps), kWarps * 32, 0, s>>>(p);
-}
 
 void launch_pm3_kspace(const PM3Args &a, cudaStream_t s) {
   PM3K p = make_k(a);
@@ -396,6 +571,129 @@ void launch_pm3_force(const PM3Args &a, cudaStream_t s) {
     k_force_zm<<<grid, kFzRows * 32, 0, s>>>(p);
   } else
     k_force<<<148 * 8, 256, 0, s>>>(p);
+}
+
+// Deposit brick by brick: the TSC weights of the brick's particles accumulate in a shared-memory
+// window (the brick plus one point on every side, widened to whole 16-byte groups along x) with
+// shared atomics; the window then goes to the mesh with one 16-byte vector reduction per group
+// of four points that received anything.  Every mesh point thus takes at most one global
+// reduction per brick that reaches it, instead of one per particle (kick.f90:420-468 sums the
+// same weights; the order of the float additions differs).
+constexpr int kDepThreads = 256;
+constexpr int kAccX = kBrick + 8;  // x window owned - 4 .. owned + kBrick + 3: whole float4 groups
+constexpr int kAccW = kBrick + 2;  // y, z window owned - 1 .. owned + kBrick
+
+__global__ void __launch_bounds__(kDepThreads) k_deposit_brick(PM3K p, int mc) {
+  __shared__ __align__(16) float acc[kAccW * kAccW * kAccX];
+  __shared__ int64_t rbase[kMaxRowsPerBrick];
+  __shared__ int rstart[kMaxRowsPerBrick + 1];
+  __shared__ int rcell[kMaxRowsPerBrick * (kMaxCb + 1)];
+  const int cb = kBrick / mc;
+  const int nbx = p.rdep[0] / cb, nby = p.rdep[1] / cb, nbz = p.rdep[2] / cb;
+  const int64_t per_job = (int64_t)nbx * nby * nbz;
+  const int j = (int)(blockIdx.x / per_job);
+  const int64_t b = blockIdx.x - (int64_t)j * per_job;
+  const MeshJob J = p.jobs[j];
+  const int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((int64_t)nbx * nby));
+  const int ci0 = J.lo[0] + bx * cb, cj0 = J.lo[1] + by * cb, ck0 = J.lo[2] + bz * cb;
+  const int64_t n = p.n;
+  const int64_t X0 = wrapi(llrint((double)(ci0 - p.ncb) * p.scale - J.off[0]) + p.shift, n);
+  const int64_t Y0 = wrapi(llrint((double)(cj0 - p.ncb) * p.scale - J.off[1]) + p.shift, n);
+  const int64_t Z0 = wrapi(llrint((double)(ck0 - p.ncb) * p.scale - J.off[2]) + p.shift, n);
+  for (int e = threadIdx.x; e < kAccW * kAccW * kAccX; e += kDepThreads) acc[e] = 0.f;
+  BrickRows br;
+  brick_rows(p, J, cb, ci0, cj0, ck0, rbase, rstart, rcell, br);  // its barriers cover the zeroing
+  if (br.total == 0) return;  // nothing reaches the mesh from an empty brick
+  for (int k = threadIdx.x; k < br.total; k += kDepThreads) {
+    int di, dj, dk;
+    const int64_t ip = brick_particle(k, br, rbase, rstart, rcell, di, dj, dk);
+    const int16_t *q = p.xp + 3 * ip;
+    float wx[3], wy[3], wz[3];
+    const int64_t ix = tsc(decode_pos(ci0 + di - p.ncb, q[0]) * p.scale - J.off[0], wx) + p.shift;
+    const int64_t iy = tsc(decode_pos(cj0 + dj - p.ncb, q[1]) * p.scale - J.off[1], wy) + p.shift;
+    const int64_t iz = tsc(decode_pos(ck0 + dk - p.ncb, q[2]) * p.scale - J.off[2], wz) + p.shift;
+    // window indices of the stencil's first point: x (ix - 1) - (X0 - 4), y (iy - 1) - (Y0 - 1)
+    const int lx = (int)wrap_near(ix - X0, n) + 3, ly = (int)wrap_near(iy - Y0, n), lz = (int)wrap_near(iz - Z0, n);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+#pragma unroll
+      for (int bb = 0; bb < 3; bb++) {
+        float *row = acc + ((lz + c) * kAccW + (ly + bb)) * kAccX + lx;
+        atomicAdd(row + 0, (wx[0] * wy[bb]) * wz[c]);
+        atomicAdd(row + 1, (wx[1] * wy[bb]) * wz[c]);
+        atomicAdd(row + 2, (wx[2] * wy[bb]) * wz[c]);
+      }
+    }
+  }
+  __syncthreads();
+  float *R = p.rho + (int64_t)J.slot * p.n3;
+  constexpr int G4 = kAccX / 4;
+  for (int e = threadIdx.x; e < kAccW * kAccW * G4; e += kDepThreads) {
+    const float4 v = reinterpret_cast<const float4 *>(acc)[e];
+    if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
+    const int xg = e % G4, y = (e / G4) % kAccW, z = e / (G4 * kAccW);
+    const int64_t gx = wrap_near(X0 - 4 + 4 * xg, n), gy = wrap_near(Y0 - 1 + y, n), gz = wrap_near(Z0 - 1 + z, n);
+    atomicAdd(reinterpret_cast<float4 *>(R + (gz * n + gy) * n + gx), v);
+  }
+}
+
+// mesh points per coarse cell when the brick kernels apply (periodic meshes, whole mesh points
+// per coarse cell dividing the brick, the deposited (dep) or gathered cells of every job a whole
+// number of bricks), else 0
+static int brick_mc(const PM3Args &a, bool dep) {
+  if (!a.wrap || a.n < 8) return 0;
+  const double mcd = a.scale;
+  const int mc = (int)llrint(mcd);
+  if (mc < 1 || (double)mc != mcd || kBrick % mc) return 0;
+  const int cb = kBrick / mc;
+  if (cb > kMaxCb) return 0;
+  for (int d = 0; d < 3; d++)
+    if ((dep ? a.rdep[d] : a.ract[d]) % cb) return 0;
+  return mc;
+}
+int pm3_brick_mc(const PM3Args &a) { return brick_mc(a, false); }
+
+// the dynamic shared-memory limit of a kernel, raised once per device (the attribute is per device)
+static void set_smem_attr_once(const void *fn, size_t bytes) {
+  constexpr int kDev = 64, kFn = 8;
+  static const void *fns[kFn] = {};
+  static bool done[kFn][kDev] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int f = 0;
+  while (f < kFn && fns[f] && fns[f] != fn) f++;
+  if (f == kFn) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return;
+  }
+  fns[f] = fn;
+  if (dev >= 0 && dev < kDev && done[f][dev]) return;
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (dev >= 0 && dev < kDev) done[f][dev] = true;
+}
+
+void launch_pm3_deposit(const PM3Args &a, cudaStream_t s) {
+  PM3K p = make_k(a);
+  const int mc = (a.n % 4 == 0) ? brick_mc(a, true) : 0;
+  if (mc) {
+    const int cb = kBrick / mc;
+    const int64_t blocks = (int64_t)(a.rdep[0] / cb) * (a.rdep[1] / cb) * (a.rdep[2] / cb) * a.njobs;
+    if (blocks > 0) k_deposit_brick<<<(unsigned)blocks, kDepThreads, 0, s>>>(p, mc);
+    return;
+  }
+  const int64_t warps = (int64_t)a.rdep[0] * a.rdep[1] * a.rdep[2] * a.njobs;
+  k_deposit<<<(unsigned)((warps + kWarps - 1) / kWarps), kWarps * 32, 0, s>>>(p);
+}
+
+bool launch_pm3_force_gather(const PM3Args &a, cudaStream_t s) {
+  const int mc = brick_mc(a, false);
+  if (!mc) return false;
+  PM3K p = make_k(a);
+  const int cb = kBrick / mc;
+  const int64_t blocks = (int64_t)(a.ract[0] / cb) * (a.ract[1] / cb) * (a.ract[2] / cb) * a.njobs;
+  set_smem_attr_once((const void *)k_force_gather, kFgSmem);
+  if (blocks > 0) k_force_gather<<<(unsigned)blocks, kFgThreads, kFgSmem, s>>>(p, mc);
+  return true;
 }
 
 void launch_pm3_gather(const PM3Args &a, cudaStream_t s) {
