@@ -788,12 +788,148 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_apply_tc(MlpApplyK p, int
     }
     tc_fence_before();  // the next tile's MMA overwrites these columns
   }
-  if (!ok && m == 0) atomicOr(err, 1 << CUBE_ERR_TIMEOUT);
+  if (!ok) {
+    // a wait gave up while this warpgroup's MMA may still run: wait once more (also bounded) for
+    // its commit before the tensor memory is released
+    if (m == 0) atomicOr(err, 1 << CUBE_ERR_TIMEOUT);
+    (void)mbar_wait(bar, phase ^ 1u);
+  }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kTcCols));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// training GEMM on the 5th-generation tensor cores: C[M][N] = A[M][K] B[N][K]^T + bias[N] with the
+// epilogue of k_gemm_nt (Z in FP32, H = act(Z) in BF16).  One warpgroup per CTA and a 128-row tile
+// of C (UMMA M = 128, one TMEM lane per row); the CTA's N columns (a multiple of 16, at most 128)
+// accumulate in TMEM.  K advances 64 at a time through two shared-memory stages: the loads of a
+// stage (cp.async, 16 bytes, into the K-major core-matrix layout) overlap the MMAs of the other,
+// whose tcgen05.commit to the stage's mbarrier frees it.  Rows of A past M and of B past N are
+// zero-filled.  K % 16 == 0, lda % 8 == 0, ldb % 8 == 0.  With gridDim.z > 1 (the weight gradients,
+// K = the batch) each CTA takes a slice of K and adds its partial sums to Z (zeroed by the caller).
+constexpr int kGtM = 128, kGtN = 128, kGtK = 64;
+constexpr size_t kGtStageA = (size_t)kGtM * kGtK * 2, kGtStageB = (size_t)kGtN * kGtK * 2;
+constexpr size_t kGtSmem = 2 * (kGtStageA + kGtStageB) + 2 * 8 + 16;
+
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void *g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+}
+
+__global__ void __launch_bounds__(kGtM, 1) k_gemm_nt_tc(const bf16 *__restrict__ A, int lda, const bf16 *__restrict__ B,
+                                                       int ldb, int M, int N, int K, const float *__restrict__ bias,
+                                                       float *Z, int ldz, bf16 *H, int ldh, int act, int32_t *err) {
+  extern __shared__ __align__(1024) unsigned char gt_smem[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(gt_smem + 2 * (kGtStageA + kGtStageB));
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int m0 = blockIdx.y * kGtM, n0 = blockIdx.x * kGtN;
+  const int nt = min(kGtN, ((N - n0 + 15) / 16) * 16);  // this CTA's columns, a multiple of 16
+  const uint32_t ncols = nt <= 32 ? 32u : (nt <= 64 ? 64u : 128u);
+  if (tid == 0) {
+    for (int b = 0; b < 2; b++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = umma_idesc(nt);
+  // this CTA's K slice, whole steps of kGtK
+  const int steps = (K + kGtK - 1) / kGtK, per = (steps + gridDim.z - 1) / gridDim.z;
+  const int kbeg = blockIdx.z * per * kGtK, kend = min(K, kbeg + per * kGtK);
+  const int nk = kend > kbeg ? (kend - kbeg + kGtK - 1) / kGtK : 0;
+  uint32_t phase[2] = {0u, 0u};
+  bool ok = true;
+  int pending = 0;  // stages with an MMA not yet waited for (bit per stage)
+  for (int ks = 0; ks < nk && ok; ks++) {
+    const int st = ks & 1;
+    unsigned char *sa = gt_smem + st * (kGtStageA + kGtStageB), *sb = sa + kGtStageA;
+    if (pending & (1 << st)) {  // the MMA that read this stage two steps ago
+      ok = mbar_wait(smem_u32(&bars[st]), phase[st]);
+      phase[st] ^= 1u;
+      pending &= ~(1 << st);
+      ok = __syncthreads_and(ok);
+      if (!ok) break;
+    }
+    const int k0 = kbeg + ks * kGtK, kc = min(kGtK, kend - k0);  // kc: a multiple of 16
+    // A: 128 rows x kc / 8 chunks; B: nt rows x kc / 8 chunks
+    for (int i = tid; i < kGtM * (kc / 8); i += kGtM) {
+      const int r = i / (kc / 8), c = i % (kc / 8);
+      const uint32_t dst = smem_u32(sa + umma_off(r, 8 * c, kGtM));
+      if (m0 + r < M) cp_async16(dst, A + (int64_t)(m0 + r) * lda + k0 + 8 * c);
+      else *reinterpret_cast<uint4 *>(sa + umma_off(r, 8 * c, kGtM)) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    for (int i = tid; i < nt * (kc / 8); i += kGtM) {
+      const int r = i / (kc / 8), c = i % (kc / 8);
+      const uint32_t dst = smem_u32(sb + umma_off(r, 8 * c, nt));
+      if (n0 + r < N) cp_async16(dst, B + (int64_t)(n0 + r) * ldb + k0 + 8 * c);
+      else *reinterpret_cast<uint4 *>(sb + umma_off(r, 8 * c, nt)) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t lbo_a = (kGtM / 8) * 128, lbo_b = (uint32_t)(nt / 8) * 128;
+      const uint32_t a_base = smem_u32(sa), b_base = smem_u32(sb);
+      for (int s16 = 0; s16 < kc / 16; s16++) {
+        const uint64_t ad = umma_desc(a_base + 2 * s16 * lbo_a, lbo_a, 128);
+        const uint64_t bd = umma_desc(b_base + 2 * s16 * lbo_b, lbo_b, 128);
+        umma_bf16(tmem, ad, bd, idesc, (ks > 0 || s16 > 0) ? 1u : 0u);
+      }
+      umma_commit(smem_u32(&bars[st]));
+    }
+    pending |= 1 << st;
+  }
+  // the last MMAs
+  for (int st = 0; st < 2; st++)
+    if (pending & (1 << st)) {
+      const bool w = mbar_wait(smem_u32(&bars[st]), phase[st]);
+      ok = ok && w;
+    }
+  ok = __syncthreads_and(ok);
+  tc_fence_after();
+  if (ok && nk > 0) {
+    // epilogue: thread = row m0 + tid (TMEM lane), 16 columns at a time
+    const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+    const int r = m0 + tid;
+    const bool split = gridDim.z > 1;
+    for (int c0 = 0; c0 < nt; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + lane_base + (uint32_t)c0, v);
+      if (r < M) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const int c = n0 + c0 + j;
+          if (c >= N) continue;
+          if (split) {
+            atomicAdd(Z + (int64_t)r * ldz + c, v[j]);
+            continue;
+          }
+          const float z = v[j] + (bias ? bias[c] : 0.f);
+          if (Z) Z[(int64_t)r * ldz + c] = z;
+          if (H) H[(int64_t)r * ldh + c] = __float2bfloat16_rn(act ? gelu_f(z) : z);
+        }
+      }
+    }
+  } else if (!ok && tid == 0) {
+    atomicOr(err, 1 << CUBE_ERR_TIMEOUT);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
   }
 }
 
@@ -833,8 +969,28 @@ void launch_mlp_features(const float4 *pos, int64_t n, const float *rho, int ng,
   k_mlp_features<<<148 * 8, 256, 0, s>>>(pos, n, rho, ng, X);
 }
 
+// The training GEMMs run on tcgen05 (k_gemm_nt_tc); CUBE_MLP_MMA_SYNC selects the mma.sync
+// kernel instead (kept as an independent cross-check).
+static int32_t *g_gemm_err = nullptr;  // status word of the current training call (MlpParams::err)
+
 void launch_gemm_nt(const bf16 *A, int lda, const bf16 *B, int ldb, int M, int N, int K, const float *bias, float *Z,
                     int ldz, bf16 *H, int ldh, int act, cudaStream_t s) {
+  if (!getenv("CUBE_MLP_MMA_SYNC") && g_gemm_err) {
+    static int attr_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (attr_dev != dev) {
+      cudaFuncSetAttribute(k_gemm_nt_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGtSmem);
+      attr_dev = dev;
+    }
+    // long K (the weight gradients sum over the batch) on few output tiles: split K over CTAs
+    int split = 1;
+    if (Z && !H && !bias && !act && M <= 2 * kGtM && K >= 4 * kGtK) split = std::min(32, K / (4 * kGtK));
+    if (split > 1) cudaMemset2DAsync(Z, sizeof(float) * (size_t)ldz, 0, sizeof(float) * (size_t)N, (size_t)M, s);
+    dim3 grid((unsigned)((N + kGtN - 1) / kGtN), (unsigned)((M + kGtM - 1) / kGtM), (unsigned)split);
+    k_gemm_nt_tc<<<grid, kGtM, kGtSmem, s>>>(A, lda, B, ldb, M, N, K, bias, Z, ldz, H, ldh, act, g_gemm_err);
+    return;
+  }
   dim3 grid((unsigned)((N + kGT - 1) / kGT), (unsigned)((M + kGT - 1) / kGT));
   k_gemm_nt<<<grid, 128, 0, s>>>(A, lda, B, ldb, M, N, K, bias, Z, ldz, H, ldh, act);
 }
@@ -859,6 +1015,7 @@ void launch_mlp_apply(const MlpParams &m, const float4 *pos, const float *rho, i
 int mlp_train_step(MlpParams &m, const bf16 *X, const float *T, const int32_t *rows, int batch, float lr,
                    float *loss, cudaStream_t s) {
   if (batch <= 0 || batch > m.cap || batch % 16) return CUBE_ERR_INVALID;
+  g_gemm_err = m.err;
   const int B = batch, W = kMlpW, OP = kMlpOutPad;
   const int g1 = 148 * 8;
   k_mlp_gather<<<g1, 256, 0, s>>>(X, T, rows, B, m.xb, m.tb);
@@ -904,6 +1061,7 @@ int mlp_train_step(MlpParams &m, const bf16 *X, const float *T, const int32_t *r
 
 // Y[rows][3] of X through the training GEMM path (no kick): for checks against the oracle
 int mlp_forward(MlpParams &m, const bf16 *X, int64_t nrows, float *Y, cudaStream_t s) {
+  g_gemm_err = m.err;
   const int W = kMlpW, OP = kMlpOutPad;
   cudaMemsetAsync(m.b4pad, 0, sizeof(float) * OP, s);
   cudaMemcpyAsync(m.b4pad, m.master + mlp_boff(3), sizeof(float) * kMlpOut, cudaMemcpyDeviceToDevice, s);
