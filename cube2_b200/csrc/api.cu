@@ -511,6 +511,8 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     a.vp = d.vp;
     a.out = (float *)g.out.p;
     a.want_vmax = want_vmax;
+    a.err = (int32_t *)g.counters.p + 2;
+    a.num_sms = g.num_sms;
     // the force difference is fused into the gather brick by brick where the geometry allows;
     // otherwise the three force arrays are written and gathered from
     const bool fused = pm3_brick_mc(a) > 0;
@@ -959,6 +961,7 @@ static int finish_times(bool do_pm3, bool do_pp) {
 static int check_err_word(int32_t w) {
   if (!w) return CUBE_OK;
   if (w & (1 << CUBE_ERR_CAPACITY)) return fail(CUBE_ERR_CAPACITY);
+  if (w & (1 << CUBE_ERR_TIMEOUT)) return fail(CUBE_ERR_TIMEOUT);
   return fail(CUBE_ERR_INVALID);
 }
 

@@ -196,6 +196,8 @@ struct PM3Args {
   float *vp;
   float *out;
   int want_vmax;
+  int32_t *err = nullptr;  // device status word (bit CUBE_ERR_TIMEOUT from a bounded wait), may be null
+  int num_sms = 148;
 };
 void launch_pm3_deposit(const PM3Args &a, cudaStream_t s);
 void launch_pm3_kspace(const PM3Args &a, cudaStream_t s);

@@ -15,6 +15,7 @@
 //            points (kick.f90:494) in the same pass;
 //   gather   TSC gather of the force at each active particle and the kick
 //            vp += dv * a_mid*dt/(6 pi) (kick.f90:497-540).
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -43,6 +44,7 @@ struct PM3K {
   int want_vmax;
   int fphys_lo, fphys_n;
   int nslots;
+  int32_t *err;
 };
 
 // a + d into [0, n) for |d| < n
@@ -341,18 +343,14 @@ __global__ void __launch_bounds__(kWarps * 32, 4) k_gather(PM3K p) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Brick kernels for the periodic meshes (wrap = 1): one block per brick of kBrick^3 mesh points,
-// i.e. (kBrick / mc)^3 coarse cells of one job, mc = mesh points per coarse cell.  The bricks of
-// a job tile its active cells, and those of all jobs tile the mesh once.  A brick's particles
-// lie in (kBrick / mc)^2 rows of (kBrick / mc) coarse cells, and every row is one contiguous run
-// of storage, so the block walks them as one flat list.
+// Brick kernels for the periodic meshes (wrap = 1): a brick is kBrick^3 mesh points, i.e.
+// (kBrick / mc)^3 coarse cells of one job, mc = mesh points per coarse cell.  The bricks of a job
+// tile its active cells, and those of all jobs tile the mesh once.  A brick's particles lie in
+// (kBrick / mc)^2 rows of (kBrick / mc) coarse cells, and every row is one contiguous run of
+// storage, so a block walks them as one flat list.
 constexpr int kBrick = 16;               // owned mesh points per brick side
-constexpr int kFgThreads = 256;
-constexpr int kPotW = kBrick + 6;        // potential window: owned -3 .. +3 (4-point difference of TSC points)
-constexpr int kForW = kBrick + 2;        // force window: owned -1 .. +1 (the TSC stencil)
 constexpr int kMaxCb = 4;                // coarse cells per brick side (mc >= 4)
 constexpr int kMaxRowsPerBrick = kMaxCb * kMaxCb;
-constexpr size_t kFgSmem = sizeof(float) * ((size_t)kPotW * kPotW * kPotW + 3 * (size_t)kForW * kForW * kForW);
 
 struct BrickRows {
   int nrows, total;
@@ -360,7 +358,7 @@ struct BrickRows {
 };
 
 // The brick's rows of coarse cells: first particle, count and the coarse cells' first particles
-// (relative to the row), in shared memory; returns the particle total.
+// (relative to the row), in shared memory.  Contains two block barriers.
 __device__ __forceinline__ void brick_rows(const PM3K &p, const MeshJob &J, int cb, int ci0, int cj0, int ck0,
                                           int64_t *rbase, int *rstart, int *rcell, BrickRows &br) {
   const int nrows = cb * cb;
@@ -409,98 +407,230 @@ __device__ __forceinline__ int64_t brick_particle(int k, const BrickRows &br, co
   return rbase[lo] + l;
 }
 
-// Force and gather in one pass: the potential of the brick plus three points on every side is
-// read once (coalesced rows, periodic indices) into shared memory; the 4-point difference of
-// potential_to_force (kick.f90:545-568) gives the three force components on the brick plus one
-// point on every side, also in shared memory, and max |F|^2 of the owned points (kick.f90:494);
-// then every active particle of the brick gathers its 27 TSC points from there and is kicked
-// (kick.f90:497-540).  The force arrays never reach HBM.  The arithmetic (weights, products,
-// summation order) is the one of k_force_zm followed by k_gather.
-__global__ void __launch_bounds__(kFgThreads, 2) k_force_gather(PM3K p, int mc) {
-  extern __shared__ float fg_smem[];
-  float *pot = fg_smem;                                 // [z][y][x] kPotW^3
-  float *fw = pot + kPotW * kPotW * kPotW;              // [3][z][y][x] kForW^3
+// brick b of the launch -> job, first coarse cell, first owned mesh point (exact: the offsets of
+// periodic jobs are whole mesh points, and the owned points start on a multiple of kBrick)
+struct BrickPos {
+  int j, ci0, cj0, ck0;
+  int64_t X0, Y0, Z0;
+};
+__device__ __forceinline__ BrickPos brick_pos(const PM3K &p, int64_t b, int cb, const int *ext, const int *lo_of) {
+  const int nbx = ext[0] / cb, nby = ext[1] / cb, nbz = ext[2] / cb;
+  const int64_t per_job = (int64_t)nbx * nby * nbz;
+  BrickPos q;
+  q.j = (int)(b / per_job);
+  const int64_t r = b - (int64_t)q.j * per_job;
+  const MeshJob &J = p.jobs[q.j];
+  const int lo[3] = {lo_of == nullptr ? J.alo[0] : J.lo[0], lo_of == nullptr ? J.alo[1] : J.lo[1],
+                     lo_of == nullptr ? J.alo[2] : J.lo[2]};
+  q.ci0 = lo[0] + (int)(r % nbx) * cb;
+  q.cj0 = lo[1] + (int)((r / nbx) % nby) * cb;
+  q.ck0 = lo[2] + (int)(r / ((int64_t)nbx * nby)) * cb;
+  const int64_t n = p.n;
+  q.X0 = wrapi(llrint((double)(q.ci0 - p.ncb) * p.scale - J.off[0]) + p.shift, n);
+  q.Y0 = wrapi(llrint((double)(q.cj0 - p.ncb) * p.scale - J.off[1]) + p.shift, n);
+  q.Z0 = wrapi(llrint((double)(q.ck0 - p.ncb) * p.scale - J.off[2]) + p.shift, n);
+  return q;
+}
+
+// ---- mbarrier and bulk-copy helpers (sm_90+) ----
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ unsigned long long ns_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+constexpr unsigned long long kBulkWaitNs = 1000000000ull;  // bound of one wait for a brick's copies: 1 s
+// wait for a phase of the mbarrier, at most kBulkWaitNs; false when the wait gave up
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  const unsigned long long t0 = ns_now();
+  while (!mbar_try_wait(bar, parity))
+    if (ns_now() - t0 > kBulkWaitNs) return false;
+  return true;
+}
+// bulk asynchronous copy global -> this CTA's shared memory, completing on the mbarrier
+// (both addresses 16-byte aligned, bytes a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+// Force and gather in one pass, persistent: each block walks bricks b = blockIdx.x + k gridDim.x.
+// A brick's potential window (the brick plus three points on every side; along x widened to
+// whole 16-byte groups, owned - 4 .. owned + kBrick + 3) arrives by bulk asynchronous copies,
+// one per row (two where the row wraps around the periodic mesh), into one of two shared
+// buffers: the next brick's window streams in while this brick is computed.  The 4-point
+// difference of potential_to_force (kick.f90:545-568) gives the three force components on the
+// brick plus one point on every side, in shared memory, and max |F|^2 of the owned points
+// (kick.f90:494); every active particle of the brick then gathers its 27 TSC points from there
+// and is kicked (kick.f90:497-540).  The force arrays never reach HBM.  The arithmetic (weights,
+// products, summation order) is the one of k_force_zm followed by k_gather.
+constexpr int kFgThreads = 512;
+constexpr int kPotX = kBrick + 8, kPotW = kBrick + 6;  // potential window: x 24, y and z 22
+constexpr int kForW = kBrick + 2;                      // force window 18^3
+constexpr int kPotElems = kPotW * kPotW * kPotX;
+constexpr uint32_t kPotBytes = sizeof(float) * kPotElems;
+constexpr int kFor3 = kForW * kForW * kForW;
+constexpr size_t kFgSmem = 2 * (size_t)kPotBytes + sizeof(float) * 3 * (size_t)kFor3;
+
+__global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, int64_t nbricks) {
+  extern __shared__ __align__(128) float fg_smem[];
+  float *pot0 = fg_smem;                    // [2][z 22][y 22][x 24]
+  float *fw = fg_smem + 2 * kPotElems;      // [3][z][y][x] 18^3
+  __shared__ __align__(8) uint64_t bars[2];
   __shared__ int64_t rbase[kMaxRowsPerBrick];
   __shared__ int rstart[kMaxRowsPerBrick + 1];
   __shared__ int rcell[kMaxRowsPerBrick * (kMaxCb + 1)];
   __shared__ float red[4][kFgThreads / 32];
+  __shared__ int s_fail;
+  const int tid = threadIdx.x;
   const int cb = kBrick / mc;
-  const int nbx = p.ract[0] / cb, nby = p.ract[1] / cb, nbz = p.ract[2] / cb;
-  const int64_t per_job = (int64_t)nbx * nby * nbz;
-  const int j = (int)(blockIdx.x / per_job);
-  const int64_t b = blockIdx.x - (int64_t)j * per_job;
-  const MeshJob J = p.jobs[j];
-  const int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((int64_t)nbx * nby));
-  const int ci0 = J.alo[0] + bx * cb, cj0 = J.alo[1] + by * cb, ck0 = J.alo[2] + bz * cb;
   const int64_t n = p.n, n3 = p.n3;
-  // first owned mesh point (exact: the offsets of periodic jobs are whole mesh points)
-  const int64_t X0 = wrapi(llrint((double)(ci0 - p.ncb) * p.scale - J.off[0]) + p.shift, n);
-  const int64_t Y0 = wrapi(llrint((double)(cj0 - p.ncb) * p.scale - J.off[1]) + p.shift, n);
-  const int64_t Z0 = wrapi(llrint((double)(ck0 - p.ncb) * p.scale - J.off[2]) + p.shift, n);
-  const float *phi = p.rho + (int64_t)J.slot * n3;
-  // potential window, owned - 3 .. owned + kBrick + 2 on every axis
-  for (int e = threadIdx.x; e < kPotW * kPotW * kPotW; e += kFgThreads) {
-    const int x = e % kPotW, y = (e / kPotW) % kPotW, z = e / (kPotW * kPotW);
-    const int64_t gx = wrap_near(X0 - 3 + x, n), gy = wrap_near(Y0 - 3 + y, n), gz = wrap_near(Z0 - 3 + z, n);
-    pot[e] = __ldg(phi + (gz * n + gy) * n + gx);
-  }
-  BrickRows br;
-  brick_rows(p, J, cb, ci0, cj0, ck0, rbase, rstart, rcell, br);  // its barriers cover the window too
-  const FDW w;
-  float m = 0.f;
-  constexpr int P2 = kPotW * kPotW;
-  for (int e = threadIdx.x; e < kForW * kForW * kForW; e += kFgThreads) {
-    const int x = e % kForW, y = (e / kForW) % kForW, z = e / (kForW * kForW);
-    const int c = (z + 2) * P2 + (y + 2) * kPotW + (x + 2);  // the point in the potential window
-    const float fx = w(pot[c - 2], pot[c - 1], pot[c + 1], pot[c + 2]);
-    const float fy = w(pot[c - 2 * kPotW], pot[c - kPotW], pot[c + kPotW], pot[c + 2 * kPotW]);
-    const float fz = w(pot[c - 2 * P2], pot[c - P2], pot[c + P2], pot[c + 2 * P2]);
-    fw[e] = fx;
-    fw[kForW * kForW * kForW + e] = fy;
-    fw[2 * kForW * kForW * kForW + e] = fz;
-    if (x >= 1 && x <= kBrick && y >= 1 && y <= kBrick && z >= 1 && z <= kBrick)
-      m = fmaxf(m, fx * fx + fy * fy + fz * fz);
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
   }
   __syncthreads();
-  // gather and kick
-  float vm0 = 0.f, vm1 = 0.f, vm2 = 0.f;
-  constexpr int F3 = kForW * kForW * kForW;
-  for (int k = threadIdx.x; k < br.total; k += kFgThreads) {
-    int di, dj, dk;
-    const int64_t ip = brick_particle(k, br, rbase, rstart, rcell, di, dj, dk);
-    const int16_t *q = p.xp + 3 * ip;
-    float wx[3], wy[3], wz[3];
-    // window coordinates: the TSC point floor(coord) lies at owned index floor(coord) - X0
-    const int64_t ix = tsc(decode_pos(ci0 + di - p.ncb, q[0]) * p.scale - J.off[0], wx) + p.shift;
-    const int64_t iy = tsc(decode_pos(cj0 + dj - p.ncb, q[1]) * p.scale - J.off[1], wy) + p.shift;
-    const int64_t iz = tsc(decode_pos(ck0 + dk - p.ncb, q[2]) * p.scale - J.off[2], wz) + p.shift;
-    const int lx = (int)wrap_near(ix - X0, n), ly = (int)wrap_near(iy - Y0, n), lz = (int)wrap_near(iz - Z0, n);
-    float d0 = 0.f, d1 = 0.f, d2 = 0.f;
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-#pragma unroll
-      for (int bb = 0; bb < 3; bb++) {
-        const int row = ((lz + c) * kForW + (ly + bb)) * kForW + lx;
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-          const float wt = (wx[a] * wy[bb]) * wz[c];
-          d0 += fw[row + a] * wt;
-          d1 += fw[F3 + row + a] * wt;
-          d2 += fw[2 * F3 + row + a] * wt;
-        }
+  // the copies of brick b's potential window into buffer `buf`: row t (z, y) = (t / 22, t % 22)
+  auto issue = [&](int64_t b, int buf) {
+    const BrickPos q = brick_pos(p, b, cb, p.ract, nullptr);
+    const float *phi = p.rho + (int64_t)p.jobs[q.j].slot * n3;
+    float *dst0 = pot0 + buf * kPotElems;
+    if (tid < kPotW * kPotW) {
+      const int z = tid / kPotW, y = tid % kPotW;
+      const int64_t gz = wrap_near(q.Z0 - 3 + z, n), gy = wrap_near(q.Y0 - 3 + y, n);
+      const float *row = phi + (gz * n + gy) * n;
+      float *dst = dst0 + (z * kPotW + y) * kPotX;
+      const int64_t xs = q.X0 - 4;  // a multiple of 4, as n: the pieces stay 16-byte aligned
+      if (xs < 0) {
+        bulk_g2s(dst, row + n + xs, (uint32_t)(-xs * 4), &bars[buf]);
+        bulk_g2s(dst - xs, row, (uint32_t)((kPotX + xs) * 4), &bars[buf]);
+      } else if (xs + kPotX > n) {
+        bulk_g2s(dst, row + xs, (uint32_t)((n - xs) * 4), &bars[buf]);
+        bulk_g2s(dst + (n - xs), row, (uint32_t)((xs + kPotX - n) * 4), &bars[buf]);
+      } else {
+        bulk_g2s(dst, row + xs, kPotBytes / (kPotW * kPotW), &bars[buf]);
       }
     }
-    float *v = p.vp + 3 * ip;
-    const float v0 = v[0] + d0 * p.kick, v1 = v[1] + d1 * p.kick, v2 = v[2] + d2 * p.kick;
-    v[0] = v0;
-    v[1] = v1;
-    v[2] = v2;
-    vm0 = fmaxf(vm0, fabsf(v0));
-    vm1 = fmaxf(vm1, fabsf(v1));
-    vm2 = fmaxf(vm2, fabsf(v2));
+  };
+  // first brick: expect its bytes, then copy
+  int64_t b = blockIdx.x;
+  if (b < nbricks) {
+    if (tid == 0) mbar_expect_tx(&bars[0], kPotBytes);
+    __syncthreads();
+    issue(b, 0);
+    if (tid == 0) mbar_arrive(&bars[0]);
+  }
+  const FDW w;
+  float m = 0.f, vm0 = 0.f, vm1 = 0.f, vm2 = 0.f;
+  int fail_k = -1;         // the iteration whose wait gave up
+  bool fail_next = false;  // ... and whether it had issued the next brick's copies
+  for (int k = 0; b < nbricks; k++, b += gridDim.x) {
+    const int cur = k & 1, nxt = cur ^ 1;
+    const int64_t bn = b + gridDim.x;
+    const BrickPos q = brick_pos(p, b, cb, p.ract, nullptr);
+    const MeshJob &J = p.jobs[q.j];
+    if (tid == 0 && bn < nbricks) mbar_expect_tx(&bars[nxt], kPotBytes);
+    BrickRows br;
+    brick_rows(p, J, cb, q.ci0, q.cj0, q.ck0, rbase, rstart, rcell, br);  // two barriers
+    if (bn < nbricks) {
+      // buffer nxt was last read for brick k - 1, before the barriers above
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(bn, nxt);
+      if (tid == 0) mbar_arrive(&bars[nxt]);
+    }
+    if (!mbar_wait_bounded(&bars[cur], (uint32_t)(k >> 1) & 1u)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) {
+      fail_k = k;
+      fail_next = bn < nbricks;
+      break;
+    }
+    const float *pot = pot0 + cur * kPotElems;
+    // force window: point (x, y, z) is mesh point (X0 - 1 + x, ...), potential (x + 3, y + 2, z + 2)
+    constexpr int PY = kPotX, PZ = kPotX * kPotW;
+    for (int e = tid; e < kFor3; e += kFgThreads) {
+      const int x = e % kForW, y = (e / kForW) % kForW, z = e / (kForW * kForW);
+      const int c = (z + 2) * PZ + (y + 2) * PY + (x + 3);
+      const float fx = w(pot[c - 2], pot[c - 1], pot[c + 1], pot[c + 2]);
+      const float fy = w(pot[c - 2 * PY], pot[c - PY], pot[c + PY], pot[c + 2 * PY]);
+      const float fz = w(pot[c - 2 * PZ], pot[c - PZ], pot[c + PZ], pot[c + 2 * PZ]);
+      fw[e] = fx;
+      fw[kFor3 + e] = fy;
+      fw[2 * kFor3 + e] = fz;
+      if (x >= 1 && x <= kBrick && y >= 1 && y <= kBrick && z >= 1 && z <= kBrick)
+        m = fmaxf(m, fx * fx + fy * fy + fz * fz);
+    }
+    __syncthreads();
+    for (int kk = tid; kk < br.total; kk += kFgThreads) {
+      int di, dj, dk;
+      const int64_t ip = brick_particle(kk, br, rbase, rstart, rcell, di, dj, dk);
+      const int16_t *qp = p.xp + 3 * ip;
+      float wx[3], wy[3], wz[3];
+      const int64_t ix = tsc(decode_pos(q.ci0 + di - p.ncb, qp[0]) * p.scale - J.off[0], wx) + p.shift;
+      const int64_t iy = tsc(decode_pos(q.cj0 + dj - p.ncb, qp[1]) * p.scale - J.off[1], wy) + p.shift;
+      const int64_t iz = tsc(decode_pos(q.ck0 + dk - p.ncb, qp[2]) * p.scale - J.off[2], wz) + p.shift;
+      // the stencil's first point ix - 1 lies at force-window index ix - X0
+      const int lx = (int)wrap_near(ix - q.X0, n), ly = (int)wrap_near(iy - q.Y0, n), lz = (int)wrap_near(iz - q.Z0, n);
+      float d0 = 0.f, d1 = 0.f, d2 = 0.f;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+#pragma unroll
+        for (int bb = 0; bb < 3; bb++) {
+          const int row = ((lz + c) * kForW + (ly + bb)) * kForW + lx;
+#pragma unroll
+          for (int a = 0; a < 3; a++) {
+            const float wt = (wx[a] * wy[bb]) * wz[c];
+            d0 += fw[row + a] * wt;
+            d1 += fw[kFor3 + row + a] * wt;
+            d2 += fw[2 * kFor3 + row + a] * wt;
+          }
+        }
+      }
+      float *v = p.vp + 3 * ip;
+      const float v0 = v[0] + d0 * p.kick, v1 = v[1] + d1 * p.kick, v2 = v[2] + d2 * p.kick;
+      v[0] = v0;
+      v[1] = v1;
+      v[2] = v2;
+      vm0 = fmaxf(vm0, fabsf(v0));
+      vm1 = fmaxf(vm1, fabsf(v1));
+      vm2 = fmaxf(vm2, fabsf(v2));
+    }
+    __syncthreads();  // the force window, the row tables and buffer cur are reused
+  }
+  if (fail_k >= 0) {
+    // a wait gave up: record it, and wait once more (also bounded) for the copies in flight
+    // before the block's shared memory is released
+    if (tid == 0 && p.err) atomicOr(p.err, 1 << CUBE_ERR_TIMEOUT);
+    (void)mbar_wait_bounded(&bars[fail_k & 1], (uint32_t)(fail_k >> 1) & 1u);
+    if (fail_next) (void)mbar_wait_bounded(&bars[(fail_k + 1) & 1], (uint32_t)((fail_k + 1) >> 1) & 1u);
   }
   // one update of each maximum per block
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = tid >> 5, lane = tid & 31;
   m = warp_max(m);
   vm0 = warp_max(vm0);
   vm1 = warp_max(vm1);
@@ -512,11 +642,11 @@ __global__ void __launch_bounds__(kFgThreads, 2) k_force_gather(PM3K p, int mc) 
     red[3][warp] = vm2;
   }
   __syncthreads();
-  if (threadIdx.x < 4) {
+  if (tid < 4) {
     float r = 0.f;
-    for (int q = 0; q < kFgThreads / 32; q++) r = fmaxf(r, red[threadIdx.x][q]);
-    if (threadIdx.x == 0) atomic_max_nonneg(&p.out[0], r);
-    else if (p.want_vmax) atomic_max_nonneg(&p.out[1 + threadIdx.x], r);
+    for (int qq = 0; qq < kFgThreads / 32; qq++) r = fmaxf(r, red[tid][qq]);
+    if (tid == 0) atomic_max_nonneg(&p.out[0], r);
+    else if (p.want_vmax) atomic_max_nonneg(&p.out[1 + tid], r);
   }
 }
 
@@ -553,6 +683,7 @@ static PM3K make_k(const PM3Args &a) {
   p.fphys_lo = a.fphys_lo;
   p.fphys_n = a.fphys_n;
   p.nslots = a.nslots;
+  p.err = a.err;
   return p;
 }
 
@@ -575,65 +706,69 @@ void launch_pm3_force(const PM3Args &a, cudaStream_t s) {
 
 // Deposit brick by brick: the TSC weights of the brick's particles accumulate in a shared-memory
 // window (the brick plus one point on every side, widened to whole 16-byte groups along x) with
-// shared atomics; the window then goes to the mesh with one 16-byte vector reduction per group
-// of four points that received anything.  Every mesh point thus takes at most one global
-// reduction per brick that reaches it, instead of one per particle (kick.f90:420-468 sums the
-// same weights; the order of the float additions differs).
+// native 32-bit integer shared atomics on fixed-point weights, w * 2^e rounded to an integer; e
+// is chosen per brick from its particle count so that no window point can overflow 2^32
+// (a point takes at most 0.75^3 of each particle).  The window then goes to the mesh as floats,
+// one 16-byte vector reduction per group of four points that received anything: every mesh point
+// takes at most one global reduction per brick that reaches it, instead of one per particle.
+// kick.f90:420-468 sums the same weights; the integer sums make the brick's part exact and
+// independent of the order of the atomics (the rounding of a weight to 2^-e, e >= 15 for
+// bricks of up to 10^5 particles, is far below the FP32 rounding of the density).
 constexpr int kDepThreads = 256;
 constexpr int kAccX = kBrick + 8;  // x window owned - 4 .. owned + kBrick + 3: whole float4 groups
 constexpr int kAccW = kBrick + 2;  // y, z window owned - 1 .. owned + kBrick
 
 __global__ void __launch_bounds__(kDepThreads) k_deposit_brick(PM3K p, int mc) {
-  __shared__ __align__(16) float acc[kAccW * kAccW * kAccX];
+  __shared__ __align__(16) unsigned acc[kAccW * kAccW * kAccX];
   __shared__ int64_t rbase[kMaxRowsPerBrick];
   __shared__ int rstart[kMaxRowsPerBrick + 1];
   __shared__ int rcell[kMaxRowsPerBrick * (kMaxCb + 1)];
   const int cb = kBrick / mc;
-  const int nbx = p.rdep[0] / cb, nby = p.rdep[1] / cb, nbz = p.rdep[2] / cb;
-  const int64_t per_job = (int64_t)nbx * nby * nbz;
-  const int j = (int)(blockIdx.x / per_job);
-  const int64_t b = blockIdx.x - (int64_t)j * per_job;
-  const MeshJob J = p.jobs[j];
-  const int bx = (int)(b % nbx), by = (int)((b / nbx) % nby), bz = (int)(b / ((int64_t)nbx * nby));
-  const int ci0 = J.lo[0] + bx * cb, cj0 = J.lo[1] + by * cb, ck0 = J.lo[2] + bz * cb;
+  const BrickPos q = brick_pos(p, blockIdx.x, cb, p.rdep, p.rdep);
+  const MeshJob &J = p.jobs[q.j];
   const int64_t n = p.n;
-  const int64_t X0 = wrapi(llrint((double)(ci0 - p.ncb) * p.scale - J.off[0]) + p.shift, n);
-  const int64_t Y0 = wrapi(llrint((double)(cj0 - p.ncb) * p.scale - J.off[1]) + p.shift, n);
-  const int64_t Z0 = wrapi(llrint((double)(ck0 - p.ncb) * p.scale - J.off[2]) + p.shift, n);
-  for (int e = threadIdx.x; e < kAccW * kAccW * kAccX; e += kDepThreads) acc[e] = 0.f;
+  for (int e = threadIdx.x; e < kAccW * kAccW * kAccX; e += kDepThreads) acc[e] = 0u;
   BrickRows br;
-  brick_rows(p, J, cb, ci0, cj0, ck0, rbase, rstart, rcell, br);  // its barriers cover the zeroing
+  brick_rows(p, J, cb, q.ci0, q.cj0, q.ck0, rbase, rstart, rcell, br);  // its barriers cover the zeroing
   if (br.total == 0) return;  // nothing reaches the mesh from an empty brick
+  // fixed-point scale 2^e: total * 0.4219 * 2^e < 2^32
+  int e = 24;
+  while (e > 1 && (double)br.total * 0.421875 * (double)(1u << e) >= 4294967040.0) e--;
+  const float fs = (float)(1u << e), inv = 1.0f / fs;
   for (int k = threadIdx.x; k < br.total; k += kDepThreads) {
     int di, dj, dk;
     const int64_t ip = brick_particle(k, br, rbase, rstart, rcell, di, dj, dk);
-    const int16_t *q = p.xp + 3 * ip;
+    const int16_t *qp = p.xp + 3 * ip;
     float wx[3], wy[3], wz[3];
-    const int64_t ix = tsc(decode_pos(ci0 + di - p.ncb, q[0]) * p.scale - J.off[0], wx) + p.shift;
-    const int64_t iy = tsc(decode_pos(cj0 + dj - p.ncb, q[1]) * p.scale - J.off[1], wy) + p.shift;
-    const int64_t iz = tsc(decode_pos(ck0 + dk - p.ncb, q[2]) * p.scale - J.off[2], wz) + p.shift;
+    const int64_t ix = tsc(decode_pos(q.ci0 + di - p.ncb, qp[0]) * p.scale - J.off[0], wx) + p.shift;
+    const int64_t iy = tsc(decode_pos(q.cj0 + dj - p.ncb, qp[1]) * p.scale - J.off[1], wy) + p.shift;
+    const int64_t iz = tsc(decode_pos(q.ck0 + dk - p.ncb, qp[2]) * p.scale - J.off[2], wz) + p.shift;
     // window indices of the stencil's first point: x (ix - 1) - (X0 - 4), y (iy - 1) - (Y0 - 1)
-    const int lx = (int)wrap_near(ix - X0, n) + 3, ly = (int)wrap_near(iy - Y0, n), lz = (int)wrap_near(iz - Z0, n);
+    const int lx = (int)wrap_near(ix - q.X0, n) + 3, ly = (int)wrap_near(iy - q.Y0, n),
+              lz = (int)wrap_near(iz - q.Z0, n);
+    const float sx0 = wx[0] * fs, sx1 = wx[1] * fs, sx2 = wx[2] * fs;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
 #pragma unroll
       for (int bb = 0; bb < 3; bb++) {
-        float *row = acc + ((lz + c) * kAccW + (ly + bb)) * kAccX + lx;
-        atomicAdd(row + 0, (wx[0] * wy[bb]) * wz[c]);
-        atomicAdd(row + 1, (wx[1] * wy[bb]) * wz[c]);
-        atomicAdd(row + 2, (wx[2] * wy[bb]) * wz[c]);
+        unsigned *row = acc + ((lz + c) * kAccW + (ly + bb)) * kAccX + lx;
+        const float yz = wy[bb] * wz[c];
+        atomicAdd(row + 0, __float2uint_rn(sx0 * yz));
+        atomicAdd(row + 1, __float2uint_rn(sx1 * yz));
+        atomicAdd(row + 2, __float2uint_rn(sx2 * yz));
       }
     }
   }
   __syncthreads();
   float *R = p.rho + (int64_t)J.slot * p.n3;
   constexpr int G4 = kAccX / 4;
-  for (int e = threadIdx.x; e < kAccW * kAccW * G4; e += kDepThreads) {
-    const float4 v = reinterpret_cast<const float4 *>(acc)[e];
-    if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
-    const int xg = e % G4, y = (e / G4) % kAccW, z = e / (G4 * kAccW);
-    const int64_t gx = wrap_near(X0 - 4 + 4 * xg, n), gy = wrap_near(Y0 - 1 + y, n), gz = wrap_near(Z0 - 1 + z, n);
-    atomicAdd(reinterpret_cast<float4 *>(R + (gz * n + gy) * n + gx), v);
+  for (int e4 = threadIdx.x; e4 < kAccW * kAccW * G4; e4 += kDepThreads) {
+    const uint4 u = reinterpret_cast<const uint4 *>(acc)[e4];
+    if ((u.x | u.y | u.z | u.w) == 0u) continue;
+    const int xg = e4 % G4, y = (e4 / G4) % kAccW, z = e4 / (G4 * kAccW);
+    const int64_t gx = wrap_near(q.X0 - 4 + 4 * xg, n), gy = wrap_near(q.Y0 - 1 + y, n), gz = wrap_near(q.Z0 - 1 + z, n);
+    atomicAdd(reinterpret_cast<float4 *>(R + (gz * n + gy) * n + gx),
+              make_float4((float)u.x * inv, (float)u.y * inv, (float)u.z * inv, (float)u.w * inv));
   }
 }
 
@@ -690,9 +825,10 @@ bool launch_pm3_force_gather(const PM3Args &a, cudaStream_t s) {
   if (!mc) return false;
   PM3K p = make_k(a);
   const int cb = kBrick / mc;
-  const int64_t blocks = (int64_t)(a.ract[0] / cb) * (a.ract[1] / cb) * (a.ract[2] / cb) * a.njobs;
+  const int64_t nbricks = (int64_t)(a.ract[0] / cb) * (a.ract[1] / cb) * (a.ract[2] / cb) * a.njobs;
   set_smem_attr_once((const void *)k_force_gather, kFgSmem);
-  if (blocks > 0) k_force_gather<<<(unsigned)blocks, kFgThreads, kFgSmem, s>>>(p, mc);
+  const int64_t grid = std::min<int64_t>(nbricks, a.num_sms > 0 ? a.num_sms : 148);
+  if (grid > 0) k_force_gather<<<(unsigned)grid, kFgThreads, kFgSmem, s>>>(p, mc, nbricks);
   return true;
 }
 
