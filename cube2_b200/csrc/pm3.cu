@@ -481,13 +481,14 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 // A brick's potential window (the brick plus three points on every side; along x widened to
 // whole 16-byte groups, owned - 4 .. owned + kBrick + 3) arrives by bulk asynchronous copies,
 // one per row (two where the row wraps around the periodic mesh), into one of two shared
-// buffers: the next brick's window streams in while this brick is computed.  The 4-point
-// difference of potential_to_force (kick.f90:545-568) gives the three force components on the
-// brick plus one point on every side, in shared memory, and max |F|^2 of the owned points
-// (kick.f90:494); every active particle of the brick then gathers its 27 TSC points from there
-// and is kicked (kick.f90:497-540).  The force arrays never reach HBM.  The arithmetic (weights,
-// products, summation order) is the one of k_force_zm followed by k_gather.
-constexpr int kFgThreads = 512;
+// buffers: the next brick's window streams in while this brick is computed.  The brick's place
+// and its row table are prepared one brick ahead by single threads.  The 4-point difference of
+// potential_to_force (kick.f90:545-568) gives the three force components on the brick plus one
+// point on every side, in shared memory, and max |F|^2 of the owned points (kick.f90:494);
+// every active particle of the brick then gathers its 27 TSC points from there and is kicked
+// (kick.f90:497-540).  The force arrays never reach HBM.  The arithmetic (weights, products,
+// summation order) is the one of k_force_zm followed by k_gather.
+constexpr int kFgThreads = 1024;
 constexpr int kPotX = kBrick + 8, kPotW = kBrick + 6;  // potential window: x 24, y and z 22
 constexpr int kForW = kBrick + 2;                      // force window 18^3
 constexpr int kPotElems = kPotW * kPotW * kPotX;
@@ -495,36 +496,72 @@ constexpr uint32_t kPotBytes = sizeof(float) * kPotElems;
 constexpr int kFor3 = kForW * kForW * kForW;
 constexpr size_t kFgSmem = 2 * (size_t)kPotBytes + sizeof(float) * 3 * (size_t)kFor3;
 
+struct BrickMeta {
+  BrickPos pos;
+  int total;
+  int64_t rbase[kMaxRowsPerBrick];
+  int rstart[kMaxRowsPerBrick + 1];
+  int rcell[kMaxRowsPerBrick * (kMaxCb + 1)];
+};
+
+// row r of brick (pos) into meta: first particle and the coarse cells' offsets (thread r)
+__device__ __forceinline__ void meta_row(const PM3K &p, int cb, BrickMeta &mt, int r) {
+  const BrickPos &q = mt.pos;
+  const int cj = q.cj0 + r % cb, ck = q.ck0 + r / cb;
+  const int64_t c0 = (((int64_t)p.jobs[q.j].t * p.nte + ck) * p.nte + cj) * p.nte + q.ci0;
+  int acc = 0;
+  for (int i = 0; i < cb; i++) {
+    mt.rcell[r * (kMaxCb + 1) + i] = acc;
+    acc += p.rhoc[c0 + i];
+  }
+  mt.rcell[r * (kMaxCb + 1) + cb] = acc;
+  mt.rbase[r] = p.cell_base[c0];
+  mt.rstart[r] = acc;  // count until meta_scan
+}
+__device__ __forceinline__ void meta_scan(BrickMeta &mt, int nrows) {
+  int acc = 0;
+  for (int r = 0; r < nrows; r++) {
+    const int c = mt.rstart[r];
+    mt.rstart[r] = acc;
+    acc += c;
+  }
+  mt.rstart[nrows] = acc;
+  mt.total = acc;
+}
+
 __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, int64_t nbricks) {
   extern __shared__ __align__(128) float fg_smem[];
   float *pot0 = fg_smem;                    // [2][z 22][y 22][x 24]
   float *fw = fg_smem + 2 * kPotElems;      // [3][z][y][x] 18^3
   __shared__ __align__(8) uint64_t bars[2];
-  __shared__ int64_t rbase[kMaxRowsPerBrick];
-  __shared__ int rstart[kMaxRowsPerBrick + 1];
-  __shared__ int rcell[kMaxRowsPerBrick * (kMaxCb + 1)];
+  __shared__ BrickMeta meta[2];
   __shared__ float red[4][kFgThreads / 32];
   __shared__ int s_fail;
   const int tid = threadIdx.x;
-  const int cb = kBrick / mc;
+  const int cb = kBrick / mc, nrows = cb * cb;
   const int64_t n = p.n, n3 = p.n3;
+  const int64_t G = gridDim.x;
+  int64_t b = blockIdx.x;
+  if (b >= nbricks) return;
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_fail = 0;
+    meta[0].pos = brick_pos(p, b, cb, p.ract, nullptr);
+    if (b + G < nbricks) meta[1].pos = brick_pos(p, b + G, cb, p.ract, nullptr);
+    mbar_expect_tx(&bars[0], kPotBytes);
   }
   __syncthreads();
-  // the copies of brick b's potential window into buffer `buf`: row t (z, y) = (t / 22, t % 22)
-  auto issue = [&](int64_t b, int buf) {
-    const BrickPos q = brick_pos(p, b, cb, p.ract, nullptr);
-    const float *phi = p.rho + (int64_t)p.jobs[q.j].slot * n3;
-    float *dst0 = pot0 + buf * kPotElems;
+  if (tid < nrows) meta_row(p, cb, meta[0], tid);
+  // the copies of a brick's potential window into buffer `buf`: row t (z, y) = (t / 22, t % 22)
+  auto issue = [&](const BrickPos &q, int buf) {
     if (tid < kPotW * kPotW) {
+      const float *phi = p.rho + (int64_t)p.jobs[q.j].slot * n3;
       const int z = tid / kPotW, y = tid % kPotW;
       const int64_t gz = wrap_near(q.Z0 - 3 + z, n), gy = wrap_near(q.Y0 - 3 + y, n);
       const float *row = phi + (gz * n + gy) * n;
-      float *dst = dst0 + (z * kPotW + y) * kPotX;
+      float *dst = pot0 + buf * kPotElems + (z * kPotW + y) * kPotX;
       const int64_t xs = q.X0 - 4;  // a multiple of 4, as n: the pieces stay 16-byte aligned
       if (xs < 0) {
         bulk_g2s(dst, row + n + xs, (uint32_t)(-xs * 4), &bars[buf]);
@@ -533,46 +570,32 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
         bulk_g2s(dst, row + xs, (uint32_t)((n - xs) * 4), &bars[buf]);
         bulk_g2s(dst + (n - xs), row, (uint32_t)((xs + kPotX - n) * 4), &bars[buf]);
       } else {
-        bulk_g2s(dst, row + xs, kPotBytes / (kPotW * kPotW), &bars[buf]);
+        bulk_g2s(dst, row + xs, sizeof(float) * kPotX, &bars[buf]);
       }
     }
   };
-  // first brick: expect its bytes, then copy
-  int64_t b = blockIdx.x;
-  if (b < nbricks) {
-    if (tid == 0) mbar_expect_tx(&bars[0], kPotBytes);
-    __syncthreads();
-    issue(b, 0);
-    if (tid == 0) mbar_arrive(&bars[0]);
-  }
+  issue(meta[0].pos, 0);
+  if (tid == 0) mbar_arrive(&bars[0]);
+  __syncthreads();
+  if (tid == 0) meta_scan(meta[0], nrows);
   const FDW w;
   float m = 0.f, vm0 = 0.f, vm1 = 0.f, vm2 = 0.f;
   int fail_k = -1;         // the iteration whose wait gave up
   bool fail_next = false;  // ... and whether it had issued the next brick's copies
-  for (int k = 0; b < nbricks; k++, b += gridDim.x) {
+  constexpr int PY = kPotX, PZ = kPotX * kPotW;
+  for (int k = 0; b < nbricks; k++, b += G) {
     const int cur = k & 1, nxt = cur ^ 1;
-    const int64_t bn = b + gridDim.x;
-    const BrickPos q = brick_pos(p, b, cb, p.ract, nullptr);
-    const MeshJob &J = p.jobs[q.j];
-    if (tid == 0 && bn < nbricks) mbar_expect_tx(&bars[nxt], kPotBytes);
-    BrickRows br;
-    brick_rows(p, J, cb, q.ci0, q.cj0, q.ck0, rbase, rstart, rcell, br);  // two barriers
-    if (bn < nbricks) {
-      // buffer nxt was last read for brick k - 1, before the barriers above
+    const bool has_next = b + G < nbricks;
+    if (tid == 0 && has_next) mbar_expect_tx(&bars[nxt], kPotBytes);
+    __syncthreads();  // (1) meta[cur] complete, buffer nxt no longer read, expect before the copies
+    if (has_next) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(bn, nxt);
+      issue(meta[nxt].pos, nxt);
       if (tid == 0) mbar_arrive(&bars[nxt]);
     }
     if (!mbar_wait_bounded(&bars[cur], (uint32_t)(k >> 1) & 1u)) s_fail = 1;
-    __syncthreads();
-    if (s_fail) {
-      fail_k = k;
-      fail_next = bn < nbricks;
-      break;
-    }
-    const float *pot = pot0 + cur * kPotElems;
     // force window: point (x, y, z) is mesh point (X0 - 1 + x, ...), potential (x + 3, y + 2, z + 2)
-    constexpr int PY = kPotX, PZ = kPotX * kPotW;
+    const float *pot = pot0 + cur * kPotElems;
     for (int e = tid; e < kFor3; e += kFgThreads) {
       const int x = e % kForW, y = (e / kForW) % kForW, z = e / (kForW * kForW);
       const int c = (z + 2) * PZ + (y + 2) * PY + (x + 3);
@@ -585,10 +608,24 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
       if (x >= 1 && x <= kBrick && y >= 1 && y <= kBrick && z >= 1 && z <= kBrick)
         m = fmaxf(m, fx * fx + fy * fy + fz * fz);
     }
-    __syncthreads();
+    if (has_next && tid < nrows) meta_row(p, cb, meta[nxt], tid);  // loads overlap the other warps' work
+    __syncthreads();  // (2) force window complete; a failed wait seen by all
+    if (s_fail) {
+      fail_k = k;
+      fail_next = has_next;
+      break;
+    }
+    if (tid == 0 && has_next) meta_scan(meta[nxt], nrows);
+    const BrickMeta &mt = meta[cur];
+    const BrickPos &q = mt.pos;
+    const MeshJob &J = p.jobs[q.j];
+    BrickRows br;
+    br.nrows = nrows;
+    br.total = mt.total;
+    br.cb = cb;
     for (int kk = tid; kk < br.total; kk += kFgThreads) {
       int di, dj, dk;
-      const int64_t ip = brick_particle(kk, br, rbase, rstart, rcell, di, dj, dk);
+      const int64_t ip = brick_particle(kk, br, mt.rbase, mt.rstart, mt.rcell, di, dj, dk);
       const int16_t *qp = p.xp + 3 * ip;
       float wx[3], wy[3], wz[3];
       const int64_t ix = tsc(decode_pos(q.ci0 + di - p.ncb, qp[0]) * p.scale - J.off[0], wx) + p.shift;
@@ -620,7 +657,8 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
       vm1 = fmaxf(vm1, fabsf(v1));
       vm2 = fmaxf(vm2, fabsf(v2));
     }
-    __syncthreads();  // the force window, the row tables and buffer cur are reused
+    __syncthreads();  // (3) the force window, meta[cur] and buffer cur are reused
+    if (tid == 0 && b + 2 * G < nbricks) meta[cur].pos = brick_pos(p, b + 2 * G, cb, p.ract, nullptr);
   }
   if (fail_k >= 0) {
     // a wait gave up: record it, and wait once more (also bounded) for the copies in flight
