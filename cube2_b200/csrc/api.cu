@@ -44,6 +44,7 @@ struct Plan {
   int n, batch;
   cufftType type;
   cufftHandle h;
+  int pad = 0;  // C2R into the interior of arrays with `pad` ghost points per side
 };
 
 struct Ctx {
@@ -105,6 +106,7 @@ struct Ctx {
   Buf dh_rhoc, dh_idx, dh_xp, dh_vp, dh_pid, dh_rhoc2, dh_idx2, dh_xp2, dh_vp2, dh_pid2;  // host-array drift
   Buf pw_grid, pw_k, pw_bins;  // power spectrum
   Buf ks_out;                  // FP64 conservation sums
+  Buf phi_pad;                 // padded potential of the brick kernels
   cudaEvent_t tune_ev[2 * kMaxPPShapes] = {};
   void *h_stage = nullptr;  // pinned staging for small tables
   size_t h_stage_cap = 0;
@@ -296,9 +298,27 @@ static int wait_vp() {
   return CUBE_OK;
 }
 
+// C2R whose output lands in the interior of [batch][(n+2 pad)^3] arrays (advanced layout)
+static int get_plan_padded_c2r(int n, int batch, int pad, cufftHandle *out) {
+  for (auto &p : g.plans)
+    if (p.n == n && p.batch == batch && p.type == CUFFT_C2R && p.pad == pad) {
+      CF(cufftSetStream(p.h, g.stream));
+      *out = p.h;
+      return CUBE_OK;
+    }
+  Plan p{n, batch, CUFFT_C2R, 0, pad};
+  const int m = n + 2 * pad;
+  int dims[3] = {n, n, n}, inembed[3] = {n, n, n / 2 + 1}, onembed[3] = {m, m, m};
+  CF(cufftPlanMany(&p.h, 3, dims, inembed, 1, n * n * (n / 2 + 1), onembed, 1, m * m * m, CUFFT_C2R, batch));
+  CF(cufftSetStream(p.h, g.stream));
+  g.plans.push_back(p);
+  *out = p.h;
+  return CUBE_OK;
+}
+
 static int get_plan(int n, int batch, cufftType type, cufftHandle *out) {
   for (auto &p : g.plans)
-    if (p.n == n && p.batch == batch && p.type == type) {
+    if (p.n == n && p.batch == batch && p.type == type && p.pad == 0) {
       CF(cufftSetStream(p.h, g.stream));
       *out = p.h;
       return CUBE_OK;
@@ -516,13 +536,18 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     // the force difference is fused into the gather brick by brick where the geometry allows;
     // otherwise the three force arrays are written and gathered from
     const bool fused = pm3_brick_mc(a) > 0;
+    const int64_t m3 = (int64_t)(n + 2 * kPotPad) * (n + 2 * kPotPad) * (n + 2 * kPotPad);
     if (!fused) {
       CK(grow(g.force, sizeof(float) * n3 * 3 * nslots));
       a.force = (float *)g.force.p;
+    } else {
+      CK(grow(g.phi_pad, sizeof(float) * m3 * nslots));
+      a.phi_pad = (float *)g.phi_pad.p;
     }
     cufftHandle fw, bw;
     CK(get_plan(n, nslots, CUFFT_R2C, &fw));
-    CK(get_plan(n, nslots, CUFFT_C2R, &bw));
+    if (fused) CK(get_plan_padded_c2r(n, nslots, kPotPad, &bw));
+    else CK(get_plan(n, nslots, CUFFT_C2R, &bw));
     CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3 * nslots, g.stream));
     if (g.xp_pending) {  // deposit each group of tiles as soon as its particles are on the device
       PM3Args at = a;
@@ -538,8 +563,16 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     }
     CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
     launch_pm3_kspace(a, g.stream);
-    CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)g.rho.p));  // potential
-    if (!fused) launch_pm3_force(a, g.stream);
+    if (fused) {
+      // the potential into the interior of the padded array, then its periodic ghost points
+      const int64_t mm = n + 2 * kPotPad;
+      float *interior = a.phi_pad + (kPotPad * mm + kPotPad) * mm + kPotPad;
+      CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)interior));
+      launch_pm3_ghosts(a, g.stream);
+    } else {
+      CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)g.rho.p));  // potential
+      launch_pm3_force(a, g.stream);
+    }
     auto gather = [&](const PM3Args &ga) {
       if (fused) launch_pm3_force_gather(ga, g.stream);
       else launch_pm3_gather(ga, g.stream);
@@ -560,7 +593,7 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       CK(wait_vp());
       gather(a);
     }
-    g.launches += fused ? 3 : 4;
+    g.launches += 4;
     CU(cudaGetLastError());
     return CUBE_OK;
   }
@@ -1976,6 +2009,7 @@ void c_pm3_fft_finalize(void) {
   release(g.rho);
   release(g.rhok);
   release(g.force);
+  release(g.phi_pad);
   release(g.jobs);
   release(g.mlp_pos);
   release(g.mlp_rho);

@@ -198,7 +198,9 @@ struct PM3Args {
   int want_vmax;
   int32_t *err = nullptr;  // device status word (bit CUBE_ERR_TIMEOUT from a bounded wait), may be null
   int num_sms = 148;
+  float *phi_pad = nullptr;  // the potential with kPotPad ghost points per side (periodic images), [nslots][(n+2P)^3]
 };
+constexpr int kPotPad = 4;  // ghost points per side of the padded potential of the brick kernels
 void launch_pm3_deposit(const PM3Args &a, cudaStream_t s);
 void launch_pm3_kspace(const PM3Args &a, cudaStream_t s);
 void launch_pm3_force(const PM3Args &a, cudaStream_t s);  // force arrays + f2max from the potential
@@ -206,7 +208,8 @@ void launch_pm3_gather(const PM3Args &a, cudaStream_t s);
 // periodic meshes: the force difference fused into the gather, brick by brick (no force arrays);
 // returns false (nothing launched) where the brick geometry does not apply
 int pm3_brick_mc(const PM3Args &a);
-bool launch_pm3_force_gather(const PM3Args &a, cudaStream_t s);
+bool launch_pm3_force_gather(const PM3Args &a, cudaStream_t s);  // reads a.phi_pad
+void launch_pm3_ghosts(const PM3Args &a, cudaStream_t s);          // fills the ghost points of a.phi_pad
 void launch_green_fp64(int n, double apm_soft, double apm_range, double gridsize, int p_order, float *G,
                        cudaStream_t s);
 

@@ -15,6 +15,9 @@
 //            points (kick.f90:494) in the same pass;
 //   gather   TSC gather of the force at each active particle and the kick
 //            vp += dv * a_mid*dt/(6 pi) (kick.f90:497-540).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 
@@ -494,7 +497,7 @@ constexpr int kForW = kBrick + 2;                      // force window 18^3
 constexpr int kPotElems = kPotW * kPotW * kPotX;
 constexpr uint32_t kPotBytes = sizeof(float) * kPotElems;
 constexpr int kFor3 = kForW * kForW * kForW;
-constexpr size_t kFgSmem = 2 * (size_t)kPotBytes + sizeof(float) * 3 * (size_t)kFor3;
+constexpr size_t kFgSmem = 2 * (size_t)kPotBytes + sizeof(float4) * (size_t)kFor3 + 128;  // + alignment slack
 
 struct BrickMeta {
   BrickPos pos;
@@ -529,17 +532,19 @@ __device__ __forceinline__ void meta_scan(BrickMeta &mt, int nrows) {
   mt.total = acc;
 }
 
-__global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, int64_t nbricks) {
+__global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, int64_t nbricks,
+                                                                const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(128) float fg_smem[];
-  float *pot0 = fg_smem;                    // [2][z 22][y 22][x 24]
-  float *fw = fg_smem + 2 * kPotElems;      // [3][z][y][x] 18^3
+  // the tensor copies land on 128-byte aligned shared addresses
+  float *pot0 = fg_smem + ((128u - (smem_addr(fg_smem) & 127u)) & 127u) / 4;  // [2][z 22][y 22][x 24]
+  float4 *fw = reinterpret_cast<float4 *>(pot0 + 2 * kPotElems);              // [z][y][x] 18^3 of (fx, fy, fz, 0)
   __shared__ __align__(8) uint64_t bars[2];
   __shared__ BrickMeta meta[2];
   __shared__ float red[4][kFgThreads / 32];
   __shared__ int s_fail;
   const int tid = threadIdx.x;
   const int cb = kBrick / mc, nrows = cb * cb;
-  const int64_t n = p.n, n3 = p.n3;
+  const int64_t n = p.n;
   const int64_t G = gridDim.x;
   int64_t b = blockIdx.x;
   if (b >= nbricks) return;
@@ -554,24 +559,18 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
   }
   __syncthreads();
   if (tid < nrows) meta_row(p, cb, meta[0], tid);
-  // the copies of a brick's potential window into buffer `buf`: row t (z, y) = (t / 22, t % 22)
+  // a brick's potential window into buffer `buf`: one tensor copy of the box (x 24, y 22, z 22)
+  // of the padded potential that starts kPotPad - 4 / - 3 points before the owned points (the
+  // ghost points hold the periodic images, so the box never wraps)
   auto issue = [&](const BrickPos &q, int buf) {
-    if (tid < kPotW * kPotW) {
-      const float *phi = p.rho + (int64_t)p.jobs[q.j].slot * n3;
-      const int z = tid / kPotW, y = tid % kPotW;
-      const int64_t gz = wrap_near(q.Z0 - 3 + z, n), gy = wrap_near(q.Y0 - 3 + y, n);
-      const float *row = phi + (gz * n + gy) * n;
-      float *dst = pot0 + buf * kPotElems + (z * kPotW + y) * kPotX;
-      const int64_t xs = q.X0 - 4;  // a multiple of 4, as n: the pieces stay 16-byte aligned
-      if (xs < 0) {
-        bulk_g2s(dst, row + n + xs, (uint32_t)(-xs * 4), &bars[buf]);
-        bulk_g2s(dst - xs, row, (uint32_t)((kPotX + xs) * 4), &bars[buf]);
-      } else if (xs + kPotX > n) {
-        bulk_g2s(dst, row + xs, (uint32_t)((n - xs) * 4), &bars[buf]);
-        bulk_g2s(dst + (n - xs), row, (uint32_t)((xs + kPotX - n) * 4), &bars[buf]);
-      } else {
-        bulk_g2s(dst, row + xs, sizeof(float) * kPotX, &bars[buf]);
-      }
+    if (tid == 0) {
+      const int cx = (int)q.X0 - 4 + kPotPad, cy = (int)q.Y0 - 3 + kPotPad, cz = (int)q.Z0 - 3 + kPotPad;
+      const int cs = p.jobs[q.j].slot;
+      asm volatile(
+          "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+          "%5}], [%6];" ::"r"(smem_addr(pot0 + buf * kPotElems)),
+          "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(cx), "r"(cy), "r"(cz), "r"(cs), "r"(smem_addr(&bars[buf]))
+          : "memory");
     }
   };
   issue(meta[0].pos, 0);
@@ -593,20 +592,28 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
       issue(meta[nxt].pos, nxt);
       if (tid == 0) mbar_arrive(&bars[nxt]);
     }
+    const BrickMeta &mt = meta[cur];
+    const BrickPos &q = mt.pos;
+    const MeshJob &J = p.jobs[q.j];
+    BrickRows br;
+    br.nrows = nrows;
+    br.total = mt.total;
+    br.cb = cb;
     if (!mbar_wait_bounded(&bars[cur], (uint32_t)(k >> 1) & 1u)) s_fail = 1;
-    // force window: point (x, y, z) is mesh point (X0 - 1 + x, ...), potential (x + 3, y + 2, z + 2)
+    // force window: point (x, y, z) is mesh point (X0 - 1 + x, ...), potential (x + 3, y + 2, z + 2);
+    // a brick without particles needs only its owned points (for max |F|^2)
     const float *pot = pot0 + cur * kPotElems;
+    const bool halo = br.total > 0;
     for (int e = tid; e < kFor3; e += kFgThreads) {
       const int x = e % kForW, y = (e / kForW) % kForW, z = e / (kForW * kForW);
+      const bool own = x >= 1 && x <= kBrick && y >= 1 && y <= kBrick && z >= 1 && z <= kBrick;
+      if (!own && !halo) continue;
       const int c = (z + 2) * PZ + (y + 2) * PY + (x + 3);
       const float fx = w(pot[c - 2], pot[c - 1], pot[c + 1], pot[c + 2]);
       const float fy = w(pot[c - 2 * PY], pot[c - PY], pot[c + PY], pot[c + 2 * PY]);
       const float fz = w(pot[c - 2 * PZ], pot[c - PZ], pot[c + PZ], pot[c + 2 * PZ]);
-      fw[e] = fx;
-      fw[kFor3 + e] = fy;
-      fw[2 * kFor3 + e] = fz;
-      if (x >= 1 && x <= kBrick && y >= 1 && y <= kBrick && z >= 1 && z <= kBrick)
-        m = fmaxf(m, fx * fx + fy * fy + fz * fz);
+      fw[e] = make_float4(fx, fy, fz, 0.f);
+      if (own) m = fmaxf(m, fx * fx + fy * fy + fz * fz);
     }
     if (has_next && tid < nrows) meta_row(p, cb, meta[nxt], tid);  // loads overlap the other warps' work
     __syncthreads();  // (2) force window complete; a failed wait seen by all
@@ -616,13 +623,6 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
       break;
     }
     if (tid == 0 && has_next) meta_scan(meta[nxt], nrows);
-    const BrickMeta &mt = meta[cur];
-    const BrickPos &q = mt.pos;
-    const MeshJob &J = p.jobs[q.j];
-    BrickRows br;
-    br.nrows = nrows;
-    br.total = mt.total;
-    br.cb = cb;
     for (int kk = tid; kk < br.total; kk += kFgThreads) {
       int di, dj, dk;
       const int64_t ip = brick_particle(kk, br, mt.rbase, mt.rstart, mt.rcell, di, dj, dk);
@@ -642,9 +642,10 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
 #pragma unroll
           for (int a = 0; a < 3; a++) {
             const float wt = (wx[a] * wy[bb]) * wz[c];
-            d0 += fw[row + a] * wt;
-            d1 += fw[kFor3 + row + a] * wt;
-            d2 += fw[2 * kFor3 + row + a] * wt;
+            const float4 f = fw[row + a];
+            d0 += f.x * wt;
+            d1 += f.y * wt;
+            d2 += f.z * wt;
           }
         }
       }
@@ -858,16 +859,85 @@ void launch_pm3_deposit(const PM3Args &a, cudaStream_t s) {
   k_deposit<<<(unsigned)((warps + kWarps - 1) / kWarps), kWarps * 32, 0, s>>>(p);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
+  }
+  return fn;
+}
+
 bool launch_pm3_force_gather(const PM3Args &a, cudaStream_t s) {
   const int mc = brick_mc(a, false);
-  if (!mc) return false;
+  if (!mc || !a.phi_pad) return false;
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return false;
+  // the padded potential as a 4-d tensor [slot][z][y][x], boxes of the potential window
+  const cuuint64_t m = (cuuint64_t)a.n + 2 * kPotPad;
+  const cuuint64_t dims[4] = {m, m, m, (cuuint64_t)a.nslots};
+  const cuuint64_t strides[3] = {m * 4, m * m * 4, m * m * m * 4};
+  const cuuint32_t box[4] = {kPotX, kPotW, kPotW, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUtensorMap tmap;
+  if (encode(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.phi_pad, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
   PM3K p = make_k(a);
   const int cb = kBrick / mc;
   const int64_t nbricks = (int64_t)(a.ract[0] / cb) * (a.ract[1] / cb) * (a.ract[2] / cb) * a.njobs;
   set_smem_attr_once((const void *)k_force_gather, kFgSmem);
   const int64_t grid = std::min<int64_t>(nbricks, a.num_sms > 0 ? a.num_sms : 148);
-  if (grid > 0) k_force_gather<<<(unsigned)grid, kFgThreads, kFgSmem, s>>>(p, mc, nbricks);
+  if (grid > 0) k_force_gather<<<(unsigned)grid, kFgThreads, kFgSmem, s>>>(p, mc, nbricks, tmap);
   return true;
+}
+
+// ghost points of the padded potential: each takes the interior point it is a periodic image of.
+// The z slabs (all y, x), the y slabs (interior z, all x) and the x slabs (interior z, y) are
+// disjoint and together cover every ghost point once.
+__global__ void k_pm3_ghosts(float *phi, int n, int nslots) {
+  const int P = kPotPad;
+  const int64_t m = n + 2 * P;
+  const int64_t nz = 2 * P * m * m, ny = (int64_t)n * 2 * P * m, nx = (int64_t)n * n * 2 * P;
+  const int64_t per = nz + ny + nx;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < per * nslots;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t sl = e / per;
+    int64_t r = e - sl * per;
+    int64_t x, y, z;
+    if (r < nz) {
+      x = r % m;
+      y = (r / m) % m;
+      const int64_t g = r / (m * m);  // 0 .. 2P-1
+      z = g < P ? g : n + g;
+    } else if ((r -= nz) < ny) {
+      x = r % m;
+      const int64_t g = (r / m) % (2 * P);
+      y = g < P ? g : n + g;
+      z = P + r / (m * 2 * P);
+    } else {
+      r -= ny;
+      const int64_t g = r % (2 * P);
+      x = g < P ? g : n + g;
+      y = P + (r / (2 * P)) % n;
+      z = P + r / (2 * P * n);
+    }
+    const int64_t sx = P + ((x - P) % n + n) % n, sy = P + ((y - P) % n + n) % n, sz = P + ((z - P) % n + n) % n;
+    float *base = phi + sl * m * m * m;
+    base[(z * m + y) * m + x] = base[(sz * m + sy) * m + sx];
+  }
+}
+
+void launch_pm3_ghosts(const PM3Args &a, cudaStream_t s) {
+  if (!a.phi_pad) return;
+  k_pm3_ghosts<<<(unsigned)((a.num_sms > 0 ? a.num_sms : 148) * 8), 256, 0, s>>>(a.phi_pad, a.n, a.nslots);
 }
 
 void launch_pm3_gather(const PM3Args &a, cudaStream_t s) {
