@@ -107,6 +107,7 @@ struct Ctx {
   Buf pw_grid, pw_k, pw_bins;  // power spectrum
   Buf ks_out;                  // FP64 conservation sums
   Buf phi_pad;                 // padded potential of the brick kernels
+  Buf brick_ctr;               // their work counter
   cudaEvent_t tune_ev[2 * kMaxPPShapes] = {};
   void *h_stage = nullptr;  // pinned staging for small tables
   size_t h_stage_cap = 0;
@@ -543,6 +544,8 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     } else {
       CK(grow(g.phi_pad, sizeof(float) * m3 * nslots));
       a.phi_pad = (float *)g.phi_pad.p;
+      CK(grow(g.brick_ctr, sizeof(int32_t) * 64));
+      a.brick_ctr = (int32_t *)g.brick_ctr.p;
     }
     cufftHandle fw, bw;
     CK(get_plan(n, nslots, CUFFT_R2C, &fw));
@@ -2010,6 +2013,7 @@ void c_pm3_fft_finalize(void) {
   release(g.rhok);
   release(g.force);
   release(g.phi_pad);
+  release(g.brick_ctr);
   release(g.jobs);
   release(g.mlp_pos);
   release(g.mlp_rho);

@@ -199,6 +199,7 @@ struct PM3Args {
   int32_t *err = nullptr;  // device status word (bit CUBE_ERR_TIMEOUT from a bounded wait), may be null
   int num_sms = 148;
   float *phi_pad = nullptr;  // the potential with kPotPad ghost points per side (periodic images), [nslots][(n+2P)^3]
+  int32_t *brick_ctr = nullptr;  // work counter of the brick kernels (one int, zeroed by the launcher)
 };
 constexpr int kPotPad = 4;  // ghost points per side of the padded potential of the brick kernels
 void launch_pm3_deposit(const PM3Args &a, cudaStream_t s);

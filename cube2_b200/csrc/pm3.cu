@@ -48,6 +48,7 @@ struct PM3K {
   int fphys_lo, fphys_n;
   int nslots;
   int32_t *err;
+  int32_t *brick_ctr;
 };
 
 // a + d into [0, n) for |d| < n
@@ -542,19 +543,25 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
   __shared__ BrickMeta meta[2];
   __shared__ float red[4][kFgThreads / 32];
   __shared__ int s_fail;
+  __shared__ int64_t s_brick[3];  // bricks k, k + 1, k + 2 of this block (claimed ahead; >= nbricks: none)
   const int tid = threadIdx.x;
   const int cb = kBrick / mc, nrows = cb * cb;
   const int64_t n = p.n;
-  const int64_t G = gridDim.x;
-  int64_t b = blockIdx.x;
+  // bricks are claimed from a work counter: a block that meets a crowded brick takes fewer bricks
+  if (tid == 0) {
+    s_brick[0] = blockIdx.x;
+    s_brick[1] = gridDim.x + atomicAdd(p.brick_ctr, 1);
+    s_fail = 0;
+  }
+  __syncthreads();
+  int64_t b = s_brick[0];
   if (b >= nbricks) return;
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_fail = 0;
     meta[0].pos = brick_pos(p, b, cb, p.ract, nullptr);
-    if (b + G < nbricks) meta[1].pos = brick_pos(p, b + G, cb, p.ract, nullptr);
+    if (s_brick[1] < nbricks) meta[1].pos = brick_pos(p, s_brick[1], cb, p.ract, nullptr);
     mbar_expect_tx(&bars[0], kPotBytes);
   }
   __syncthreads();
@@ -582,9 +589,9 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
   int fail_k = -1;         // the iteration whose wait gave up
   bool fail_next = false;  // ... and whether it had issued the next brick's copies
   constexpr int PY = kPotX, PZ = kPotX * kPotW;
-  for (int k = 0; b < nbricks; k++, b += G) {
+  for (int k = 0; b < nbricks; k++) {
     const int cur = k & 1, nxt = cur ^ 1;
-    const bool has_next = b + G < nbricks;
+    const bool has_next = s_brick[1] < nbricks;
     if (tid == 0 && has_next) mbar_expect_tx(&bars[nxt], kPotBytes);
     __syncthreads();  // (1) meta[cur] complete, buffer nxt no longer read, expect before the copies
     if (has_next) {
@@ -659,7 +666,14 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
       vm2 = fmaxf(vm2, fabsf(v2));
     }
     __syncthreads();  // (3) the force window, meta[cur] and buffer cur are reused
-    if (tid == 0 && b + 2 * G < nbricks) meta[cur].pos = brick_pos(p, b + 2 * G, cb, p.ract, nullptr);
+    if (tid == 0) {
+      const int64_t b2 = has_next ? gridDim.x + atomicAdd(p.brick_ctr, 1) : nbricks;
+      if (b2 < nbricks) meta[cur].pos = brick_pos(p, b2, cb, p.ract, nullptr);
+      s_brick[0] = s_brick[1];
+      s_brick[1] = b2;
+    }
+    __syncthreads();
+    b = s_brick[0];
   }
   if (fail_k >= 0) {
     // a wait gave up: record it, and wait once more (also bounded) for the copies in flight
@@ -723,6 +737,7 @@ static PM3K make_k(const PM3Args &a) {
   p.fphys_n = a.fphys_n;
   p.nslots = a.nslots;
   p.err = a.err;
+  p.brick_ctr = a.brick_ctr;
   return p;
 }
 
@@ -895,6 +910,8 @@ bool launch_pm3_force_gather(const PM3Args &a, cudaStream_t s) {
   const int64_t nbricks = (int64_t)(a.ract[0] / cb) * (a.ract[1] / cb) * (a.ract[2] / cb) * a.njobs;
   set_smem_attr_once((const void *)k_force_gather, kFgSmem);
   const int64_t grid = std::min<int64_t>(nbricks, a.num_sms > 0 ? a.num_sms : 148);
+  if (!a.brick_ctr) return false;
+  cudaMemsetAsync(a.brick_ctr, 0, sizeof(int32_t), s);
   if (grid > 0) k_force_gather<<<(unsigned)grid, kFgThreads, kFgSmem, s>>>(p, mc, nbricks, tmap);
   return true;
 }
@@ -904,40 +921,43 @@ bool launch_pm3_force_gather(const PM3Args &a, cudaStream_t s) {
 // disjoint and together cover every ghost point once.
 __global__ void k_pm3_ghosts(float *phi, int n, int nslots) {
   const int P = kPotPad;
-  const int64_t m = n + 2 * P;
-  const int64_t nz = 2 * P * m * m, ny = (int64_t)n * 2 * P * m, nx = (int64_t)n * n * 2 * P;
-  const int64_t per = nz + ny + nx;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < per * nslots;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t sl = e / per;
-    int64_t r = e - sl * per;
-    int64_t x, y, z;
+  const int m = n + 2 * P;
+  const int nz = 2 * P * m * m, ny = n * 2 * P * m, nx = n * n * 2 * P;
+  const int per = nz + ny + nx;
+  const int sl = blockIdx.y;
+  float *base = phi + (int64_t)sl * m * m * m;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < per; e += gridDim.x * blockDim.x) {
+    int r = e, x, y, z;
     if (r < nz) {
       x = r % m;
       y = (r / m) % m;
-      const int64_t g = r / (m * m);  // 0 .. 2P-1
+      const int g = r / (m * m);  // 0 .. 2P-1
       z = g < P ? g : n + g;
     } else if ((r -= nz) < ny) {
       x = r % m;
-      const int64_t g = (r / m) % (2 * P);
+      const int g = (r / m) % (2 * P);
       y = g < P ? g : n + g;
       z = P + r / (m * 2 * P);
     } else {
       r -= ny;
-      const int64_t g = r % (2 * P);
+      const int g = r % (2 * P);
       x = g < P ? g : n + g;
       y = P + (r / (2 * P)) % n;
       z = P + r / (2 * P * n);
     }
-    const int64_t sx = P + ((x - P) % n + n) % n, sy = P + ((y - P) % n + n) % n, sz = P + ((z - P) % n + n) % n;
-    float *base = phi + sl * m * m * m;
-    base[(z * m + y) * m + x] = base[(sz * m + sy) * m + sx];
+    const int sx = x < P ? x + n : (x >= n + P ? x - n : x);
+    const int sy = y < P ? y + n : (y >= n + P ? y - n : y);
+    const int sz = z < P ? z + n : (z >= n + P ? z - n : z);
+    base[((int64_t)z * m + y) * m + x] = base[((int64_t)sz * m + sy) * m + sx];
   }
 }
 
 void launch_pm3_ghosts(const PM3Args &a, cudaStream_t s) {
   if (!a.phi_pad) return;
-  k_pm3_ghosts<<<(unsigned)((a.num_sms > 0 ? a.num_sms : 148) * 8), 256, 0, s>>>(a.phi_pad, a.n, a.nslots);
+  const int m = a.n + 2 * kPotPad;
+  const int64_t per = (int64_t)2 * kPotPad * m * m + (int64_t)a.n * 2 * kPotPad * m + (int64_t)a.n * a.n * 2 * kPotPad;
+  const unsigned gx = (unsigned)std::min<int64_t>((per + 255) / 256, 4096);
+  k_pm3_ghosts<<<dim3(gx, (unsigned)a.nslots), 256, 0, s>>>(a.phi_pad, a.n, a.nslots);
 }
 
 void launch_pm3_gather(const PM3Args &a, cudaStream_t s) {
