@@ -499,8 +499,69 @@ def learned_variant(args, img, tables, stream, truth_plain, value_plain, ms_plai
         res["note"] = ("the sampled error exceeds the bound: the kick falls back to the plain cutoff-2 kick, "
                        "whose value is the line's value" if rms > LEARNED_BOUND else
                        "within the bound: the learned kick stands")
+        # the per-cell check: the full-cutoff kick judges the network cell by cell, and the cells
+        # over the bound take its velocities (cube_learned_fallback)
+        try:
+            res["per_cell_fallback"] = per_cell_fallback(args, img, tables, stream, kick, vp, vp0, Ft, samp, kc,
+                                                         ms_plain)
+        except Exception as e:  # reported beside the learned kick, never instead of it
+            res["per_cell_fallback"] = {"error": repr(e)}
     shell.close()
     return res
+
+
+FALLBACK_SAMPLES = 4  # particles checked per coarse cell
+
+
+def per_cell_fallback(args, img, tables, stream, learned_kick, vp, vp0, Ft, samp, kc, ms_plain):
+    """The learned kick with its per-cell check: learned kick, full-cutoff kick on a copy of the
+    starting velocities, then every coarse cell checked on its first FALLBACK_SAMPLES particles
+    against the full-cutoff kick and the cells over the bound recomputed at cutoff 2 (they take
+    the full-cutoff velocities).  Timed over the same steps as the plain kick; the error after
+    the fallback is stated against the FP64 truth on the same sampled particles."""
+    import torch
+    from cube2_b200 import learned as Ln
+    from cube2_b200.kick import CUBE_PM3_PERIODIC, FineKick
+    from cube2_b200.layout import apm3_table
+    L = img.layout
+    isort, ires, ix, _, rs = tables
+    rho, idx, xp, _ = Ln.device_image(img, vp.device)
+    fk1 = FineKick(L, pm3_mode=CUBE_PM3_PERIODIC, apm3f=Ln.SHORT.apm3f)
+    fk2 = FineKick(L, pm3_mode=CUBE_PM3_PERIODIC, apm3f=Ln.PLAIN.apm3f)
+    a2 = apm3_table(Ln.PLAIN.apm3f)
+    vpf = vp0.clone()
+    out = torch.zeros(8, device=vp.device)
+    a_mid, dt = float(np.float32(6 * np.pi)), 1.0
+
+    def step():  # the layout's PM3 softening is switched between the two splits (cube_set_layout)
+        vp.copy_(vp0)
+        fk1.configure()
+        learned_kick(True)
+        vpf.copy_(vp0)
+        fk2.configure()
+        fk2.kick_fine_device(rho, idx, xp, img.n_used, vpf, out, isort, ires, ix, a2, rs, 1.0, a_mid, dt,
+                             stream=stream)
+        return Ln.fallback(rho, idx, img.n_used, vp0, vp, vpf, LEARNED_BOUND, FALLBACK_SAMPLES, stream=stream)
+    for _ in range(max(args.warmup, 1)):
+        st = step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        st = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    F = (vp - vp0).cpu().numpy().reshape(-1, 3).astype(np.float64)[samp] / kc
+    d = np.linalg.norm(F - Ft, axis=1)
+    m = np.linalg.norm(Ft, axis=1)
+    return {"bound": LEARNED_BOUND, "samples_per_cell": FALLBACK_SAMPLES, **st,
+            "fraction_fallen_back": st["particles_fallen_back"] / max(img.n_particles, 1),
+            "force_error_after": {"rms_rel": float(np.sqrt(np.sum(d ** 2) / np.sum(m ** 2))),
+                                  "p99_rel": float(np.percentile(d / np.maximum(m, 1e-30), 99))},
+            "ms_per_step": ms, "value": img.n_particles / (ms * 1e-3), "unit": UNIT,
+            "speedup_vs_plain": ms_plain / ms,
+            "what": "learned kick + full-cutoff kick (the judge) + per-cell check and fallback, per step"}
 
 
 def _batch_boxes(workload: str):

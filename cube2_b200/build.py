@@ -19,7 +19,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr"]
-SOURCES = ["binning.cu", "pp.cu", "pm3.cu", "ewald.cu", "probe.cu", "noalloc.cu", "mlp.cu", "drift.cu", "power.cu", "snapshot.cu", "sums.cu", "api.cu"]
+SOURCES = ["binning.cu", "pp.cu", "pm3.cu", "ewald.cu", "probe.cu", "noalloc.cu", "mlp.cu", "drift.cu", "power.cu", "snapshot.cu", "sums.cu", "fallback.cu", "api.cu"]
 HEADERS = ["common.cuh"]
 
 

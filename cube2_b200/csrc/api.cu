@@ -106,6 +106,7 @@ struct Ctx {
   Buf dh_rhoc, dh_idx, dh_xp, dh_vp, dh_pid, dh_rhoc2, dh_idx2, dh_xp2, dh_vp2, dh_pid2;  // host-array drift
   Buf pw_grid, pw_k, pw_bins;  // power spectrum
   Buf ks_out;                  // FP64 conservation sums
+  Buf fb_out;                  // learned-shell fallback statistics
   Buf phi_pad;                 // padded potential of the brick kernels
   Buf brick_ctr;               // their work counter
   cudaEvent_t tune_ev[2 * kMaxPPShapes] = {};
@@ -1662,6 +1663,40 @@ int cube_kick_sums(const int32_t *d_rhoc, const int64_t *d_idx_b_r, int64_t n_us
   return CUBE_OK;
 }
 
+int cube_learned_fallback(const int32_t *d_rhoc, const int64_t *d_idx_b_r, int64_t n_used, const float *d_vp0,
+                          const float *d_vp_learned, const float *d_vp_full, float bound, int32_t samples,
+                          float *d_vp_out, double out[5], void *stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  t_last_error = CUBE_OK;
+  if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
+  if (!d_rhoc || !d_idx_b_r || !out || n_used < 0 || samples < 1 || samples > 32 || !(bound >= 0.f))
+    return fail(CUBE_ERR_INVALID);
+  if (n_used > 0 && (!d_vp0 || !d_vp_learned || !d_vp_full || !d_vp_out)) return fail(CUBE_ERR_INVALID);
+  CK(ensure_device());
+  CK(grow(g.fb_out, sizeof(double) * 8));
+  cudaStream_t st = stream ? (cudaStream_t)stream : g.stream;
+  unsigned long long *stats = (unsigned long long *)g.fb_out.p;
+  double *err = (double *)g.fb_out.p + 4;
+  CU(cudaMemsetAsync(g.fb_out.p, 0, sizeof(double) * 8, st));
+  if (n_used > 0 && d_vp_out != d_vp_learned)
+    CU(cudaMemcpyAsync(d_vp_out, d_vp_learned, sizeof(float) * 3 * (size_t)n_used, cudaMemcpyDeviceToDevice, st));
+  launch_learned_fallback(g.L, d_rhoc, d_idx_b_r, d_vp0, d_vp_learned, d_vp_full, bound, samples, d_vp_out, stats,
+                          err, st);
+  g.launches += 1;
+  CU(cudaGetLastError());
+  unsigned long long hs[4];
+  double he[2];
+  CU(cudaMemcpyAsync(hs, stats, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(he, err, sizeof(he), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  out[0] = (double)hs[0];
+  out[1] = (double)hs[1];
+  out[2] = (double)hs[2];
+  out[3] = he[1] > 0.0 ? std::sqrt(he[0] / he[1]) : 0.0;
+  out[4] = (double)samples;
+  return CUBE_OK;
+}
+
 int cube_power_spectrum(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp, int64_t n_used,
                         int64_t n_physical, int32_t nw, int32_t nbin, double *bins, void *stream) {
   std::lock_guard<std::mutex> lk(g_mu);
@@ -2025,7 +2060,7 @@ void c_gpu_velocity_finalize(void) {
   cudaSetDevice(g.device);
   cudaStreamSynchronize(g.stream);
   Buf *bufs[] = {&g.xp, &g.rhoc, &g.idx, &g.vp, &g.cell_base, &g.tiles, &g.count, &g.cell_start, &g.scan_tmp,
-                 &g.spos, &g.spill, &g.spill_rank, &g.counters, &g.items, &g.range_loc, &g.sched, &g.out, &g.ks_out};
+                 &g.spos, &g.spill, &g.spill_rank, &g.counters, &g.items, &g.range_loc, &g.sched, &g.out, &g.ks_out, &g.fb_out};
   for (Buf *b : bufs) release(*b);
 }
 

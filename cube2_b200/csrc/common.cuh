@@ -160,6 +160,12 @@ struct PPArgs {
 constexpr int kNumKickSums = 8;
 void launch_kick_sums(const Lay &L, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const float *d_va,
                       const float *d_vb, float mass, double *d_out, cudaStream_t s);
+// learned shell: per-cell check of the learned velocities against the full-cutoff ones on the
+// first `samples` physical particles of each coarse cell; cells over the bound take the
+// full-cutoff velocities (fallback.cu).  d_out must already hold a copy of d_vpl.
+void launch_learned_fallback(const Lay &L, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const float *d_vp0,
+                             const float *d_vpl, const float *d_vpf, float bound, int samples, float *d_out,
+                             unsigned long long *d_stats, double *d_err, cudaStream_t s);
 size_t sched_ints(int ntile);
 int64_t sched_total_index(int ntile);  // where the work list's item count lies in `sched`
 int pp_num_shapes();

@@ -58,7 +58,7 @@ EXPORTS = ("cube_set_layout", "cube_get_layout", "cube_last_error", "cube_error_
            "cube_mlp_get_params", "cube_mlp_features", "cube_mlp_train_step", "cube_mlp_forward", "cube_mlp_kick",
            "cube_pp_set_shape", "cube_pp_shapes", "cube_drift_device", "cube_drift", "cube_buffer_v_device",
            "cube_power_spectrum", "cube_snapshot_write", "cube_snapshot_read", "cube_pm1_force_device",
-           "cube_pm2_force_device", "cube_pp_work_stats", "cube_kick_sums")
+           "cube_pm2_force_device", "cube_pp_work_stats", "cube_kick_sums", "cube_learned_fallback")
 
 
 def lib() -> ctypes.CDLL:

@@ -121,6 +121,20 @@ def features(layout: Layout, d_rhoc, d_idx, d_xp, n_used: int, stream=None):
     return X
 
 
+def fallback(d_rhoc, d_idx, n_used: int, d_vp0, d_vp_learned, d_vp_full, bound: float, samples: int = 4,
+             d_vp_out=None, stream=None) -> dict:
+    """Per-cell check of the learned kick against the full-cutoff kick and fallback of the cells
+    over the bound (cube_learned_fallback); d_vp_out defaults to d_vp_learned (in place)."""
+    out = np.zeros(5, np.float64)
+    dst = d_vp_learned if d_vp_out is None else d_vp_out
+    _check(lib().cube_learned_fallback(_dp(d_rhoc), _dp(d_idx), ctypes.c_int64(int(n_used)), _dp(d_vp0),
+                                       _dp(d_vp_learned), _dp(d_vp_full), ctypes.c_float(bound),
+                                       ctypes.c_int32(samples), _dp(dst), _p(out), _sp(stream)),
+           "cube_learned_fallback")
+    return dict(cells_checked=int(out[0]), cells_over=int(out[1]), particles_fallen_back=int(out[2]),
+                sampled_rms_vs_full=float(out[3]), samples=int(out[4]))
+
+
 def kick_coef(a_mid: float, dt: float) -> float:
     return float(np.float32(np.float32(a_mid) * np.float32(dt) / np.float32(6.0))) / np.pi
 

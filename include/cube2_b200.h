@@ -311,6 +311,20 @@ int cube_mlp_forward(cube_mlp *mlp, const void *d_X, int64_t rows, float *d_Y, v
 int cube_mlp_kick(cube_mlp *mlp, const int32_t *d_rhoc, const int64_t *d_idx_b_r, const int16_t *d_xp,
                   int64_t n_used, float *d_vp, float scale, float a_mid, float dt, void *stream);
 
+/* The learned shell's per-cell check and fallback.  d_vp_learned and d_vp_full hold the
+ * velocities after the learned kick (cutoff-1 split plus cube_mlp_kick) and after the
+ * full-cutoff kick (the plain cube_kick_fine_device) of the same image, both from d_vp0.  The
+ * full-cutoff kick judges the network: every coarse cell with physical particles is checked
+ * on its first `samples` (1..32) particles in storage order, by the relative rms difference of
+ * the two velocity changes there; a cell over `bound` takes the full-cutoff velocities for all
+ * its particles, the others keep the learned ones.  d_vp_out (may be d_vp_learned) receives
+ * the result.  out[0] = cells checked, out[1] = cells over the bound, out[2] = particles that
+ * fell back, out[3] = relative rms of the learned change against the full-cutoff one over all
+ * samples, out[4] = samples.  Waits for `stream`.  No reference counterpart. */
+int cube_learned_fallback(const int32_t *d_rhoc, const int64_t *d_idx_b_r, int64_t n_used, const float *d_vp0,
+                          const float *d_vp_learned, const float *d_vp_full, float bound, int32_t samples,
+                          float *d_vp_out, double out[5], void *stream);
+
 /* ---- allocation-free PP kick ---- */
 
 /* Largest input cube_pp_force_noalloc accepts: stored particles (n_used) and
