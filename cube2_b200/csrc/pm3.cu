@@ -481,28 +481,36 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                : "memory");
 }
 
-// Force and gather in one pass, persistent: each block walks bricks b = blockIdx.x + k gridDim.x.
-// A brick's potential window (the brick plus three points on every side; along x widened to
-// whole 16-byte groups, owned - 4 .. owned + kBrick + 3) arrives by bulk asynchronous copies,
-// one per row (two where the row wraps around the periodic mesh), into one of two shared
-// buffers: the next brick's window streams in while this brick is computed.  The brick's place
-// and its row table are prepared one brick ahead by single threads.  The 4-point difference of
-// potential_to_force (kick.f90:545-568) gives the three force components on the brick plus one
-// point on every side, in shared memory, and max |F|^2 of the owned points (kick.f90:494);
-// every active particle of the brick then gathers its 27 TSC points from there and is kicked
-// (kick.f90:497-540).  The force arrays never reach HBM.  The arithmetic (weights, products,
-// summation order) is the one of k_force_zm followed by k_gather.
+// Force and gather in one pass, persistent and warp-specialised: one 1024-thread block per SM
+// claims bricks from a work counter.  Its 16 producer warps compute a brick's force window
+// while its 16 consumer warps gather the previous brick, so the two phases overlap instead of
+// alternating behind block barriers.
+//   producers: the brick's potential window (the brick plus three points on every side; along
+//     x widened to whole 16-byte groups) arrives by one 4-d tensor copy of the ghost-padded
+//     potential (cp.async.bulk.tensor, the ghost points hold the periodic images so the box
+//     never wraps); the 4-point difference of potential_to_force (kick.f90:545-568) gives the
+//     three force components on the brick plus one point on every side, in one of two force
+//     buffers, and max |F|^2 of the owned points (kick.f90:494); the brick's row table goes
+//     beside it; then the next brick's window is requested.
+//   consumers: every active particle of the brick gathers its 27 TSC points from the force
+//     buffer and is kicked (kick.f90:497-540).
+// The buffers change hands through mbarriers (full: producers -> consumers, empty: back), every
+// wait bounded; a decision to stop is voted group-wide, so a group's barriers stay matched.
+// The arithmetic (weights, products, summation order) is the one of k_force_zm followed by
+// k_gather, and the force arrays never reach HBM.
 constexpr int kFgThreads = 1024;
+constexpr int kFgGroup = kFgThreads / 2;      // threads per group
+constexpr int kFgGroupWarps = kFgGroup / 32;  // mbarrier arrivals per hand-off
 constexpr int kPotX = kBrick + 8, kPotW = kBrick + 6;  // potential window: x 24, y and z 22
 constexpr int kForW = kBrick + 2;                      // force window 18^3
 constexpr int kPotElems = kPotW * kPotW * kPotX;
 constexpr uint32_t kPotBytes = sizeof(float) * kPotElems;
 constexpr int kFor3 = kForW * kForW * kForW;
-constexpr size_t kFgSmem = 2 * (size_t)kPotBytes + sizeof(float4) * (size_t)kFor3 + 128;  // + alignment slack
+constexpr size_t kFgSmem = (size_t)kPotBytes + 2 * sizeof(float) * 3 * (size_t)kFor3 + 128;  // + alignment slack
 
 struct BrickMeta {
   BrickPos pos;
-  int total;
+  int total;  // particles of the brick; -1: no brick (the consumers stop)
   int64_t rbase[kMaxRowsPerBrick];
   int rstart[kMaxRowsPerBrick + 1];
   int rcell[kMaxRowsPerBrick * (kMaxCb + 1)];
@@ -533,157 +541,191 @@ __device__ __forceinline__ void meta_scan(BrickMeta &mt, int nrows) {
   mt.total = acc;
 }
 
+// barrier of one group (named barrier `id`, kFgGroup threads) that also ORs a flag over the group
+__device__ __forceinline__ bool group_any(int id, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(kFgGroup)
+      : "memory");
+  return r != 0;
+}
+
 __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, int64_t nbricks,
                                                                 const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(128) float fg_smem[];
-  // the tensor copies land on 128-byte aligned shared addresses
-  float *pot0 = fg_smem + ((128u - (smem_addr(fg_smem) & 127u)) & 127u) / 4;  // [2][z 22][y 22][x 24]
-  float4 *fw = reinterpret_cast<float4 *>(pot0 + 2 * kPotElems);              // [z][y][x] 18^3 of (fx, fy, fz, 0)
-  __shared__ __align__(8) uint64_t bars[2];
+  // the tensor copies land on a 128-byte aligned shared address
+  float *pot = fg_smem + ((128u - (smem_addr(fg_smem) & 127u)) & 127u) / 4;  // [z 22][y 22][x 24]
+  float *fwb = pot + kPotElems;                                                 // [2][3][z][y][x] 18^3
+  __shared__ __align__(8) uint64_t bar_pot, bar_full[2], bar_empty[2];
   __shared__ BrickMeta meta[2];
+  __shared__ BrickPos s_next;     // the producers' next brick
+  __shared__ int64_t s_next_id;   // its index (>= nbricks: none)
   __shared__ float red[4][kFgThreads / 32];
   __shared__ int s_fail;
-  __shared__ int64_t s_brick[3];  // bricks k, k + 1, k + 2 of this block (claimed ahead; >= nbricks: none)
   const int tid = threadIdx.x;
   const int cb = kBrick / mc, nrows = cb * cb;
   const int64_t n = p.n;
-  // bricks are claimed from a work counter: a block that meets a crowded brick takes fewer bricks
-  if (tid == 0) {
-    s_brick[0] = blockIdx.x;
-    s_brick[1] = gridDim.x + atomicAdd(p.brick_ctr, 1);
-    s_fail = 0;
-  }
-  __syncthreads();
-  int64_t b = s_brick[0];
-  if (b >= nbricks) return;
-  if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    meta[0].pos = brick_pos(p, b, cb, p.ract, nullptr);
-    if (s_brick[1] < nbricks) meta[1].pos = brick_pos(p, s_brick[1], cb, p.ract, nullptr);
-    mbar_expect_tx(&bars[0], kPotBytes);
-  }
-  __syncthreads();
-  if (tid < nrows) meta_row(p, cb, meta[0], tid);
-  // a brick's potential window into buffer `buf`: one tensor copy of the box (x 24, y 22, z 22)
-  // of the padded potential that starts kPotPad - 4 / - 3 points before the owned points (the
-  // ghost points hold the periodic images, so the box never wraps)
-  auto issue = [&](const BrickPos &q, int buf) {
-    if (tid == 0) {
-      const int cx = (int)q.X0 - 4 + kPotPad, cy = (int)q.Y0 - 3 + kPotPad, cz = (int)q.Z0 - 3 + kPotPad;
-      const int cs = p.jobs[q.j].slot;
-      asm volatile(
-          "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-          "%5}], [%6];" ::"r"(smem_addr(pot0 + buf * kPotElems)),
-          "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(cx), "r"(cy), "r"(cz), "r"(cs), "r"(smem_addr(&bars[buf]))
-          : "memory");
-    }
+  const bool producer = tid < kFgGroup;
+  const int gt = producer ? tid : tid - kFgGroup;  // thread index in the group
+  const int lane = tid & 31;
+  if (blockIdx.x >= nbricks) return;
+  auto request = [&](const BrickPos &q) {  // thread 0: the potential window of brick q
+    mbar_expect_tx(&bar_pot, kPotBytes);
+    const int cx = (int)q.X0 - 4 + kPotPad, cy = (int)q.Y0 - 3 + kPotPad, cz = (int)q.Z0 - 3 + kPotPad;
+    const int cs = p.jobs[q.j].slot;
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_addr(pot)),
+        "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(cx), "r"(cy), "r"(cz), "r"(cs), "r"(smem_addr(&bar_pot))
+        : "memory");
   };
-  issue(meta[0].pos, 0);
-  if (tid == 0) mbar_arrive(&bars[0]);
+  if (tid == 0) {
+    mbar_init(&bar_pot, 1);
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&bar_full[b], kFgGroupWarps);
+      mbar_init(&bar_empty[b], kFgGroupWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+    s_next_id = blockIdx.x;
+    s_next = brick_pos(p, blockIdx.x, cb, p.ract, nullptr);
+    request(s_next);
+  }
   __syncthreads();
-  if (tid == 0) meta_scan(meta[0], nrows);
   const FDW w;
   float m = 0.f, vm0 = 0.f, vm1 = 0.f, vm2 = 0.f;
-  int fail_k = -1;         // the iteration whose wait gave up
-  bool fail_next = false;  // ... and whether it had issued the next brick's copies
-  constexpr int PY = kPotX, PZ = kPotX * kPotW;
-  for (int k = 0; b < nbricks; k++) {
-    const int cur = k & 1, nxt = cur ^ 1;
-    const bool has_next = s_brick[1] < nbricks;
-    if (tid == 0 && has_next) mbar_expect_tx(&bars[nxt], kPotBytes);
-    __syncthreads();  // (1) meta[cur] complete, buffer nxt no longer read, expect before the copies
-    if (has_next) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(meta[nxt].pos, nxt);
-      if (tid == 0) mbar_arrive(&bars[nxt]);
-    }
-    const BrickMeta &mt = meta[cur];
-    const BrickPos &q = mt.pos;
-    const MeshJob &J = p.jobs[q.j];
-    BrickRows br;
-    br.nrows = nrows;
-    br.total = mt.total;
-    br.cb = cb;
-    if (!mbar_wait_bounded(&bars[cur], (uint32_t)(k >> 1) & 1u)) s_fail = 1;
-    // force window: point (x, y, z) is mesh point (X0 - 1 + x, ...), potential (x + 3, y + 2, z + 2);
-    // a brick without particles needs only its owned points (for max |F|^2)
-    const float *pot = pot0 + cur * kPotElems;
-    const bool halo = br.total > 0;
-    for (int e = tid; e < kFor3; e += kFgThreads) {
-      const int x = e % kForW, y = (e / kForW) % kForW, z = e / (kForW * kForW);
-      const bool own = x >= 1 && x <= kBrick && y >= 1 && y <= kBrick && z >= 1 && z <= kBrick;
-      if (!own && !halo) continue;
-      const int c = (z + 2) * PZ + (y + 2) * PY + (x + 3);
-      const float fx = w(pot[c - 2], pot[c - 1], pot[c + 1], pot[c + 2]);
-      const float fy = w(pot[c - 2 * PY], pot[c - PY], pot[c + PY], pot[c + 2 * PY]);
-      const float fz = w(pot[c - 2 * PZ], pot[c - PZ], pot[c + PZ], pot[c + 2 * PZ]);
-      fw[e] = make_float4(fx, fy, fz, 0.f);
-      if (own) m = fmaxf(m, fx * fx + fy * fy + fz * fz);
-    }
-    if (has_next && tid < nrows) meta_row(p, cb, meta[nxt], tid);  // loads overlap the other warps' work
-    __syncthreads();  // (2) force window complete; a failed wait seen by all
-    if (s_fail) {
-      fail_k = k;
-      fail_next = has_next;
-      break;
-    }
-    if (tid == 0 && has_next) meta_scan(meta[nxt], nrows);
-    for (int kk = tid; kk < br.total; kk += kFgThreads) {
-      int di, dj, dk;
-      const int64_t ip = brick_particle(kk, br, mt.rbase, mt.rstart, mt.rcell, di, dj, dk);
-      const int16_t *qp = p.xp + 3 * ip;
-      float wx[3], wy[3], wz[3];
-      const int64_t ix = tsc(decode_pos(q.ci0 + di - p.ncb, qp[0]) * p.scale - J.off[0], wx) + p.shift;
-      const int64_t iy = tsc(decode_pos(q.cj0 + dj - p.ncb, qp[1]) * p.scale - J.off[1], wy) + p.shift;
-      const int64_t iz = tsc(decode_pos(q.ck0 + dk - p.ncb, qp[2]) * p.scale - J.off[2], wz) + p.shift;
-      // the stencil's first point ix - 1 lies at force-window index ix - X0
-      const int lx = (int)wrap_near(ix - q.X0, n), ly = (int)wrap_near(iy - q.Y0, n), lz = (int)wrap_near(iz - q.Z0, n);
-      float d0 = 0.f, d1 = 0.f, d2 = 0.f;
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-#pragma unroll
-        for (int bb = 0; bb < 3; bb++) {
-          const int row = ((lz + c) * kForW + (ly + bb)) * kForW + lx;
-#pragma unroll
-          for (int a = 0; a < 3; a++) {
-            const float wt = (wx[a] * wy[bb]) * wz[c];
-            const float4 f = fw[row + a];
-            d0 += f.x * wt;
-            d1 += f.y * wt;
-            d2 += f.z * wt;
-          }
+  int nreq = 1;  // tensor copies requested (thread 0)
+  int nok = 0;   // tensor copies waited for: the next one completes phase nok & 1 of bar_pot
+  if (producer) {
+    for (int k = 0;; k++) {
+      const int b = k & 1;
+      float *fw = fwb + b * 3 * kFor3;
+      BrickMeta &mt = meta[b];
+      // the consumers are done with buffer b (brick k - 2)
+      bool bad = k >= 2 && !mbar_wait_bounded(&bar_empty[b], (uint32_t)((k - 2) >> 1) & 1u);
+      const bool stop = group_any(1, bad);
+      const int64_t id = s_next_id;  // thread 0 wrote it before the barrier above
+      if (stop || id >= nbricks) {
+        // no more bricks (or a wait gave up): the consumers stop at this buffer
+        if (gt == 0) {
+          mt.total = -1;
+          if (bad) s_fail = 1;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bar_full[b]);
+        break;
+      }
+      if (gt == 0) mt.pos = s_next;
+      group_any(1, false);  // mt.pos visible to the group
+      if (gt < nrows) meta_row(p, cb, mt, gt);
+      // this brick's potential window
+      bad = !mbar_wait_bounded(&bar_pot, (uint32_t)nok & 1u);
+      if (!bad) nok++;
+      if (group_any(1, bad)) {
+        if (gt == 0) {
+          mt.total = -1;
+          s_fail = 1;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bar_full[b]);
+        break;
+      }
+      constexpr int PY = kPotX, PZ = kPotX * kPotW;
+      for (int e = gt; e < kFor3; e += kFgGroup) {
+        const int x = e % kForW, y = (e / kForW) % kForW, z = e / (kForW * kForW);
+        const int c = (z + 2) * PZ + (y + 2) * PY + (x + 3);
+        const float fx = w(pot[c - 2], pot[c - 1], pot[c + 1], pot[c + 2]);
+        const float fy = w(pot[c - 2 * PY], pot[c - PY], pot[c + PY], pot[c + 2 * PY]);
+        const float fz = w(pot[c - 2 * PZ], pot[c - PZ], pot[c + PZ], pot[c + 2 * PZ]);
+        fw[e] = fx;
+        fw[kFor3 + e] = fy;
+        fw[2 * kFor3 + e] = fz;
+        if (x >= 1 && x <= kBrick && y >= 1 && y <= kBrick && z >= 1 && z <= kBrick)
+          m = fmaxf(m, fx * fx + fy * fy + fz * fz);
+      }
+      group_any(1, false);  // the window is read, the force buffer and the row counts written
+      if (gt == 0) {
+        meta_scan(mt, nrows);
+        // claim and request the next brick (the window buffer is free)
+        const int64_t nid = gridDim.x + atomicAdd(p.brick_ctr, 1);
+        s_next_id = nid;
+        if (nid < nbricks) {
+          s_next = brick_pos(p, nid, cb, p.ract, nullptr);
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          request(s_next);
+          nreq++;
         }
       }
-      float *v = p.vp + 3 * ip;
-      const float v0 = v[0] + d0 * p.kick, v1 = v[1] + d1 * p.kick, v2 = v[2] + d2 * p.kick;
-      v[0] = v0;
-      v[1] = v1;
-      v[2] = v2;
-      vm0 = fmaxf(vm0, fabsf(v0));
-      vm1 = fmaxf(vm1, fabsf(v1));
-      vm2 = fmaxf(vm2, fabsf(v2));
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bar_full[b]);
     }
-    __syncthreads();  // (3) the force window, meta[cur] and buffer cur are reused
-    if (tid == 0) {
-      const int64_t b2 = has_next ? gridDim.x + atomicAdd(p.brick_ctr, 1) : nbricks;
-      if (b2 < nbricks) meta[cur].pos = brick_pos(p, b2, cb, p.ract, nullptr);
-      s_brick[0] = s_brick[1];
-      s_brick[1] = b2;
+    // a tensor copy still in flight (a wait gave up) lands before the block's memory is released
+    if (gt == 0 && nreq > nok) (void)mbar_wait_bounded(&bar_pot, (uint32_t)nok & 1u);
+  } else {
+    for (int k = 0;; k++) {
+      const int b = k & 1;
+      const float *fw = fwb + b * 3 * kFor3;
+      const bool bad = !mbar_wait_bounded(&bar_full[b], (uint32_t)(k >> 1) & 1u);
+      if (group_any(2, bad)) {
+        if (gt == 0) s_fail = 1;
+        break;
+      }
+      const BrickMeta &mt = meta[b];
+      if (mt.total < 0) break;
+      const BrickPos &q = mt.pos;
+      const MeshJob &J = p.jobs[q.j];
+      BrickRows br;
+      br.nrows = nrows;
+      br.total = mt.total;
+      br.cb = cb;
+      for (int kk = gt; kk < br.total; kk += kFgGroup) {
+        int di, dj, dk;
+        const int64_t ip = brick_particle(kk, br, mt.rbase, mt.rstart, mt.rcell, di, dj, dk);
+        const int16_t *qp = p.xp + 3 * ip;
+        float wx[3], wy[3], wz[3];
+        const int64_t ix = tsc(decode_pos(q.ci0 + di - p.ncb, qp[0]) * p.scale - J.off[0], wx) + p.shift;
+        const int64_t iy = tsc(decode_pos(q.cj0 + dj - p.ncb, qp[1]) * p.scale - J.off[1], wy) + p.shift;
+        const int64_t iz = tsc(decode_pos(q.ck0 + dk - p.ncb, qp[2]) * p.scale - J.off[2], wz) + p.shift;
+        // the stencil's first point ix - 1 lies at force-window index ix - X0
+        const int lx = (int)wrap_near(ix - q.X0, n), ly = (int)wrap_near(iy - q.Y0, n),
+                  lz = (int)wrap_near(iz - q.Z0, n);
+        float d0 = 0.f, d1 = 0.f, d2 = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+#pragma unroll
+          for (int bb = 0; bb < 3; bb++) {
+            const int row = ((lz + c) * kForW + (ly + bb)) * kForW + lx;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+              const float wt = (wx[a] * wy[bb]) * wz[c];
+              d0 += fw[row + a] * wt;
+              d1 += fw[kFor3 + row + a] * wt;
+              d2 += fw[2 * kFor3 + row + a] * wt;
+            }
+          }
+        }
+        float *v = p.vp + 3 * ip;
+        const float v0 = v[0] + d0 * p.kick, v1 = v[1] + d1 * p.kick, v2 = v[2] + d2 * p.kick;
+        v[0] = v0;
+        v[1] = v1;
+        v[2] = v2;
+        vm0 = fmaxf(vm0, fabsf(v0));
+        vm1 = fmaxf(vm1, fabsf(v1));
+        vm2 = fmaxf(vm2, fabsf(v2));
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bar_empty[b]);
     }
-    __syncthreads();
-    b = s_brick[0];
   }
-  if (fail_k >= 0) {
-    // a wait gave up: record it, and wait once more (also bounded) for the copies in flight
-    // before the block's shared memory is released
-    if (tid == 0 && p.err) atomicOr(p.err, 1 << CUBE_ERR_TIMEOUT);
-    (void)mbar_wait_bounded(&bars[fail_k & 1], (uint32_t)(fail_k >> 1) & 1u);
-    if (fail_next) (void)mbar_wait_bounded(&bars[(fail_k + 1) & 1], (uint32_t)((fail_k + 1) >> 1) & 1u);
-  }
+  __syncthreads();
+  if (tid == 0 && s_fail && p.err) atomicOr(p.err, 1 << CUBE_ERR_TIMEOUT);
   // one update of each maximum per block
-  const int warp = tid >> 5, lane = tid & 31;
+  const int warp = tid >> 5;
   m = warp_max(m);
   vm0 = warp_max(vm0);
   vm1 = warp_max(vm1);
