@@ -441,8 +441,11 @@ __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+// arrive on the mbarrier and expect `bytes` of asynchronous copies in the same phase
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+                   smem_addr(bar)),
+               "r"(bytes)
                : "memory");
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
@@ -575,7 +578,7 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
   const int lane = tid & 31;
   if (blockIdx.x >= nbricks) return;
   auto request = [&](const BrickPos &q) {  // thread 0: the potential window of brick q
-    mbar_expect_tx(&bar_pot, kPotBytes);
+    mbar_arrive_expect_tx(&bar_pot, kPotBytes);  // the phase completes when the bytes have landed
     const int cx = (int)q.X0 - 4 + kPotPad, cy = (int)q.Y0 - 3 + kPotPad, cz = (int)q.Z0 - 3 + kPotPad;
     const int cs = p.jobs[q.j].slot;
     asm volatile(
