@@ -485,9 +485,9 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 }
 
 // Force and gather in one pass, persistent and warp-specialised: one 1024-thread block per SM
-// claims bricks from a work counter.  Its 16 producer warps compute a brick's force window
-// while its 16 consumer warps gather the previous brick, so the two phases overlap instead of
-// alternating behind block barriers.
+// claims bricks from a work counter.  Its producer warps (the first kFgProd threads) compute a
+// brick's force window while its consumer warps gather the previous brick, so the two phases
+// overlap instead of alternating behind block barriers.
 //   producers: the brick's potential window (the brick plus three points on every side; along
 //     x widened to whole 16-byte groups) arrives by one 4-d tensor copy of the ghost-padded
 //     potential (cp.async.bulk.tensor, the ghost points hold the periodic images so the box
@@ -502,8 +502,12 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 // The arithmetic (weights, products, summation order) is the one of k_force_zm followed by
 // k_gather, and the force arrays never reach HBM.
 constexpr int kFgThreads = 1024;
-constexpr int kFgGroup = kFgThreads / 2;      // threads per group
-constexpr int kFgGroupWarps = kFgGroup / 32;  // mbarrier arrivals per hand-off
+#ifndef CUBE_FG_PRODUCERS
+#define CUBE_FG_PRODUCERS 512
+#endif
+constexpr int kFgProd = CUBE_FG_PRODUCERS;    // producer threads (the first warps of the block)
+constexpr int kFgCons = kFgThreads - kFgProd;  // consumer threads
+static_assert(kFgProd % 32 == 0 && kFgProd >= 128 && kFgCons >= 128, "whole warps in both groups");
 constexpr int kPotX = kBrick + 8, kPotW = kBrick + 6;  // potential window: x 24, y and z 22
 constexpr int kForW = kBrick + 2;                      // force window 18^3
 constexpr int kPotElems = kPotW * kPotW * kPotX;
@@ -544,8 +548,8 @@ __device__ __forceinline__ void meta_scan(BrickMeta &mt, int nrows) {
   mt.total = acc;
 }
 
-// barrier of one group (named barrier `id`, kFgGroup threads) that also ORs a flag over the group
-__device__ __forceinline__ bool group_any(int id, bool v) {
+// barrier of one group (named barrier `id`, `count` threads) that also ORs a flag over the group
+__device__ __forceinline__ bool group_any(int id, int count, bool v) {
   uint32_t r;
   asm volatile(
       "{\n\t.reg .pred p, q;\n\t"
@@ -553,7 +557,7 @@ __device__ __forceinline__ bool group_any(int id, bool v) {
       "bar.red.or.pred q, %2, %3, p;\n\t"
       "selp.u32 %0, 1, 0, q;\n\t}\n"
       : "=r"(r)
-      : "r"((uint32_t)v), "r"(id), "r"(kFgGroup)
+      : "r"((uint32_t)v), "r"(id), "r"(count)
       : "memory");
   return r != 0;
 }
@@ -573,8 +577,8 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
   const int tid = threadIdx.x;
   const int cb = kBrick / mc, nrows = cb * cb;
   const int64_t n = p.n;
-  const bool producer = tid < kFgGroup;
-  const int gt = producer ? tid : tid - kFgGroup;  // thread index in the group
+  const bool producer = tid < kFgProd;
+  const int gt = producer ? tid : tid - kFgProd;  // thread index in the group
   const int lane = tid & 31;
   if (blockIdx.x >= nbricks) return;
   auto request = [&](const BrickPos &q) {  // thread 0: the potential window of brick q
@@ -590,8 +594,8 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
   if (tid == 0) {
     mbar_init(&bar_pot, 1);
     for (int b = 0; b < 2; b++) {
-      mbar_init(&bar_full[b], kFgGroupWarps);
-      mbar_init(&bar_empty[b], kFgGroupWarps);
+      mbar_init(&bar_full[b], kFgProd / 32);
+      mbar_init(&bar_empty[b], kFgCons / 32);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_fail = 0;
@@ -611,7 +615,7 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
       BrickMeta &mt = meta[b];
       // the consumers are done with buffer b (brick k - 2)
       bool bad = k >= 2 && !mbar_wait_bounded(&bar_empty[b], (uint32_t)((k - 2) >> 1) & 1u);
-      const bool stop = group_any(1, bad);
+      const bool stop = group_any(1, kFgProd, bad);
       const int64_t id = s_next_id;  // thread 0 wrote it before the barrier above
       if (stop || id >= nbricks) {
         // no more bricks (or a wait gave up): the consumers stop at this buffer
@@ -624,12 +628,12 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
         break;
       }
       if (gt == 0) mt.pos = s_next;
-      group_any(1, false);  // mt.pos visible to the group
+      group_any(1, kFgProd, false);  // mt.pos visible to the group
       if (gt < nrows) meta_row(p, cb, mt, gt);
       // this brick's potential window
       bad = !mbar_wait_bounded(&bar_pot, (uint32_t)nok & 1u);
       if (!bad) nok++;
-      if (group_any(1, bad)) {
+      if (group_any(1, kFgProd, bad)) {
         if (gt == 0) {
           mt.total = -1;
           s_fail = 1;
@@ -639,7 +643,7 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
         break;
       }
       constexpr int PY = kPotX, PZ = kPotX * kPotW;
-      for (int e = gt; e < kFor3; e += kFgGroup) {
+      for (int e = gt; e < kFor3; e += kFgProd) {
         const int x = e % kForW, y = (e / kForW) % kForW, z = e / (kForW * kForW);
         const int c = (z + 2) * PZ + (y + 2) * PY + (x + 3);
         const float fx = w(pot[c - 2], pot[c - 1], pot[c + 1], pot[c + 2]);
@@ -651,7 +655,7 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
         if (x >= 1 && x <= kBrick && y >= 1 && y <= kBrick && z >= 1 && z <= kBrick)
           m = fmaxf(m, fx * fx + fy * fy + fz * fz);
       }
-      group_any(1, false);  // the window is read, the force buffer and the row counts written
+      group_any(1, kFgProd, false);  // the window is read, the force buffer and the row counts written
       if (gt == 0) {
         meta_scan(mt, nrows);
         // claim and request the next brick (the window buffer is free)
@@ -674,7 +678,7 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
       const int b = k & 1;
       const float *fw = fwb + b * 3 * kFor3;
       const bool bad = !mbar_wait_bounded(&bar_full[b], (uint32_t)(k >> 1) & 1u);
-      if (group_any(2, bad)) {
+      if (group_any(2, kFgCons, bad)) {
         if (gt == 0) s_fail = 1;
         break;
       }
@@ -686,7 +690,7 @@ __global__ void __launch_bounds__(kFgThreads, 1) k_force_gather(PM3K p, int mc, 
       br.nrows = nrows;
       br.total = mt.total;
       br.cb = cb;
-      for (int kk = gt; kk < br.total; kk += kFgGroup) {
+      for (int kk = gt; kk < br.total; kk += kFgCons) {
         int di, dj, dk;
         const int64_t ip = brick_particle(kk, br, mt.rbase, mt.rstart, mt.rcell, di, dj, dk);
         const int16_t *qp = p.xp + 3 * ip;
