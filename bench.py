@@ -320,6 +320,20 @@ def run_ours(args, rank, world, local_rank):
                 "traffic": float(PP_DRAM_BYTES_PER_STORED * img.n_used),
                 "traffic_source": "ncu DRAM bytes of k_pp_force on clustered192, scaled by stored particles"}
 
+    # the whole kick against its roofline model: algorithmic bytes B = 64 B per particle + 66 B per
+    # mesh point (binning 16, deposit 6, PP 12, gather 6, velocity 24 B per particle; deposit 4,
+    # R2C 8, k-space 18, inverse transforms 24, gather 12 B per mesh point) and F = 38 FLOP per
+    # accepted pair, each at its measured peak; frac = (B / BW + F / FP32) / time per kick
+    n_mesh = (w["box"] * w["rsf"]) ** 3 * L.nnt ** 3 if batch else (L.ng * w["rsf"]) ** 3
+    kick_bytes = 64.0 * N + 66.0 * n_mesh
+    hbm_peak, hbm_src = measured_hbm_peak()
+    t_model = kick_bytes / (hbm_peak * 1e9) + flops / (fp32_peak * 1e12)
+    roofline_kick = {"bound": "hbm + fp32", "bytes": kick_bytes, "flops": float(flops),
+                     "model_ms": 1e3 * t_model, "ms": ms_step, "frac": 1e3 * t_model / ms_step,
+                     "peaks": {"hbm_gbs": hbm_peak, "hbm_source": hbm_src, "fp32_tflops": fp32_peak},
+                     "what": "B / BW + F / FP32 over the kick's time: 64 B per particle + 66 B per mesh point, "
+                             "38 FLOP per accepted PP pair"}
+
     loop = per_box_loop(args.workload, fk, img, stream, a_mid, dt, ms_step) if batch and rank == 0 else None
     if batch:
         fk.configure()
@@ -370,7 +384,7 @@ def run_ours(args, rank, world, local_rank):
                               if batch else "inputs larger than L2 (mesh 512^3 fp32 = 537 MB, particle arrays > 120 MB)")},
             "stages_ms": {"pm3": pm3_ms, "pp_binning_and_worklist": ppb_ms, "pp_force": ppf_ms,
                           "note": "the PP binning and work list run on a second stream beside PM3"},
-            "roofline": roofline, "force_error": truth, "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": roofline, "roofline_kick": roofline_kick, "force_error": truth, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": ck, "cpu_baseline": cpu, "graph": graph, "pp_shape": pp_shape, "drift": drift, "learned": learned,
             "conservation": conservation, "batch": batch_obj}
     if loop is not None:
