@@ -109,6 +109,7 @@ struct Ctx {
   Buf fb_out;                  // learned-shell fallback statistics
   Buf phi_pad;                 // padded potential of the brick kernels
   Buf brick_ctr;               // their work counter
+  Buf dep_items;               // the brick deposit's work list
   cudaEvent_t tune_ev[2 * kMaxPPShapes] = {};
   void *h_stage = nullptr;  // pinned staging for small tables
   size_t h_stage_cap = 0;
@@ -548,6 +549,11 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       CK(grow(g.brick_ctr, sizeof(int32_t) * 64));
       a.brick_ctr = (int32_t *)g.brick_ctr.p;
     }
+    {
+      CK(grow(g.dep_items, pm3_dep_items_bytes((int64_t)a.rdep[0] * a.rdep[1] * a.rdep[2], a.njobs, d.n_used)));
+      a.dep_items = (int2 *)g.dep_items.p;
+      a.n_particles_hint = d.n_used;
+    }
     cufftHandle fw, bw;
     CK(get_plan(n, nslots, CUFFT_R2C, &fw));
     if (fused) CK(get_plan_padded_c2r(n, nslots, kPotPad, &bw));
@@ -559,11 +565,10 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
         CK(wait_xp(g.stream, k));
         at.jobs = (const MeshJob *)g.jobs.p + g.grp_lo[k];
         at.njobs = g.grp_lo[k + 1] - g.grp_lo[k];
-        launch_pm3_deposit(at, g.stream);
+        g.launches += launch_pm3_deposit(at, g.stream);
       }
-      g.launches += g.ngrp - 1;
     } else {
-      launch_pm3_deposit(a, g.stream);
+      g.launches += launch_pm3_deposit(a, g.stream);
     }
     CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
     launch_pm3_kspace(a, g.stream);
@@ -597,7 +602,7 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       CK(wait_vp());
       gather(a);
     }
-    g.launches += 4;
+    g.launches += 3;  // k-space, then ghosts + force-gather or force + gather
     CU(cudaGetLastError());
     return CUBE_OK;
   }
@@ -2049,6 +2054,7 @@ void c_pm3_fft_finalize(void) {
   release(g.force);
   release(g.phi_pad);
   release(g.brick_ctr);
+  release(g.dep_items);
   release(g.jobs);
   release(g.mlp_pos);
   release(g.mlp_rho);

@@ -206,9 +206,13 @@ struct PM3Args {
   int num_sms = 148;
   float *phi_pad = nullptr;  // the potential with kPotPad ghost points per side (periodic images), [nslots][(n+2P)^3]
   int32_t *brick_ctr = nullptr;  // work counter of the brick kernels (one int, zeroed by the launcher)
+  int2 *dep_items = nullptr;      // deposit work list: pm3_dep_items_bytes(...) of scratch
+  int64_t n_particles_hint = 0;   // stored particles (sizes the deposit work list)
 };
+// scratch of the deposit work list for a launch over `njobs` jobs of `cells` coarse cells each
+size_t pm3_dep_items_bytes(int64_t cells_per_job, int njobs, int64_t n_used);
 constexpr int kPotPad = 4;  // ghost points per side of the padded potential of the brick kernels
-void launch_pm3_deposit(const PM3Args &a, cudaStream_t s);
+int launch_pm3_deposit(const PM3Args &a, cudaStream_t s);  // returns the kernels it launched
 void launch_pm3_kspace(const PM3Args &a, cudaStream_t s);
 void launch_pm3_force(const PM3Args &a, cudaStream_t s);  // force arrays + f2max from the potential
 void launch_pm3_gather(const PM3Args &a, cudaStream_t s);

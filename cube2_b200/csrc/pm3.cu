@@ -821,24 +821,60 @@ constexpr int kDepThreads = 256;
 constexpr int kAccX = kBrick + 8;  // x window owned - 4 .. owned + kBrick + 3: whole float4 groups
 constexpr int kAccW = kBrick + 2;  // y, z window owned - 1 .. owned + kBrick
 
-__global__ void __launch_bounds__(kDepThreads) k_deposit_brick(PM3K p, int mc) {
+constexpr int kDepChunk = 2048;  // particles of one deposit work item (a crowded brick makes several)
+
+// The deposit's work list: every brick with particles makes ceil(particles / kDepChunk) items
+// (brick, chunk, chunks), so a crowded brick is spread over several blocks whose windows add up
+// in the mesh; empty bricks make none.  One thread per brick; items[0..count) in any order.
+__global__ void k_dep_items(PM3K p, int mc, int64_t nbricks, int chunk, int2 *items, int *count, int64_t cap) {
+  const int cb = kBrick / mc;
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nbricks;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    const BrickPos q = brick_pos(p, b, cb, p.rdep, p.rdep);
+    const int64_t t = p.jobs[q.j].t;
+    int total = 0;
+    for (int k = 0; k < cb; k++)
+      for (int j = 0; j < cb; j++) {
+        const int32_t *r = p.rhoc + ((t * p.nte + q.ck0 + k) * p.nte + q.cj0 + j) * p.nte + q.ci0;
+        for (int i = 0; i < cb; i++) total += r[i];
+      }
+    if (total == 0) continue;
+    const int nch = min((total + chunk - 1) / chunk, 0x7fff);
+    const int at = atomicAdd(count, nch);
+    if (at + nch > cap) {  // more particles in the cells than stored: the cell counts are wrong
+      if (p.err) atomicOr(p.err, 1 << CUBE_ERR_CAPACITY);
+      continue;
+    }
+    for (int c = 0; c < nch; c++) items[at + c] = make_int2((int)b, c | (nch << 16));
+  }
+}
+
+__global__ void __launch_bounds__(kDepThreads) k_deposit_brick(PM3K p, int mc, const int2 *items, const int *count) {
   __shared__ __align__(16) unsigned acc[kAccW * kAccW * kAccX];
   __shared__ int64_t rbase[kMaxRowsPerBrick];
   __shared__ int rstart[kMaxRowsPerBrick + 1];
   __shared__ int rcell[kMaxRowsPerBrick * (kMaxCb + 1)];
+  int2 item = make_int2((int)blockIdx.x, 1 << 16);  // without a work list: one block per whole brick
+  if (items) {
+    if ((int)blockIdx.x >= min(*count, (int)gridDim.x)) return;
+    item = items[blockIdx.x];
+  }
+  const int chunk = item.y & 0xffff, nch = item.y >> 16;
   const int cb = kBrick / mc;
-  const BrickPos q = brick_pos(p, blockIdx.x, cb, p.rdep, p.rdep);
+  const BrickPos q = brick_pos(p, item.x, cb, p.rdep, p.rdep);
   const MeshJob &J = p.jobs[q.j];
   const int64_t n = p.n;
   for (int e = threadIdx.x; e < kAccW * kAccW * kAccX; e += kDepThreads) acc[e] = 0u;
   BrickRows br;
   brick_rows(p, J, cb, q.ci0, q.cj0, q.ck0, rbase, rstart, rcell, br);  // its barriers cover the zeroing
-  if (br.total == 0) return;  // nothing reaches the mesh from an empty brick
-  // fixed-point scale 2^e: total * 0.4219 * 2^e < 2^32
+  // this item's particles of the brick
+  const int k0 = (int)((int64_t)br.total * chunk / nch), k1 = (int)((int64_t)br.total * (chunk + 1) / nch);
+  if (k1 <= k0) return;
+  // fixed-point scale 2^e: particles * 0.4219 * 2^e < 2^32
   int e = 24;
-  while (e > 1 && (double)br.total * 0.421875 * (double)(1u << e) >= 4294967040.0) e--;
+  while (e > 1 && (double)(k1 - k0) * 0.421875 * (double)(1u << e) >= 4294967040.0) e--;
   const float fs = (float)(1u << e), inv = 1.0f / fs;
-  for (int k = threadIdx.x; k < br.total; k += kDepThreads) {
+  for (int k = k0 + threadIdx.x; k < k1; k += kDepThreads) {
     int di, dj, dk;
     const int64_t ip = brick_particle(k, br, rbase, rstart, rcell, di, dj, dk);
     const int16_t *qp = p.xp + 3 * ip;
@@ -910,17 +946,36 @@ static void set_smem_attr_once(const void *fn, size_t bytes) {
   if (dev >= 0 && dev < kDev) done[f][dev] = true;
 }
 
-void launch_pm3_deposit(const PM3Args &a, cudaStream_t s) {
+size_t pm3_dep_items_bytes(int64_t cells_per_job, int njobs, int64_t n_used) {
+  // bricks hold at least one coarse cell: one item per cell, plus one per kDepChunk particles, plus the count
+  return sizeof(int2) * ((size_t)cells_per_job * njobs + (size_t)(n_used / kDepChunk) + 2);
+}
+
+int launch_pm3_deposit(const PM3Args &a, cudaStream_t s) {
   PM3K p = make_k(a);
   const int mc = (a.n % 4 == 0) ? brick_mc(a, true) : 0;
   if (mc) {
+    constexpr int chunk = kDepChunk;
+    auto kern = k_deposit_brick;
     const int cb = kBrick / mc;
-    const int64_t blocks = (int64_t)(a.rdep[0] / cb) * (a.rdep[1] / cb) * (a.rdep[2] / cb) * a.njobs;
-    if (blocks > 0) k_deposit_brick<<<(unsigned)blocks, kDepThreads, 0, s>>>(p, mc);
-    return;
+    const int64_t nbricks = (int64_t)(a.rdep[0] / cb) * (a.rdep[1] / cb) * (a.rdep[2] / cb) * a.njobs;
+    if (nbricks <= 0) return 0;
+    if (!a.dep_items) {
+      kern<<<(unsigned)nbricks, kDepThreads, 0, s>>>(p, mc, nullptr, nullptr);
+      return 1;
+    }
+    // at most one item per brick plus one per `chunk` particles
+    const int64_t cap = nbricks + a.n_particles_hint / chunk + 1;
+    int *count = reinterpret_cast<int *>(a.dep_items + cap);
+    cudaMemsetAsync(count, 0, sizeof(int), s);
+    k_dep_items<<<(unsigned)std::min<int64_t>((nbricks + 255) / 256, 4096), 256, 0, s>>>(p, mc, nbricks, chunk,
+                                                                                       a.dep_items, count, cap);
+    kern<<<(unsigned)cap, kDepThreads, 0, s>>>(p, mc, a.dep_items, count);
+    return 2;
   }
   const int64_t warps = (int64_t)a.rdep[0] * a.rdep[1] * a.rdep[2] * a.njobs;
   k_deposit<<<(unsigned)((warps + kWarps - 1) / kWarps), kWarps * 32, 0, s>>>(p);
+  return 1;
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link to libcuda)
