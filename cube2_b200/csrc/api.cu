@@ -44,7 +44,8 @@ struct Plan {
   int n, batch;
   cufftType type;
   cufftHandle h;
-  int pad = 0;  // C2R into the interior of arrays with `pad` ghost points per side
+  int pad = 0;   // C2R into the interior of arrays with `pad` ghost points per side
+  int rank = 3;  // 3: whole meshes; 2: the x-y planes of meshes (batch = planes)
 };
 
 struct Ctx {
@@ -302,9 +303,33 @@ static int wait_vp() {
 }
 
 // C2R whose output lands in the interior of [batch][(n+2 pad)^3] arrays (advanced layout)
+// Two-dimensional transforms of `batch` consecutive x-y planes of side n: R2C from real planes
+// of n^2 points to half-spectrum planes of n (n/2 + 1); C2R back, into planes of n^2 points or,
+// with pad > 0, into the interior rows of planes of (n + 2 pad)^2 points.
+static int get_plan2d(int n, int batch, cufftType type, int pad, cufftHandle *out) {
+  for (auto &p : g.plans)
+    if (p.rank == 2 && p.n == n && p.batch == batch && p.type == type && p.pad == pad) {
+      CF(cufftSetStream(p.h, g.stream));
+      *out = p.h;
+      return CUBE_OK;
+    }
+  Plan p{n, batch, type, 0, pad, 2};
+  const int h = n / 2 + 1, m = n + 2 * pad;
+  int dims[2] = {n, n}, real[2] = {m, m}, cplx[2] = {n, h};
+  if (type == CUFFT_R2C) {
+    CF(cufftPlanMany(&p.h, 2, dims, real, 1, m * m, cplx, 1, n * h, CUFFT_R2C, batch));
+  } else {
+    CF(cufftPlanMany(&p.h, 2, dims, cplx, 1, n * h, real, 1, m * m, CUFFT_C2R, batch));
+  }
+  CF(cufftSetStream(p.h, g.stream));
+  g.plans.push_back(p);
+  *out = p.h;
+  return CUBE_OK;
+}
+
 static int get_plan_padded_c2r(int n, int batch, int pad, cufftHandle *out) {
   for (auto &p : g.plans)
-    if (p.n == n && p.batch == batch && p.type == CUFFT_C2R && p.pad == pad) {
+    if (p.rank == 3 && p.n == n && p.batch == batch && p.type == CUFFT_C2R && p.pad == pad) {
       CF(cufftSetStream(p.h, g.stream));
       *out = p.h;
       return CUBE_OK;
@@ -321,7 +346,7 @@ static int get_plan_padded_c2r(int n, int batch, int pad, cufftHandle *out) {
 
 static int get_plan(int n, int batch, cufftType type, cufftHandle *out) {
   for (auto &p : g.plans)
-    if (p.n == n && p.batch == batch && p.type == type && p.pad == 0) {
+    if (p.rank == 3 && p.n == n && p.batch == batch && p.type == type && p.pad == 0) {
       CF(cufftSetStream(p.h, g.stream));
       *out = p.h;
       return CUBE_OK;
@@ -554,10 +579,18 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       a.dep_items = (int2 *)g.dep_items.p;
       a.n_particles_hint = d.n_used;
     }
+    // k-space step: two-dimensional transforms of the x-y planes around the fused z step where
+    // the mesh side allows, otherwise three-dimensional transforms around the Green multiply
+    const bool zsplit = pm3_kspace_z_ok(n);
     cufftHandle fw, bw;
-    CK(get_plan(n, nslots, CUFFT_R2C, &fw));
-    if (fused) CK(get_plan_padded_c2r(n, nslots, kPotPad, &bw));
-    else CK(get_plan(n, nslots, CUFFT_C2R, &bw));
+    if (zsplit) {
+      CK(get_plan2d(n, n * nslots, CUFFT_R2C, 0, &fw));
+      CK(get_plan2d(n, fused ? n : n * nslots, CUFFT_C2R, fused ? kPotPad : 0, &bw));
+    } else {
+      CK(get_plan(n, nslots, CUFFT_R2C, &fw));
+      if (fused) CK(get_plan_padded_c2r(n, nslots, kPotPad, &bw));
+      else CK(get_plan(n, nslots, CUFFT_C2R, &bw));
+    }
     CU(cudaMemsetAsync(g.rho.p, 0, sizeof(float) * n3 * nslots, g.stream));
     if (g.xp_pending) {  // deposit each group of tiles as soon as its particles are on the device
       PM3Args at = a;
@@ -571,12 +604,18 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       g.launches += launch_pm3_deposit(a, g.stream);
     }
     CF(cufftExecR2C(fw, (cufftReal *)g.rho.p, (cufftComplex *)g.rhok.p));
-    launch_pm3_kspace(a, g.stream);
+    if (zsplit) launch_pm3_kspace_z(a, g.stream);
+    else launch_pm3_kspace(a, g.stream);
     if (fused) {
       // the potential into the interior of the padded array, then its periodic ghost points
       const int64_t mm = n + 2 * kPotPad;
       float *interior = a.phi_pad + (kPotPad * mm + kPotPad) * mm + kPotPad;
-      CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)interior));
+      if (zsplit) {  // plane transforms, one mesh at a time (the padded meshes are m^3 apart)
+        for (int sl = 0; sl < nslots; sl++)
+          CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p + (int64_t)sl * nk, (cufftReal *)(interior + sl * mm * mm * mm)));
+      } else {
+        CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)interior));
+      }
       launch_pm3_ghosts(a, g.stream);
     } else {
       CF(cufftExecC2R(bw, (cufftComplex *)g.rhok.p, (cufftReal *)g.rho.p));  // potential

@@ -214,6 +214,10 @@ size_t pm3_dep_items_bytes(int64_t cells_per_job, int njobs, int64_t n_used);
 constexpr int kPotPad = 4;  // ghost points per side of the padded potential of the brick kernels
 int launch_pm3_deposit(const PM3Args &a, cudaStream_t s);  // returns the kernels it launched
 void launch_pm3_kspace(const PM3Args &a, cudaStream_t s);
+// the k-space step on the spectrum of two-dimensional x-y transforms: z transform, Green
+// multiply, inverse z transform (mesh sides where pm3_kspace_z_ok)
+bool pm3_kspace_z_ok(int n);
+void launch_pm3_kspace_z(const PM3Args &a, cudaStream_t s);
 void launch_pm3_force(const PM3Args &a, cudaStream_t s);  // force arrays + f2max from the potential
 void launch_pm3_gather(const PM3Args &a, cudaStream_t s);
 // periodic meshes: the force difference fused into the gather, brick by brick (no force arrays);

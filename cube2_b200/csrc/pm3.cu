@@ -796,6 +796,277 @@ void launch_pm3_kspace(const PM3Args &a, cudaStream_t s) {
   k_kspace<<<148 * 8, 256, 0, s>>>(p);
 }
 
+// ---------------------------------------------------------------------------------------------
+// k-space step fused along z.  After two-dimensional R2C transforms of the x-y planes, the
+// half-spectrum is laid out [z][ky][kx] (kx < n/2 + 1); every (kx, ky) column is transformed
+// along z, multiplied by the Green table (real), and transformed back, in one read and one write
+// of the spectrum (the three-dimensional path reads and writes it three times for the same:
+// the last forward pass, the k-space multiply and the first inverse pass).  The two-dimensional
+// C2R transforms of the planes then finish the inverse.
+//
+// The z transforms are iterative Stockham radix-8 FFTs in shared memory (Govindaraju et al.,
+// "High performance discrete Fourier transforms on graphics processors", SC 2008), with a
+// radix-4 or radix-2 last pass for lengths that are not powers of 8; twiddles exp(-2 pi i k/N)
+// are rounded from double precision.  The inverse runs as the forward transform of the complex
+// conjugate (G is real): conj(FFT(conj(X) G)).  Unnormalised, like cuFFT.
+constexpr int kZThreads = 512;
+constexpr int kZRows = 4;  // ky rows per block (the twiddle table is built once per block)
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }  // a * (-i)
+
+// 8-point DFT in place (decimation in frequency: radix-2 passes, outputs put back in order)
+__device__ __forceinline__ void dft8(float2 v[8]) {
+  constexpr float h = 0.70710678118654752f;  // sqrt(2) / 2
+  float2 a[8];
+  for (int k = 0; k < 4; k++) {
+    a[k] = cadd(v[k], v[k + 4]);
+    a[k + 4] = csub(v[k], v[k + 4]);
+  }
+  a[5] = make_float2(h * (a[5].x + a[5].y), h * (a[5].y - a[5].x));    // * exp(-i pi/4)
+  a[6] = mul_mi(a[6]);                                                 // * exp(-i pi/2)
+  a[7] = make_float2(h * (a[7].y - a[7].x), -h * (a[7].x + a[7].y));   // * exp(-3i pi/4)
+  float2 b[8];
+  for (int q = 0; q < 8; q += 4) {
+    b[q] = cadd(a[q], a[q + 2]);
+    b[q + 2] = csub(a[q], a[q + 2]);
+    b[q + 1] = cadd(a[q + 1], a[q + 3]);
+    b[q + 3] = mul_mi(csub(a[q + 1], a[q + 3]));
+  }
+  v[0] = cadd(b[0], b[1]);
+  v[4] = csub(b[0], b[1]);
+  v[2] = cadd(b[2], b[3]);
+  v[6] = csub(b[2], b[3]);
+  v[1] = cadd(b[4], b[5]);
+  v[5] = csub(b[4], b[5]);
+  v[3] = cadd(b[6], b[7]);
+  v[7] = csub(b[6], b[7]);
+}
+
+// One Stockham pass of radix R over the TX columns in s[z * TX + c]: butterfly j of column c
+// reads points j + r N/R, applies the twiddles of its position k = j mod Ns and writes the
+// R outputs to (j / Ns) Ns R + k + r Ns.
+template <int N, int TX, int R, int Ns>
+__device__ __forceinline__ void stockham_pass(float2 *s, const float2 *w) {
+  constexpr int kButterflies = N / R, kPer = kButterflies * TX / kZThreads;  // per thread
+  float2 v[kPer][R];
+  int dst[kPer];
+  const int c = threadIdx.x % TX;
+#pragma unroll
+  for (int u = 0; u < kPer; u++) {
+    const int j = threadIdx.x / TX + u * (kZThreads / TX);
+    const int k = j % Ns;
+#pragma unroll
+    for (int r = 0; r < R; r++) v[u][r] = s[(j + r * kButterflies) * TX + c];
+#pragma unroll
+    for (int r = 1; r < R; r++) v[u][r] = cmul(v[u][r], w[r * k * (N / (Ns * R))]);
+    if (R == 8) {
+      dft8(v[u]);
+    } else if (R == 4) {
+      const float2 a0 = cadd(v[u][0], v[u][2]), a2 = csub(v[u][0], v[u][2]), a1 = cadd(v[u][1], v[u][3]),
+                   a3 = mul_mi(csub(v[u][1], v[u][3]));
+      v[u][0] = cadd(a0, a1);
+      v[u][2] = csub(a0, a1);
+      v[u][1] = cadd(a2, a3);
+      v[u][3] = csub(a2, a3);
+    } else {
+      const float2 t = v[u][1];
+      v[u][1] = csub(v[u][0], t);
+      v[u][0] = cadd(v[u][0], t);
+    }
+    dst[u] = (j / Ns) * Ns * R + k;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < kPer; u++)
+#pragma unroll
+    for (int r = 0; r < R; r++) s[(dst[u] + r * Ns) * TX + c] = v[u][r];
+  __syncthreads();
+}
+
+// radix-8 passes while 8 Ns divides N, then one radix-4 or radix-2 pass
+template <int N, int TX, int Ns = 1>
+__device__ __forceinline__ void fft_columns(float2 *s, const float2 *w) {
+  if constexpr (Ns * 8 <= N) {
+    stockham_pass<N, TX, 8, Ns>(s, w);
+    fft_columns<N, TX, Ns * 8>(s, w);
+  } else if constexpr (Ns * 4 == N) {
+    stockham_pass<N, TX, 4, Ns>(s, w);
+  } else if constexpr (Ns * 2 == N) {
+    stockham_pass<N, TX, 2, Ns>(s, w);
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(kZThreads, 3) k_kspace_z(float2 *C, const float *G, float gscale) {
+  constexpr int H = N / 2 + 1, TX = kZThreads * 8 / N;
+  constexpr int64_t kPlane = (int64_t)N * H;  // z stride of the spectrum
+  __shared__ float2 s[N * TX];
+  __shared__ float2 w[N];
+  for (int k = threadIdx.x; k < N; k += kZThreads) {
+    double sn, cs;
+    sincospi(-2.0 * (double)k / (double)N, &sn, &cs);
+    w[k] = make_float2((float)cs, (float)sn);
+  }
+  const int kx0 = blockIdx.x * TX;
+  float2 *slot = C + (int64_t)blockIdx.z * N * kPlane;
+  for (int ky = blockIdx.y * kZRows; ky < min((int)(blockIdx.y + 1) * kZRows, N); ky++) {
+    float2 *col = slot + (int64_t)ky * H + kx0;
+    const float *g = G + (int64_t)ky * H + kx0;
+    __syncthreads();  // the previous row's stores have read s; the twiddles are written
+    constexpr int kPer = N * TX / kZThreads;  // points per thread
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {
+      const int e = threadIdx.x + u * kZThreads, z = e / TX, c = e % TX;
+      const bool in = kx0 + c < H;
+      s[e] = in ? col[z * kPlane + c] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    fft_columns<N, TX>(s, w);
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {
+      const int e = threadIdx.x + u * kZThreads;
+      const int z = e / TX, cc = e % TX;
+      const float gs = (kx0 + cc < H ? g[z * kPlane + cc] : 0.f) * gscale;
+      s[e] = make_float2(s[e].x * gs, -s[e].y * gs);  // conj(X) G
+    }
+    __syncthreads();
+    fft_columns<N, TX>(s, w);
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {
+      const int e = threadIdx.x + u * kZThreads, z = e / TX, c = e % TX;
+      if (kx0 + c < H) col[z * kPlane + c] = make_float2(s[e].x, -s[e].y);
+    }
+  }
+}
+
+// Mesh sides that are powers of 8 (64, 512): every pass is radix 8, so the first pass of each
+// transform reads its eight points straight from registers (loaded from the spectrum, or left
+// by the last forward pass: the last pass of a Stockham transform leaves point j + r N/8 with
+// butterfly j, which is what the first pass wants) and the last pass keeps its outputs in
+// registers; only the passes in between go through shared memory, double-buffered (two
+// barriers per transform).  Point z of column c sits in shared row z xor (bit 3 of z) (a
+// permutation of the rows), which spreads the first pass's stores over all banks for TX = 8.
+template <int N>
+struct Pow8 {
+  static constexpr int P = N == 64 ? 2 : (N == 512 ? 3 : 0);
+};
+template <int TX>
+__device__ __forceinline__ int zpos(int z, int c) {
+  return (z ^ ((z >> 3) & 1)) * TX + c;
+}
+
+// Radix-8 pass Ns of butterfly j on v (twiddles, then the 8-point DFT)
+template <int N, int Ns>
+__device__ __forceinline__ void r8_pass(float2 v[8], const float2 *w, int j) {
+  if constexpr (Ns > 1) {
+    const int k = j % Ns;
+#pragma unroll
+    for (int r = 1; r < 8; r++) v[r] = cmul(v[r], w[r * k * (N / (Ns * 8))]);
+  }
+  dft8(v);
+}
+template <int N, int TX, int Ns>
+__device__ __forceinline__ void r8_store(float2 *buf, const float2 v[8], int j, int c) {
+  const int d = (j / Ns) * Ns * 8 + j % Ns;
+#pragma unroll
+  for (int r = 0; r < 8; r++) buf[zpos<TX>(d + r * Ns, c)] = v[r];
+}
+template <int N, int TX>
+__device__ __forceinline__ void r8_load(const float2 *buf, float2 v[8], int j, int c) {
+#pragma unroll
+  for (int r = 0; r < 8; r++) v[r] = buf[zpos<TX>(j + r * (N / 8), c)];
+}
+// the transform of v (point j + r N/8 of column c), result in v at the same points.  Three
+// passes store to sa then sb and read them in that order; two passes store to and read sa.
+template <int N, int TX>
+__device__ __forceinline__ void fft8_regs(float2 v[8], float2 *sa, float2 *sb, const float2 *w, int j, int c) {
+  r8_pass<N, 1>(v, w, j);
+  r8_store<N, TX, 1>(sa, v, j, c);
+  __syncthreads();
+  r8_load<N, TX>(sa, v, j, c);
+  if constexpr (Pow8<N>::P == 3) {
+    r8_pass<N, 8>(v, w, j);
+    r8_store<N, TX, 8>(sb, v, j, c);
+    __syncthreads();
+    r8_load<N, TX>(sb, v, j, c);
+    r8_pass<N, 64>(v, w, j);
+  } else {
+    r8_pass<N, 8>(v, w, j);
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(kZThreads, 2) k_kspace_z8(float2 *C, const float *G, float gscale) {
+  constexpr int H = N / 2 + 1, TX = kZThreads * 8 / N;
+  constexpr int64_t kPlane = (int64_t)N * H;
+  constexpr int kBuf = N * TX;
+  extern __shared__ float2 zs[];
+  float2 *const sa = zs, *const sb = zs + kBuf, *const w = zs + 2 * kBuf;
+  for (int k = threadIdx.x; k < N; k += kZThreads) {
+    double sn, cs;
+    sincospi(-2.0 * (double)k / (double)N, &sn, &cs);
+    w[k] = make_float2((float)cs, (float)sn);
+  }
+  __syncthreads();
+  const int c = threadIdx.x % TX, j = threadIdx.x / TX, kx0 = blockIdx.x * TX;
+  const bool in = kx0 + c < H;
+  float2 *slot = C + (int64_t)blockIdx.z * N * kPlane;
+  for (int ky = blockIdx.y * kZRows; ky < min((int)(blockIdx.y + 1) * kZRows, N); ky++) {
+    float2 *col = slot + (int64_t)ky * H + kx0 + c;
+    const float *g = G + (int64_t)ky * H + kx0 + c;
+    float2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) v[r] = in ? col[(j + r * (N / 8)) * kPlane] : make_float2(0.f, 0.f);
+    fft8_regs<N, TX>(v, sa, sb, w, j, c);  // last read: sb (three passes) or sa (two)
+#pragma unroll
+    for (int r = 0; r < 8; r++) {  // conj(X) G
+      const float gs = (in ? g[(j + r * (N / 8)) * kPlane] : 0.f) * gscale;
+      v[r] = make_float2(v[r].x * gs, -v[r].y * gs);
+    }
+    // the inverse's first store goes to the buffer that no thread may still be reading
+    if constexpr (Pow8<N>::P == 3) fft8_regs<N, TX>(v, sa, sb, w, j, c);
+    else fft8_regs<N, TX>(v, sb, sa, w, j, c);
+    if (in) {
+#pragma unroll
+      for (int r = 0; r < 8; r++) col[(j + r * (N / 8)) * kPlane] = make_float2(v[r].x, -v[r].y);
+    }
+  }
+}
+constexpr size_t kz8_smem(int n) { return sizeof(float2) * (2 * (size_t)(n * (kZThreads * 8 / n)) + n); }
+
+bool pm3_kspace_z_ok(int n) { return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024; }
+
+static void set_smem_attr_once(const void *fn, size_t bytes);
+
+template <int N>
+static void launch_kz(const PM3K &p, cudaStream_t s) {
+  constexpr int TX = kZThreads * 8 / N;
+  const dim3 grid((unsigned)((N / 2 + 1 + TX - 1) / TX), (unsigned)((N + kZRows - 1) / kZRows), (unsigned)p.nslots);
+  if constexpr (Pow8<N>::P > 0) {
+    constexpr size_t smem = kz8_smem(N);
+    set_smem_attr_once((const void *)k_kspace_z8<N>, smem);
+    k_kspace_z8<N><<<grid, kZThreads, smem, s>>>(p.rhok, p.green, p.gscale);
+  } else {
+    k_kspace_z<N><<<grid, kZThreads, 0, s>>>(p.rhok, p.green, p.gscale);
+  }
+}
+
+void launch_pm3_kspace_z(const PM3Args &a, cudaStream_t s) {
+  PM3K p = make_k(a);
+  switch (a.n) {
+    case 64: launch_kz<64>(p, s); break;
+    case 128: launch_kz<128>(p, s); break;
+    case 256: launch_kz<256>(p, s); break;
+    case 512: launch_kz<512>(p, s); break;
+    default: launch_kz<1024>(p, s); break;
+  }
+}
+
 void launch_pm3_force(const PM3Args &a, cudaStream_t s) {
   PM3K p = make_k(a);
   if (a.n % 4 == 0) {
@@ -929,7 +1200,7 @@ int pm3_brick_mc(const PM3Args &a) { return brick_mc(a, false); }
 
 // the dynamic shared-memory limit of a kernel, raised once per device (the attribute is per device)
 static void set_smem_attr_once(const void *fn, size_t bytes) {
-  constexpr int kDev = 64, kFn = 8;
+  constexpr int kDev = 64, kFn = 16;
   static const void *fns[kFn] = {};
   static bool done[kFn][kDev] = {};
   int dev = 0;
