@@ -580,8 +580,10 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
       a.n_particles_hint = d.n_used;
     }
     // k-space step: two-dimensional transforms of the x-y planes around the fused z step where
-    // the mesh side allows, otherwise three-dimensional transforms around the Green multiply
-    const bool zsplit = pm3_kspace_z_ok(n);
+    // the mesh side allows, otherwise three-dimensional transforms around the Green multiply.
+    // Several padded meshes (one per tile) take the three-dimensional path: their planes are
+    // not equally spaced, and one plane C2R call per mesh costs more than it saves.
+    const bool zsplit = pm3_kspace_z_ok(n) && (!fused || nslots == 1);
     cufftHandle fw, bw;
     if (zsplit) {
       CK(get_plan2d(n, n * nslots, CUFFT_R2C, 0, &fw));
