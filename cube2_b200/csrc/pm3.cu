@@ -1135,7 +1135,8 @@ __global__ void __launch_bounds__(kDepThreads) k_deposit_brick(PM3K p, int mc, c
   const BrickPos q = brick_pos(p, item.x, cb, p.rdep, p.rdep);
   const MeshJob &J = p.jobs[q.j];
   const int64_t n = p.n;
-  for (int e = threadIdx.x; e < kAccW * kAccW * kAccX; e += kDepThreads) acc[e] = 0u;
+  for (int e4 = threadIdx.x; e4 < kAccW * kAccW * kAccX / 4; e4 += kDepThreads)
+    reinterpret_cast<uint4 *>(acc)[e4] = make_uint4(0u, 0u, 0u, 0u);
   BrickRows br;
   brick_rows(p, J, cb, q.ci0, q.cj0, q.ck0, rbase, rstart, rcell, br);  // its barriers cover the zeroing
   // this item's particles of the brick
@@ -1170,15 +1171,22 @@ __global__ void __launch_bounds__(kDepThreads) k_deposit_brick(PM3K p, int mc, c
     }
   }
   __syncthreads();
+  // Flush: lane (w, xg) of a warp takes x group xg (lane % 6) of window rows 5 pass + w (w < 5), so
+  // the group's mesh x index is worked out once and each row's once per pass.
   float *R = p.rho + (int64_t)J.slot * p.n3;
-  constexpr int G4 = kAccX / 4;
-  for (int e4 = threadIdx.x; e4 < kAccW * kAccW * G4; e4 += kDepThreads) {
-    const uint4 u = reinterpret_cast<const uint4 *>(acc)[e4];
-    if ((u.x | u.y | u.z | u.w) == 0u) continue;
-    const int xg = e4 % G4, y = (e4 / G4) % kAccW, z = e4 / (G4 * kAccW);
-    const int64_t gx = wrap_near(q.X0 - 4 + 4 * xg, n), gy = wrap_near(q.Y0 - 1 + y, n), gz = wrap_near(q.Z0 - 1 + z, n);
-    atomicAdd(reinterpret_cast<float4 *>(R + (gz * n + gy) * n + gx),
-              make_float4((float)u.x * inv, (float)u.y * inv, (float)u.z * inv, (float)u.w * inv));
+  constexpr int G4 = kAccX / 4, kRowsPerWarp = 32 / G4, kRows = kAccW * kAccW;
+  const int lane = threadIdx.x & 31, w = lane / G4, xg = lane - w * G4;
+  if (w < kRowsPerWarp) {
+    const int ni = (int)n;
+    auto wrap32 = [ni](int a) { return a < 0 ? a + ni : (a >= ni ? a - ni : a); };
+    const int gx = wrap32((int)q.X0 - 4 + 4 * xg);
+    for (int row = (threadIdx.x >> 5) * kRowsPerWarp + w; row < kRows; row += (kDepThreads / 32) * kRowsPerWarp) {
+      const uint4 u = reinterpret_cast<const uint4 *>(acc)[row * G4 + xg];
+      if ((u.x | u.y | u.z | u.w) == 0u) continue;
+      const int gy = wrap32((int)q.Y0 - 1 + row % kAccW), gz = wrap32((int)q.Z0 - 1 + row / kAccW);
+      atomicAdd(reinterpret_cast<float4 *>(R + ((int64_t)gz * ni + gy) * ni + gx),
+                make_float4((float)u.x * inv, (float)u.y * inv, (float)u.z * inv, (float)u.w * inv));
+    }
   }
 }
 
