@@ -49,6 +49,28 @@ def test_pm3_periodic_matches_restatement(gpu, case):
     assert pt.sum() == act.sum()
 
 
+@pytest.mark.parametrize("ng", [64, 128])
+def test_pm3_periodic_mesh_sides(gpu, ng):
+    """Periodic meshes of 128^3 and 256^3 (the k-space step of two-dimensional plane transforms
+    around the fused z transforms, all Stockham passes through shared memory) against the
+    restatement, on 20 000 uniform particles."""
+    from cube2_b200 import ic
+    from cube2_b200.kick import CUBE_PM3_PERIODIC, FineKick
+    from cube2_b200.layout import RATIO_SF, Layout, build_image, ixyz3_table
+    from oracle import oracle as O
+    L = Layout(ng=ng, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1)
+    pos, vel = ic.uniform_random(20000, float(ng), 11)
+    img = build_image(pos, vel, L)
+    fk = FineKick(L, pm3_mode=CUBE_PM3_PERIODIC, apm3f=4.0)
+    vp, f2, vmax, pt = fk.c_pm3_force_kernel(img, np.arange(1, L.ns3 + 1, dtype=np.int32), np.full(L.ns3, 2, np.int32),
+                                             ixyz3_table(L), RATIO_SF, 1.0, SIXPI, 1.0)
+    ref = O.pm3_periodic(img, 2, O.green(L.ng * 2, 4.0, 0.0, 0.5), 1.0, SIXPI, 1.0)
+    act = img.active
+    assert _rel_rms((vp - img.vp)[act].astype(np.float64), (ref["vp"] - img.vp)[act].astype(np.float64)) < TOL
+    assert abs(f2 - ref["f2max"]) <= 1e-5 * ref["f2max"]
+    np.testing.assert_allclose(vmax, ref["vmax"], rtol=1e-5)
+
+
 @pytest.mark.parametrize("mixed", [False, True])
 def test_pm3_subtile_matches_restatement(gpu, mixed):
     """Reference geometry: nft = nfp + 2 nfb meshes per subtile, range-limited Green tables
