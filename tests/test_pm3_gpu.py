@@ -71,6 +71,33 @@ def test_pm3_periodic_mesh_sides(gpu, ng):
     np.testing.assert_allclose(vmax, ref["vmax"], rtol=1e-5)
 
 
+def test_pm3_periodic_crowded_brick(gpu):
+    """A clump of 12 000 particles inside one brick of 16^3 mesh points (over 2048, so the
+    deposit splits the brick into several work items whose windows add up in the mesh), on
+    20 000 uniform ones, against the restatement."""
+    from cube2_b200 import ic
+    from cube2_b200.kick import CUBE_PM3_PERIODIC, FineKick
+    from cube2_b200.layout import RATIO_SF, Layout, build_image, ixyz3_table
+    from oracle import oracle as O
+    L = Layout(ng=64, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1)
+    pos, vel = ic.uniform_random(20000, 64.0, 12)
+    rng = np.random.default_rng(13)
+    clump = np.mod(np.array([20.3, 33.7, 41.1]) + 0.8 * rng.standard_normal((12000, 3)), 64.0)
+    pos = np.concatenate([pos, clump])
+    vel = np.concatenate([vel, (0.05 * rng.standard_normal((12000, 3))).astype(np.float32)])
+    brick = np.floor(pos / 8).astype(int)  # 16 mesh points = 8 fine cells at ratio_sf 2
+    assert np.bincount((brick[:, 2] * 8 + brick[:, 1]) * 8 + brick[:, 0]).max() > 2048
+    img = build_image(pos, vel, L)
+    fk = FineKick(L, pm3_mode=CUBE_PM3_PERIODIC, apm3f=4.0)
+    vp, f2, vmax, pt = fk.c_pm3_force_kernel(img, np.arange(1, L.ns3 + 1, dtype=np.int32), np.full(L.ns3, 2, np.int32),
+                                             ixyz3_table(L), RATIO_SF, 1.0, SIXPI, 1.0)
+    ref = O.pm3_periodic(img, 2, O.green(L.ng * 2, 4.0, 0.0, 0.5), 1.0, SIXPI, 1.0)
+    act = img.active
+    assert _rel_rms((vp - img.vp)[act].astype(np.float64), (ref["vp"] - img.vp)[act].astype(np.float64)) < TOL
+    assert abs(f2 - ref["f2max"]) <= 1e-5 * ref["f2max"]
+    np.testing.assert_allclose(vmax, ref["vmax"], rtol=1e-5)
+
+
 @pytest.mark.parametrize("mixed", [False, True])
 def test_pm3_subtile_matches_restatement(gpu, mixed):
     """Reference geometry: nft = nfp + 2 nfb meshes per subtile, range-limited Green tables
