@@ -21,7 +21,9 @@ cutoff 2 fine cells; see cube2_b200/workloads.py).
   the whole image per step.
 * ``batch``   the batched uneven boxes (batch512) in one kick, as a CUDA graph
   and against one kick call per box; ``conservation`` the FP64 momentum and
-  kinetic-energy change of one kick; ``drift`` and ``learned`` the other legs.
+  kinetic-energy change of one kick; ``drift`` and ``learned`` the other legs;
+  ``loop`` the 20-step kick-drift loop of 512^3 particles on a 1024^3 mesh
+  (loop512), plain and with the learned shell (``--no-loop`` skips it).
 """
 from __future__ import annotations
 
@@ -62,6 +64,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-loop", action="store_true")
     return ap.parse_args()
 
 
@@ -360,6 +363,18 @@ def run_ours(args, rank, world, local_rank):
             learned = {"error": repr(e)}
         fk.configure()
 
+    loop_obj = None
+    if not batch and rank == 0 and not args.no_loop:
+        # the 20-step kick-drift loop of 512^3 particles (plain, and with the learned shell)
+        try:
+            loop_obj = loop_leg("loop512", 20, max(args.warmup, 3), dev, stream, ("learned",))
+            loop_obj["what"] = ("drift + buffer_grid + buffer_x + kick + buffer_v per step on device-resident "
+                                "arrays (cube_drift_device, cube_kick_fine_device); the learned variant's P(k) "
+                                "against the plain loop's after the same steps")
+        except Exception as e:  # reported beside the kick, never instead of it
+            loop_obj = {"error": repr(e)}
+        fk.configure()
+
     cpu = None
     if batch:
         cpu = {"unavailable": "the reference CPU baseline is timed on the single-image workloads"}
@@ -386,7 +401,7 @@ def run_ours(args, rank, world, local_rank):
                           "note": "the PP binning and work list run on a second stream beside PM3"},
             "roofline": roofline, "roofline_kick": roofline_kick, "force_error": truth, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": ck, "cpu_baseline": cpu, "graph": graph, "pp_shape": pp_shape, "drift": drift, "learned": learned,
-            "conservation": conservation, "batch": batch_obj}
+            "conservation": conservation, "batch": batch_obj, "loop": loop_obj}
     if loop is not None:
         line["per_box_loop"] = loop
     if rank == 0:
@@ -789,25 +804,20 @@ def _timed_steps(loop, steps, stream):
     return ev[0][0].elapsed_time(ev[-1][2]) / max(steps, 1), drift / max(steps, 1), kick / max(steps, 1)
 
 
-def run_loop(args, rank, world, local_rank):
+def loop_leg(workload: str, steps: int, warmup: int, dev, stream, variant_names=("learned", "learned_lognormal_boxes",
+                                                                            "cutoff1_without_shell"), world: int = 1):
     """The kick-drift time loop (drift, buffer_grid, buffer_x, kick, buffer_v per step) on
     Zel'dovich initial conditions built on the device.  The plain loop (cutoff 2) is timed;
     the same start is then run with the learned shell (cutoff 1 + MLP) and with cutoff 1 alone,
     and the final states are compared with the plain one by CIC power-spectrum ratio (k up to
     k_Nyquist / 2 of the P(k) grid) and rms position difference."""
     import torch
-    import torch.distributed as dist
     from cube2_b200 import learned as Ln
     from cube2_b200 import loop as LP
     from cube2_b200 import workloads as W
     from cube2_b200.layout import Layout
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    if world > 1:
-        dist.init_process_group("nccl", device_id=dev)
-    w = W.LOOP_WORKLOADS[args.workload]
+    w = W.LOOP_WORKLOADS[workload]
     L = Layout(**w["layout"])
-    stream = torch.cuda.Stream(dev)
     t0 = time.perf_counter()
     di, dt, c = LP.start_with_growth(L, w["rms"], w["seed"], w["growth_per_step"], w["apm3f"], dev)
     torch.cuda.synchronize()
@@ -817,7 +827,7 @@ def run_loop(args, rank, world, local_rank):
     pk0 = di.power_spectrum(nw)
     start_learned, start_short = LP.clone_image(di), LP.clone_image(di)
     plain = LP.TimeLoop(di, w["apm3f"], coef=dt, dt_mid=dt, stream=stream)
-    for _ in range(max(args.warmup, 0)):
+    for _ in range(max(warmup, 0)):
         plain.step()
     torch.cuda.synchronize()
     if plain.error_word():
@@ -829,21 +839,21 @@ def run_loop(args, rank, world, local_rank):
         pass
     clocks = Clocks(uuid)
     if world > 1:
+        import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    ms, ms_drift, ms_kick = _timed_steps(plain, args.steps, stream)
+    ms, ms_drift, ms_kick = _timed_steps(plain, steps, stream)
     ck = clocks.stop()
     ms = max_over_ranks(ms, world, dev)
-    value = N * world / (ms * 1e-3)
     pk_plain = di.power_spectrum(nw)
     n_phys_ok = di.n_physical == N
 
     def run_variant(start, apm3f, shell=None, scale=1.0):
         lp = LP.TimeLoop(start, apm3f, coef=dt, dt_mid=dt, shell=shell, shell_scale=scale, stream=stream)
-        for _ in range(max(args.warmup, 0)):
+        for _ in range(max(warmup, 0)):
             lp.step()
-        m, md, mk = _timed_steps(lp, args.steps, stream)
+        m, md, mk = _timed_steps(lp, steps, stream)
         pk = start.power_spectrum(nw)
         kmax = nw // 4
         ok = (pk_plain["modes"] > 0) & (np.arange(pk_plain["modes"].size) >= 1) & (np.arange(pk_plain["modes"].size) <= kmax)
@@ -854,14 +864,14 @@ def run_loop(args, rank, world, local_rank):
                 "rms_position_difference_fine_cells": LP.rms_position_difference(start, di),
                 "within_1pct": bool(np.max(np.abs(ratio - 1.0)) <= 0.01), "error_word": lp.error_word()}
     variants = {}
-    if rank == 0 and not args.no_learned:
-        start_lognormal = LP.clone_image(start_learned)
+    start_lognormal = LP.clone_image(start_learned) if "learned_lognormal_boxes" in variant_names else None
+    if "learned" in variant_names:
         try:
             # the method's own snapshots: a 128^3 companion box of the same statistics (another seed),
             # every 5 steps of a plain loop as long as this one
             sl = dict(w["layout"], ng=128)
             snaps = LP.snapshots(Layout(**sl), w["rms"], w["seed"] + 7, w["growth_per_step"], w["apm3f"],
-                                 args.warmup + args.steps, 2, dev)
+                                 warmup + steps, 2, dev)
             shell, scale, tinfo = Ln.train_shell_on(snaps, dev, steps=12000,
                                                     fields="snapshots 0, 2, 4, ... of a plain 128^3 loop of the "
                                                     f"same statistics (seed {w['seed'] + 7})")
@@ -871,6 +881,7 @@ def run_loop(args, rank, world, local_rank):
             shell.close()
         except Exception as e:  # reported beside the plain loop, never instead of it
             variants["learned"] = {"error": repr(e)}
+    if start_lognormal is not None:
         try:
             shell, scale, tinfo = Ln.train_shell(dev)
             variants["learned_lognormal_boxes"] = run_variant(start_lognormal, 2.0, shell, scale)
@@ -878,24 +889,45 @@ def run_loop(args, rank, world, local_rank):
             shell.close()
         except Exception as e:
             variants["learned_lognormal_boxes"] = {"error": repr(e)}
+    if "cutoff1_without_shell" in variant_names:
         try:
             variants["cutoff1_without_shell"] = run_variant(start_short, 2.0)
         except Exception as e:
             variants["cutoff1_without_shell"] = {"error": repr(e)}
     growth = pk_plain["pk"][1:nw // 4 + 1] / pk0["pk"][1:nw // 4 + 1]
+    return {"workload": workload, "particles": N, "layout": L.as_dict(), "pm3_mesh": L.ng * 2,
+            "pp_cutoff_fine_cells": w["apm3f"] / 2, "growth_per_step": w["growth_per_step"], "dt": dt,
+            "growth_rate_c": c, "steps": steps, "warmup": warmup, "ms_per_step": ms, "value": N * world / (ms * 1e-3),
+            "unit": LOOP_UNIT, "stages_ms": {"drift_and_buffers": ms_drift, "kick_and_buffer_v": ms_kick},
+            "initial_conditions_seconds": t_ic, "particles_conserved": bool(n_phys_ok),
+            "pk_growth_plain": [round(float(x), 4) for x in growth[:8]], "pk_grid": nw, "variants": variants,
+            "clocks": ck}
+
+
+def run_loop(args, rank, world, local_rank):
+    """--workload loop*: the time loop as the bench line itself (see loop_leg)."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev)
+    stream = torch.cuda.Stream(dev)
+    names = () if (rank != 0 or args.no_learned) else ("learned", "learned_lognormal_boxes", "cutoff1_without_shell")
+    r = loop_leg(args.workload, args.steps, args.warmup, dev, stream, names, world)
     peak, src = measured_hbm_peak()
-    line = {"metric": LOOP_METRIC, "value": value, "unit": LOOP_UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+    line = {"metric": LOOP_METRIC, "value": r["value"], "unit": LOOP_UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32 (int16 fixed-point positions, fp64 Green table)",
             "data": "synthetic (Zel'dovich lattice, P(k) ~ k^-2, built on the device; see cube2_b200/loop.py)",
-            "config": {"workload": args.workload, "particles": N, "layout": L.as_dict(), "pm3_mesh": L.ng * 2,
-                       "pp_cutoff_fine_cells": w["apm3f"] / 2, "growth_per_step": w["growth_per_step"],
-                       "dt": dt, "growth_rate_c": c, "parallelism": f"replicas x{world}",
+            "config": {"workload": args.workload, "particles": r["particles"], "layout": r["layout"],
+                       "pm3_mesh": r["pm3_mesh"], "pp_cutoff_fine_cells": r["pp_cutoff_fine_cells"],
+                       "growth_per_step": r["growth_per_step"], "dt": r["dt"], "growth_rate_c": r["growth_rate_c"],
+                       "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (mesh 1024^3 fp32 = 4.3 GB, particle arrays > 3 GB)"},
-            "stages_ms": {"drift_and_buffers": ms_drift, "kick_and_buffer_v": ms_kick},
-            "initial_conditions_seconds": t_ic, "particles_conserved": bool(n_phys_ok),
-            "pk_growth_plain": [round(float(x), 4) for x in growth[:8]],
-            "pk_grid": nw, "variants": variants, "clocks": ck, "hbm_peak_gbs": peak,
+            "stages_ms": r["stages_ms"], "initial_conditions_seconds": r["initial_conditions_seconds"],
+            "particles_conserved": r["particles_conserved"], "pk_growth_plain": r["pk_growth_plain"],
+            "pk_grid": r["pk_grid"], "variants": r["variants"], "clocks": r["clocks"], "hbm_peak_gbs": peak,
             "e2e": {"unavailable": "the loop keeps the image on the device between steps; the host-array "
                                    "entry points (cube_kick_fine, cube_drift) are timed on the single-kick workloads"},
             "cpu_baseline": {"unavailable": "the reference loop is the Fortran driver (no Fortran compiler here)"}}
