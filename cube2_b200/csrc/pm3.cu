@@ -850,15 +850,15 @@ __device__ __forceinline__ void dft8(float2 v[8]) {
 // One Stockham pass of radix R over the TX columns in s[z * TX + c]: butterfly j of column c
 // reads points j + r N/R, applies the twiddles of its position k = j mod Ns and writes the
 // R outputs to (j / Ns) Ns R + k + r Ns.
-template <int N, int TX, int R, int Ns>
+template <int N, int TX, int R, int Ns, int T>
 __device__ __forceinline__ void stockham_pass(float2 *s, const float2 *w) {
-  constexpr int kButterflies = N / R, kPer = kButterflies * TX / kZThreads;  // per thread
+  constexpr int kButterflies = N / R, kPer = kButterflies * TX / T;  // per thread
   float2 v[kPer][R];
   int dst[kPer];
   const int c = threadIdx.x % TX;
 #pragma unroll
   for (int u = 0; u < kPer; u++) {
-    const int j = threadIdx.x / TX + u * (kZThreads / TX);
+    const int j = threadIdx.x / TX + u * (T / TX);
     const int k = j % Ns;
 #pragma unroll
     for (int r = 0; r < R; r++) v[u][r] = s[(j + r * kButterflies) * TX + c];
@@ -888,26 +888,34 @@ __device__ __forceinline__ void stockham_pass(float2 *s, const float2 *w) {
   __syncthreads();
 }
 
-// radix-8 passes while 8 Ns divides N, then one radix-4 or radix-2 pass
-template <int N, int TX, int Ns = 1>
+// radix-8 passes while 8 Ns divides N, then one radix-4 or radix-2 pass (T threads)
+template <int N, int TX, int T, int Ns = 1>
 __device__ __forceinline__ void fft_columns(float2 *s, const float2 *w) {
   if constexpr (Ns * 8 <= N) {
-    stockham_pass<N, TX, 8, Ns>(s, w);
-    fft_columns<N, TX, Ns * 8>(s, w);
+    stockham_pass<N, TX, 8, Ns, T>(s, w);
+    fft_columns<N, TX, T, Ns * 8>(s, w);
   } else if constexpr (Ns * 4 == N) {
-    stockham_pass<N, TX, 4, Ns>(s, w);
+    stockham_pass<N, TX, 4, Ns, T>(s, w);
   } else if constexpr (Ns * 2 == N) {
-    stockham_pass<N, TX, 2, Ns>(s, w);
+    stockham_pass<N, TX, 2, Ns, T>(s, w);
   }
 }
 
+// threads of the generic kernel: columns of eight points (64-byte rows of the spectrum)
 template <int N>
-__global__ void __launch_bounds__(kZThreads, 3) k_kspace_z(float2 *C, const float *G, float gscale) {
-  constexpr int H = N / 2 + 1, TX = kZThreads * 8 / N;
+struct ZThreads {
+  static constexpr int T = N >= 1024 ? 1024 : kZThreads;
+};
+
+template <int N>
+__global__ void __launch_bounds__(ZThreads<N>::T, (ZThreads<N>::T == 1024 ? 1 : 3))
+    k_kspace_z(float2 *C, const float *G, float gscale) {
+  constexpr int T = ZThreads<N>::T;
+  constexpr int H = N / 2 + 1, TX = T * 8 / N;
   constexpr int64_t kPlane = (int64_t)N * H;  // z stride of the spectrum
-  __shared__ float2 s[N * TX];
-  __shared__ float2 w[N];
-  for (int k = threadIdx.x; k < N; k += kZThreads) {
+  extern __shared__ float2 zg[];
+  float2 *const s = zg, *const w = zg + N * TX;
+  for (int k = threadIdx.x; k < N; k += T) {
     double sn, cs;
     sincospi(-2.0 * (double)k / (double)N, &sn, &cs);
     w[k] = make_float2((float)cs, (float)sn);
@@ -918,27 +926,27 @@ __global__ void __launch_bounds__(kZThreads, 3) k_kspace_z(float2 *C, const floa
     float2 *col = slot + (int64_t)ky * H + kx0;
     const float *g = G + (int64_t)ky * H + kx0;
     __syncthreads();  // the previous row's stores have read s; the twiddles are written
-    constexpr int kPer = N * TX / kZThreads;  // points per thread
+    constexpr int kPer = N * TX / T;  // points per thread
 #pragma unroll
     for (int u = 0; u < kPer; u++) {
-      const int e = threadIdx.x + u * kZThreads, z = e / TX, c = e % TX;
+      const int e = threadIdx.x + u * T, z = e / TX, c = e % TX;
       const bool in = kx0 + c < H;
       s[e] = in ? col[z * kPlane + c] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_columns<N, TX>(s, w);
+    fft_columns<N, TX, T>(s, w);
 #pragma unroll
     for (int u = 0; u < kPer; u++) {
-      const int e = threadIdx.x + u * kZThreads;
+      const int e = threadIdx.x + u * T;
       const int z = e / TX, cc = e % TX;
       const float gs = (kx0 + cc < H ? g[z * kPlane + cc] : 0.f) * gscale;
       s[e] = make_float2(s[e].x * gs, -s[e].y * gs);  // conj(X) G
     }
     __syncthreads();
-    fft_columns<N, TX>(s, w);
+    fft_columns<N, TX, T>(s, w);
 #pragma unroll
     for (int u = 0; u < kPer; u++) {
-      const int e = threadIdx.x + u * kZThreads, z = e / TX, c = e % TX;
+      const int e = threadIdx.x + u * T, z = e / TX, c = e % TX;
       if (kx0 + c < H) col[z * kPlane + c] = make_float2(s[e].x, -s[e].y);
     }
   }
@@ -1039,23 +1047,25 @@ __global__ void __launch_bounds__(kZThreads, 2) k_kspace_z8(float2 *C, const flo
 }
 constexpr size_t kz8_smem(int n) { return sizeof(float2) * (2 * (size_t)(n * (kZThreads * 8 / n)) + n); }
 
-// Mesh sides that take the fused z step.  At 1024 the generic kernel's columns are four points
-// wide (32-byte rows), and the three-dimensional path measured faster (7.39 against 7.63 ms for
-// a kick on a 1024^3 mesh).
-bool pm3_kspace_z_ok(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
+// Mesh sides that take the fused z step
+bool pm3_kspace_z_ok(int n) { return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024; }
 
 static void set_smem_attr_once(const void *fn, size_t bytes);
 
 template <int N>
 static void launch_kz(const PM3K &p, cudaStream_t s) {
-  constexpr int TX = kZThreads * 8 / N;
-  const dim3 grid((unsigned)((N / 2 + 1 + TX - 1) / TX), (unsigned)((N + kZRows - 1) / kZRows), (unsigned)p.nslots);
   if constexpr (Pow8<N>::P > 0) {
+    constexpr int TX = kZThreads * 8 / N;
+    const dim3 grid((unsigned)((N / 2 + 1 + TX - 1) / TX), (unsigned)((N + kZRows - 1) / kZRows), (unsigned)p.nslots);
     constexpr size_t smem = kz8_smem(N);
     set_smem_attr_once((const void *)k_kspace_z8<N>, smem);
     k_kspace_z8<N><<<grid, kZThreads, smem, s>>>(p.rhok, p.green, p.gscale);
   } else {
-    k_kspace_z<N><<<grid, kZThreads, 0, s>>>(p.rhok, p.green, p.gscale);
+    constexpr int T = ZThreads<N>::T, TX = T * 8 / N;
+    const dim3 grid((unsigned)((N / 2 + 1 + TX - 1) / TX), (unsigned)((N + kZRows - 1) / kZRows), (unsigned)p.nslots);
+    constexpr size_t smem = sizeof(float2) * (size_t)(N * TX + N);
+    set_smem_attr_once((const void *)k_kspace_z<N>, smem);
+    k_kspace_z<N><<<grid, T, smem, s>>>(p.rhok, p.green, p.gscale);
   }
 }
 
@@ -1066,6 +1076,7 @@ void launch_pm3_kspace_z(const PM3Args &a, cudaStream_t s) {
     case 128: launch_kz<128>(p, s); break;
     case 256: launch_kz<256>(p, s); break;
     case 512: launch_kz<512>(p, s); break;
+    case 1024: launch_kz<1024>(p, s); break;
     default: break;  // other sides take the three-dimensional path (pm3_kspace_z_ok)
   }
 }
