@@ -1061,21 +1061,32 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
   const int64_t nrows = (int64_t)L.ntile * L.nte * L.nte;
   const int64_t n_used = idx_b_r[nrows - 1];  // pm3_fft_cuda.cu:533-536
   if (n_used < 0 || n_used >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
-  // the spine must be non-decreasing and consistent with rhoc row sums
-  {
+  // The spine must be non-decreasing and consistent with the rhoc row sums.  The tile groups'
+  // bounds are checked before the uploads (they size the copies); the full check runs on the
+  // host while the copies are under way, and a failure returns before any kernel is launched,
+  // with the caller's arrays untouched.
+  const int64_t rows_per_tile = (int64_t)L.nte * L.nte;
+  for (int t = 1; t <= L.ntile; t++) {
+    const int64_t a = idx_b_r[(t - 1) * rows_per_tile], b = idx_b_r[t * rows_per_tile - 1];
+    const int64_t before = t > 1 ? idx_b_r[(t - 1) * rows_per_tile - 1] : 0;
+    if (a < before || b < a || b > n_used) return fail(CUBE_ERR_INVALID);
+  }
+  auto spine_ok = [&]() {
     int64_t prev = 0;
     for (int64_t r = 0; r < nrows; r++) {
       int64_t s = 0;
       for (int i = 0; i < L.nte; i++) {
         const int32_t c = rhoc[r * L.nte + i];
-        if (c < 0) return fail(CUBE_ERR_INVALID);
+        if (c < 0) return false;
         s += c;
       }
-      if (idx_b_r[r] - prev != s) return fail(CUBE_ERR_INVALID);
+      if (idx_b_r[r] - prev != s) return false;
       prev = idx_b_r[r];
     }
-  }
-  CK(ensure_device());
+    return true;
+  };
+  if (const int dst = ensure_device(); dst != CUBE_OK)  // no device: still report a bad spine as such
+    return spine_ok() ? dst : fail(CUBE_ERR_INVALID);
   CK(grow(g.xp, sizeof(int16_t) * 3 * (size_t)std::max<int64_t>(n_used, 1)));
   CK(grow(g.vp, sizeof(float) * 3 * (size_t)std::max<int64_t>(n_used, 1)));
   CK(grow(g.rhoc, sizeof(int32_t) * (size_t)nrows * L.nte));
@@ -1113,6 +1124,13 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
     }
     g.vp_tiles = g.ngrp;
     g.vp_pending = true;
+  }
+  if (!spine_ok()) {  // nothing launched yet: let the uploads finish and return
+    cudaStreamSynchronize(g.copy);
+    cudaStreamSynchronize(g.stream);
+    g.xp_pending = g.vp_pending = false;
+    g.xp_tiles = g.vp_tiles = 0;
+    return fail(CUBE_ERR_INVALID);
   }
   Dev d{(const int16_t *)g.xp.p, (const int32_t *)g.rhoc.p, (const int64_t *)g.idx.p, (float *)g.vp.p, n_used};
   d.h_vp = vp;
