@@ -302,7 +302,6 @@ static int wait_vp() {
   return CUBE_OK;
 }
 
-// C2R whose output lands in the interior of [batch][(n+2 pad)^3] arrays (advanced layout)
 // Two-dimensional transforms of `batch` consecutive x-y planes of side n: R2C from real planes
 // of n^2 points to half-spectrum planes of n (n/2 + 1); C2R back, into planes of n^2 points or,
 // with pad > 0, into the interior rows of planes of (n + 2 pad)^2 points.
@@ -327,6 +326,7 @@ static int get_plan2d(int n, int batch, cufftType type, int pad, cufftHandle *ou
   return CUBE_OK;
 }
 
+// C2R whose output lands in the interior of [batch][(n+2 pad)^3] arrays (advanced layout)
 static int get_plan_padded_c2r(int n, int batch, int pad, cufftHandle *out) {
   for (auto &p : g.plans)
     if (p.rank == 3 && p.n == n && p.batch == batch && p.type == CUFFT_C2R && p.pad == pad) {
