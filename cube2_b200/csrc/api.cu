@@ -71,6 +71,8 @@ struct Ctx {
   static_assert(kPipeGroups <= kMaxTileEvents, "one event of each kind per group");
   int ngrp = 0;
   int grp_lo[kMaxTileEvents + 1] = {};
+  int grp_order[kMaxTileEvents] = {};  // host kicks: groups by decreasing particle count (the
+                                       // order of vp uploads, gathers, PP launches and copies back)
   cudaEvent_t ev_tile[kMaxTileEvents] = {};  // per-group PP force done (host kicks)
   cudaEvent_t ev_copied = nullptr;           // last per-group vp copy enqueued
   bool vp_copied = false;                    // this host kick's vp is already on its way back
@@ -297,7 +299,8 @@ static int wait_xp(cudaStream_t st, int t = -1) {
 // order the compute stream after a pending vp upload
 static int wait_vp() {
   if (!g.vp_pending) return CUBE_OK;
-  CU(cudaStreamWaitEvent(g.stream, g.vp_tiles ? g.ev_vp[g.vp_tiles - 1] : g.vp_ready, 0));
+  // the group parts go up in grp_order: the last one recorded covers them all
+  CU(cudaStreamWaitEvent(g.stream, g.vp_tiles ? g.ev_vp[g.grp_order[g.vp_tiles - 1]] : g.vp_ready, 0));
   g.vp_pending = false;
   return CUBE_OK;
 }
@@ -629,7 +632,8 @@ static int run_pm3(const Meta &m, const int32_t *ires, const int32_t *ratio_sf, 
     };
     if (g.vp_pending && g.vp_tiles == g.ngrp && g.ngrp > 0) {  // gather each group once its vp is in
       PM3Args at = a;
-      for (int k = 0; k < g.ngrp; k++) {
+      for (int kk = 0; kk < g.ngrp; kk++) {
+        const int k = g.grp_order[kk];
         CU(cudaStreamWaitEvent(g.stream, g.ev_vp[k], 0));
         at.jobs = (const MeshJob *)g.jobs.p + g.grp_lo[k];
         at.njobs = g.grp_lo[k + 1] - g.grp_lo[k];
@@ -931,8 +935,9 @@ static int run_pp_force_tiles(const PPArgs &p, const Dev &d) {
   CU(cudaStreamWaitEvent(g.side2, g.ev_join, 0));  // binning (on side) done
   if (g.timing) CU(cudaEventRecord(g.ring[g.ring_cur][3], g.side));
   const int64_t rows = (int64_t)L.nte * L.nte;
-  for (int k = 0; k < g.ngrp; k++) {
-    cudaStream_t st = (k & 1) ? g.side2 : g.side;
+  for (int kk = 0; kk < g.ngrp; kk++) {
+    const int k = g.grp_order[kk];
+    cudaStream_t st = (kk & 1) ? g.side2 : g.side;
     CU(cudaStreamWaitEvent(st, g.ready_tiles ? g.ev_ready[k] : g.ev_pm3done, 0));
     launch_pp_force(p, st, g.grp_lo[k], g.grp_lo[k + 1]);
     g.launches += 1;
@@ -940,7 +945,8 @@ static int run_pp_force_tiles(const PPArgs &p, const Dev &d) {
     CU(cudaEventRecord(g.ev_tile[k], st));
   }
   // copies after all launches: a copy into pageable host memory returns only when done
-  for (int k = 0; k < g.ngrp; k++) {
+  for (int kk = 0; kk < g.ngrp; kk++) {
+    const int k = g.grp_order[kk];
     const int t0 = g.grp_lo[k], t1 = g.grp_lo[k + 1];
     const int64_t lo = t0 ? d.h_idx[t0 * rows - 1] : 0, hi = d.h_idx[t1 * rows - 1];
     if (hi <= lo) continue;
@@ -1113,8 +1119,21 @@ static int host_kick(const int32_t *ires, const int32_t *ixyz3, const int32_t *r
     }
     g.xp_pending = true;
     g.xp_tiles = g.ngrp;
-    // vp travels beside the deposit and FFTs, group by group; its users wait for their part
-    for (int k = 0; k < g.ngrp; k++) {
+    // The groups are gathered, kicked by PP and copied back largest first, so that the last
+    // PP launch and the last copy, which nothing overlaps, are the shortest.
+    {
+      int64_t cnt[Ctx::kMaxTileEvents];
+      for (int k = 0; k < g.ngrp; k++) {
+        const int t0 = g.grp_lo[k], t1 = g.grp_lo[k + 1];
+        cnt[k] = idx_b_r[t1 * rows - 1] - (t0 ? idx_b_r[t0 * rows - 1] : 0);
+        g.grp_order[k] = k;
+      }
+      std::stable_sort(g.grp_order, g.grp_order + g.ngrp, [&](int x, int y) { return cnt[x] > cnt[y]; });
+    }
+    // vp travels beside the deposit and FFTs, group by group in that order; its users wait for
+    // their part
+    for (int kk = 0; kk < g.ngrp; kk++) {
+      const int k = g.grp_order[kk];
       const int t0 = g.grp_lo[k], t1 = g.grp_lo[k + 1];
       const int64_t lo = t0 ? idx_b_r[t0 * rows - 1] : 0, hi = idx_b_r[t1 * rows - 1];
       if (hi > lo)
