@@ -528,7 +528,7 @@ def learned_variant(args, img, tables, stream, truth_plain, value_plain, ms_plai
         res["note"] = ("the sampled error exceeds the bound: the kick falls back to the plain cutoff-2 kick, "
                        "whose value is the line's value" if rms > LEARNED_BOUND else
                        "within the bound: the learned kick stands")
-        # the per-cell check: the full-cutoff kick judges the network cell by cell, and the cells
+        # the per-cell check: the network against the full-cutoff kick cell by cell, and the cells
         # over the bound take its velocities (cube_learned_fallback)
         try:
             res["per_cell_fallback"] = per_cell_fallback(args, img, tables, stream, kick, vp, vp0, Ft, samp, kc,
@@ -590,7 +590,7 @@ def per_cell_fallback(args, img, tables, stream, learned_kick, vp, vp0, Ft, samp
                                   "p99_rel": float(np.percentile(d / np.maximum(m, 1e-30), 99))},
             "ms_per_step": ms, "value": img.n_particles / (ms * 1e-3), "unit": UNIT,
             "speedup_vs_plain": ms_plain / ms,
-            "what": "learned kick + full-cutoff kick (the judge) + per-cell check and fallback, per step"}
+            "what": "learned kick + full-cutoff kick (the reference for the check) + per-cell check and fallback, per step"}
 
 
 def _batch_boxes(workload: str):

@@ -1,9 +1,9 @@
 // Per-cell check and fallback of the learned PP shell.  The learned kick (the cutoff-1 split plus
 // the network) and the full-cutoff kick (PM3 + PP at cutoff 2, the plain method) of one image
-// start from the same velocities; the full-cutoff kick judges the network.  Every coarse cell
-// that holds physical particles is checked on its first `samples` particles in storage order:
-// the relative rms difference of the two velocity changes over those particles, against the
-// bound.  A cell over the bound takes the full-cutoff velocities for all its particles; the
+// start from the same velocities; the full-cutoff kick is the reference for the network.  Every
+// coarse cell that holds physical particles is checked on its first `samples` particles in storage
+// order: the relative rms difference of the two velocity changes over those particles, against
+// the bound.  A cell over the bound takes the full-cutoff velocities for all its particles; the
 // other cells keep the learned ones.  No reference counterpart (the learned shell is new).
 //
 // One warp per interior coarse cell (tile, i, j, k): its particles are one contiguous run of

@@ -244,7 +244,7 @@ int cube_power_spectrum(const int32_t *d_rhoc, const int64_t *d_idx_b_r, const i
 /* Momentum and kinetic-energy change of the physical particles (the interior coarse cells of
  * every tile) between two velocity arrays of the same device image, typically vp before and
  * after a kick: out[0..2] = sum m (vb - va) per axis, out[3] = sum m/2 (|vb|^2 - |va|^2),
- * out[4..6] = sum |m (vb - va)| per axis (the scale against which out[0..2] is judged),
+ * out[4..6] = sum |m (vb - va)| per axis (the scale against which out[0..2] is measured),
  * out[7] = the number of physical particles.  Reduced in FP64 on the device; the call waits
  * for `stream`.  The reference prints sums of the same kind as its own invariants
  * ("sum of PM3 density", kick.f90:183; "sum of PP count", kick.f90:230). */
@@ -314,8 +314,8 @@ int cube_mlp_kick(cube_mlp *mlp, const int32_t *d_rhoc, const int64_t *d_idx_b_r
 /* The learned shell's per-cell check and fallback.  d_vp_learned and d_vp_full hold the
  * velocities after the learned kick (cutoff-1 split plus cube_mlp_kick) and after the
  * full-cutoff kick (the plain cube_kick_fine_device) of the same image, both from d_vp0.  The
- * full-cutoff kick judges the network: every coarse cell with physical particles is checked
- * on its first `samples` (1..32) particles in storage order, by the relative rms difference of
+ * full-cutoff kick is the reference for the network: every coarse cell with physical particles
+ * is checked on its first `samples` (1..32) particles in storage order, by the relative rms difference of
  * the two velocity changes there; a cell over `bound` takes the full-cutoff velocities for all
  * its particles, the others keep the learned ones.  d_vp_out (may be d_vp_learned) receives
  * the result.  out[0] = cells checked, out[1] = cells over the bound, out[2] = particles that
