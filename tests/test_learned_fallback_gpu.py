@@ -2,10 +2,9 @@
 
 The full-cutoff kick (PM3 + PP at cutoff 2, the plain method) is the reference for the
 network: every coarse cell with physical particles is checked on its first few particles, and
-a cell whose learned
-velocity change differs from the full-cutoff one by more than the bound (relative rms) is
-recomputed at cutoff 2, i.e. takes the full-cutoff velocities.  After the fallback every
-checked cell is within the bound.
+a cell whose learned velocity change differs from the full-cutoff one by more than the bound
+(relative rms) is recomputed at cutoff 2, i.e. takes the full-cutoff velocities.  After the
+fallback every checked cell is within the bound.
 """
 import numpy as np
 import pytest
