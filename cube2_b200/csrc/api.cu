@@ -1372,7 +1372,8 @@ int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32
   std::lock_guard<std::mutex> lk(g_mu);
   t_last_error = CUBE_OK;
   if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
-  if (!apm3 || !d_rhoc || !d_idx_b_r || !d_xp || !d_vp || !d_out) return fail(CUBE_ERR_INVALID);
+  // an image without particles may pass null particle arrays
+  if (!apm3 || !d_rhoc || !d_idx_b_r || !d_out || (n_used > 0 && (!d_xp || !d_vp))) return fail(CUBE_ERR_INVALID);
   if (n_used < 0 || n_used >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
   CK(ensure_device());
   cudaStream_t own = g.stream;
@@ -2015,7 +2016,7 @@ int cube_kick_graph_create(const int32_t *isort, const int32_t *ires, const int3
   if (!g.configured) return fail(CUBE_ERR_NOT_CONFIGURED);
   // the subtile geometry synchronises the host between mesh batches, which a graph cannot hold
   if (g.L.pm3_mode == CUBE_PM3_SUBTILE) return fail(CUBE_ERR_INVALID);
-  if (!apm3 || !d_rhoc || !d_idx_b_r || !d_xp || !d_vp || !d_out) return fail(CUBE_ERR_INVALID);
+  if (!apm3 || !d_rhoc || !d_idx_b_r || !d_out || (n_used > 0 && (!d_xp || !d_vp))) return fail(CUBE_ERR_INVALID);
   if (n_used < 0 || n_used >= ((int64_t)1 << 31)) return fail(CUBE_ERR_INVALID);
   CK(ensure_device());
   const float *gk[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -2023,7 +2024,9 @@ int cube_kick_graph_create(const int32_t *isort, const int32_t *ires, const int3
   {
     float *scratch = nullptr;
     CU(cudaMalloc(&scratch, sizeof(float) * 3 * (size_t)std::max<int64_t>(n_used, 1)));
-    cudaError_t e = cudaMemcpyAsync(scratch, d_vp, sizeof(float) * 3 * n_used, cudaMemcpyDeviceToDevice, g.stream);
+    cudaError_t e = n_used > 0 ? cudaMemcpyAsync(scratch, d_vp, sizeof(float) * 3 * n_used,
+                                                 cudaMemcpyDeviceToDevice, g.stream)
+                               : cudaSuccess;
     Meta m;
     Dev d{d_xp, d_rhoc, d_idx_b_r, scratch, n_used};
     int st = e == cudaSuccess ? run_kick(ires, ixyz3, ratio_sf, apm3, gk, d, mass, a_mid, dt, true, true, m)

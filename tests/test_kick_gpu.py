@@ -119,3 +119,67 @@ def test_host_kick_rejects_an_inconsistent_spine_and_recovers(gpu):
     got, out_got = fk.kick_fine(img, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0)
     d_w, d_g = (want - img.vp).astype(np.float64), (got - img.vp).astype(np.float64)
     assert np.sqrt(np.sum((d_g - d_w) ** 2) / np.sum(d_w ** 2)) < 1e-6
+
+
+def _device_kick(img, fk, tables):
+    import torch
+    dev = torch.device("cuda:0")
+    d_rhoc = torch.from_numpy(img.rhoc.reshape(-1).copy()).to(dev)
+    d_idx = torch.from_numpy(img.idx_b_r.reshape(-1).copy()).to(dev)
+    d_xp = torch.from_numpy(img.xp.reshape(-1).copy()).to(dev)
+    d_vp = torch.from_numpy(img.vp.reshape(-1).copy()).to(dev)
+    d_out = torch.zeros(8, dtype=torch.float32, device=dev)
+    fk.kick_fine_device(d_rhoc, d_idx, d_xp, img.n_used, d_vp, d_out, *tables, 1.0, SIXPI, 1.0)
+    torch.cuda.synchronize()
+    return d_vp.cpu().numpy().reshape(-1, 3), d_out.cpu().numpy()
+
+
+def test_periodic_kick_with_empty_tiles(gpu):
+    """Particles in the middle of two of the eight parent tiles only (more than a coarse cell
+    from every tile face, so no buffer copies either): the host kick's tile groups include
+    empty ones (nothing to copy, no PP items, bricks without particles), and it must equal the
+    device kick; PM3 alone equals the restatement."""
+    from cube2_b200 import ic
+    from cube2_b200.kick import CUBE_PM3_PERIODIC, FineKick
+    from cube2_b200.layout import Layout, build_image
+    from oracle import oracle as O
+    L = Layout(ng=32, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1)
+    a, va = ic.uniform_random(3000, 8.0, 21)
+    b, vb = ic.uniform_random(3000, 8.0, 22)
+    a = a + 4.0                             # tile (0, 0, 0)
+    b = b + np.array([20.0, 4.0, 20.0])     # tile (1, 0, 1)
+    img = build_image(np.concatenate([a, b]), np.concatenate([va, vb]), L)
+    idx = img.idx_b_r.reshape(8, -1)[:, -1]
+    assert list(np.diff(np.concatenate([[0], idx]))) == [3000, 0, 0, 0, 0, 3000, 0, 0]
+    fk = FineKick(L, pm3_mode=CUBE_PM3_PERIODIC, apm3f=4.0)
+    tables = _tables(L)
+    isort, ires, ix, apm3, rs = tables
+    vh, out_h = fk.kick_fine(img, isort, ires, ix, apm3, rs, 1.0, SIXPI, 1.0)
+    vd, out_d = _device_kick(img, fk, tables)
+    d_h, d_d = (vh - img.vp).astype(np.float64), (vd - img.vp).astype(np.float64)
+    assert np.sum(d_h ** 2) > 0
+    assert np.sqrt(np.sum((d_d - d_h) ** 2) / np.sum(d_h ** 2)) < 1e-6
+    np.testing.assert_allclose(out_d[:5], out_h, rtol=1e-5)
+    assert out_d[5:6].view(np.int32)[0] == 0
+    vp, f2, vmax, pt = fk.c_pm3_force_kernel(img, isort, ires, ix, rs, 1.0, SIXPI, 1.0)
+    ref = O.pm3_periodic(img, 2, O.green(L.ng * 2, 4.0, 0.0, 0.5), 1.0, SIXPI, 1.0)
+    act = img.active
+    dv, dr = (vp - img.vp)[act].astype(np.float64), (ref["vp"] - img.vp)[act].astype(np.float64)
+    assert np.sqrt(np.sum((dv - dr) ** 2) / np.sum(dr ** 2)) < 1e-5
+    assert abs(f2 - ref["f2max"]) <= 1e-5 * ref["f2max"]
+
+
+def test_periodic_kick_of_an_empty_image(gpu):
+    """No particles at all: the host and the device kick return zero maxima and no error."""
+    from cube2_b200.kick import CUBE_PM3_PERIODIC, FineKick
+    from cube2_b200.layout import Image, Layout
+    L = Layout(ng=32, nnt=2, nns=2, ratio_cs=4, ngb=4, app=0.1)
+    img = Image(L, np.zeros((0, 3), np.int16), np.zeros((0, 3), np.float32),
+                np.zeros((2, 2, 2, L.nte, L.nte, L.nte), np.int32), np.zeros((2, 2, 2, L.nte, L.nte), np.int64),
+                np.zeros(0, np.int64), np.zeros(0, bool), 0)
+    fk = FineKick(L, pm3_mode=CUBE_PM3_PERIODIC, apm3f=4.0)
+    tables = _tables(L)
+    vh, out_h = fk.kick_fine(img, *tables, 1.0, SIXPI, 1.0)
+    assert vh.size == 0 and np.all(out_h == 0)
+    vd, out_d = _device_kick(img, fk, tables)
+    assert np.all(out_d[:5] == 0) and out_d[5:6].view(np.int32)[0] == 0
