@@ -2,7 +2,7 @@
 //
 // Some callers cannot let a library call cudaMalloc: a driver that hands out
 // every byte of device memory through its own pool, a run under an
-// allocation-free capture or watchdog policy, or an embedding where the
+// allocation-free execution or watchdog policy, or an embedding where the
 // allocator belongs to another runtime.  cube_pp_force_noalloc serves them:
 // the caller passes device-resident inputs and outputs, and all the scratch the
 // PP kick needs (cell table, PP-cell counts and starts, sorted particles, work
@@ -13,8 +13,8 @@
 //
 // Host code cannot use the array's name as a device address (there it is only a
 // host-side stand-in), so the first call on each device looks the address up
-// with cudaGetSymbolAddress while that device is current; that first call
-// should therefore come before any stream capture.  All calls share the one
+// with cudaGetSymbolAddress while that device is current and keeps it for the
+// later calls on that device.  All calls share the one
 // array and it keeps the previous call's contents: the counters are cleared on
 // every call, and calls that overlap on the GPU (two streams, or two host
 // threads) race on it.

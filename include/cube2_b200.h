@@ -343,8 +343,8 @@ int cube_learned_fallback(const int32_t *d_rhoc, const int64_t *d_idx_b_r, int64
  * 2..4 and a device failure mask in word 5), and all scratch lives in a
  * file-scope device array.  Enqueued on `stream` (NULL = the default stream)
  * on the current device, without host synchronisation.
- * The first call on each device looks up the array's device address, so make
- * that first call before any stream capture.  Every call shares the array and
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) and keeps it.  Every call shares the array and
  * it keeps the previous call's contents (counters are reset by each call):
  * calls that overlap on the GPU race on it.  Returns CUBE_ERR_CAPACITY beyond
  * CUBE_NOALLOC_MAX_PARTICLES / CUBE_NOALLOC_MAX_CELLS, 64 tiles or 4096
