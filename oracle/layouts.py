@@ -67,6 +67,8 @@ GPU_BUILDS = {
     "t32b": _gpu_params(LAYOUTS["t32b"]),
     "cfg0": _gpu_params(LAYOUTS["cfg0"]),
     "c96": _gpu_params(LAYOUTS["c96"]),
+    # the bench's clustered256 image (2^3 tiles of 32^3 coarse cells): parity and timing at scale
+    "cfg1": _gpu_params(LAYOUTS["cfg1"]),
     # t32's image with one subtile per tile: the reference PM3 then solves one mesh of
     # (nt + 2) ratio_cs points per tile, the geometry of PM2 when ngb = ratio_cs
     "t32s1": _gpu_params(dict(LAYOUTS["t32"], nns=1)),

@@ -305,6 +305,46 @@ class RefCuda:
         out.update(vp=vp, f2max_pp=float(f2p[0]), vmax=vmax, ptotal_pp=ptp, seconds_pp=tt)
         return out
 
+    def kick_wall(self, img, isort, ires, ixyz3, apm3, ratio_sf, greens: dict, mass, a_mid, dt, vp):
+        """The two entry points as kick.f90:143-205 calls them (PM3, then PP, which applies the
+        PM3 change from the device accumulator), on the caller's host arrays; vp is kicked in
+        place.  Returns (seconds of c_pm3_force_kernel, seconds of c_pp_force_kernel), wall clock
+        around each call (each returns with its results on the host)."""
+        import time
+        L = img.layout
+        isort = np.ascontiguousarray(isort, dtype=np.int32)
+        ires = np.ascontiguousarray(ires, dtype=np.int32)
+        ixyz3 = np.ascontiguousarray(ixyz3, dtype=np.int32)
+        apm3 = np.ascontiguousarray(apm3, dtype=np.float32)
+        ratio_sf = np.ascontiguousarray(ratio_sf, dtype=np.int32)
+        self._check(img, ires, ixyz3)
+        if L.nns ** 3 > 64:
+            raise ValueError("more than 64 subtiles per parent tile")
+        if vp.dtype != np.float32 or not vp.flags.c_contiguous or vp.shape != img.vp.shape:
+            raise ValueError("vp must be a C-contiguous float32 array shaped like img.vp")
+        keep = [np.ascontiguousarray(greens[lev], dtype=np.float32) if greens.get(lev) is not None else None
+                for lev in range(2, 7)]
+        for lev in set(int(v) for v in ires.tolist()):
+            n = L.ntt * L.ratio_cs * int(ratio_sf[lev - 1]) + 2 * L.ratio_cs * int(ratio_sf[lev - 1])
+            if keep[lev - 2] is None or keep[lev - 2].size != n * n * (n // 2 + 1):
+                raise ValueError(f"level {lev} needs a Green table of {n}^2 x {n // 2 + 1}")
+        gk = [None if g is None else g.ctypes.data_as(_p) for g in keep]
+        f2 = np.zeros(1, np.float32)
+        vm = np.zeros(3, np.float32)
+        pt = np.zeros(L.ns3, np.float64)
+        tt = np.zeros(L.ns3, np.float64)
+        t0 = time.perf_counter()
+        self.lib.c_pm3_force_kernel(_ptr(isort), _ptr(ires), _ptr(ixyz3), _ptr(ratio_sf), _ptr(img.rhoc),
+                                    _ptr(img.idx_b_r), _ptr(img.xp), *gk, _ptr(vp), _c_f(mass), _c_f(a_mid),
+                                    _c_f(dt), _ptr(f2), _ptr(vm), _ptr(pt))
+        t1 = time.perf_counter()
+        self.lib.c_pp_force_kernel(_ptr(isort), _ptr(ires), _ptr(ixyz3), _ptr(apm3), _ptr(ratio_sf),
+                                   _ptr(img.rhoc), _ptr(img.idx_b_r), _ptr(img.xp), _ptr(vp), _c_f(mass),
+                                   _c_f(a_mid), _c_f(dt), _ptr(f2), _ptr(vm), _ptr(pt), _ptr(tt))
+        t2 = time.perf_counter()
+        del keep
+        return t1 - t0, t2 - t1
+
     def finalize(self):
         self.lib.c_gpu_velocity_finalize()
         self.lib.c_pm3_fft_finalize()
