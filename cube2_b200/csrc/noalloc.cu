@@ -14,7 +14,8 @@
 // Host code cannot use the array's name as a device address (there it is only a
 // host-side stand-in), so the first call on each device looks the address up
 // with cudaGetSymbolAddress while that device is current and keeps it for the
-// later calls on that device.  All calls share the one
+// later calls on that device; that first call belongs before any stream capture
+// begins.  All calls share the one
 // array and it keeps the previous call's contents: the counters are cleared on
 // every call, and calls that overlap on the GPU (two streams, or two host
 // threads) race on it.

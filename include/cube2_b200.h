@@ -344,7 +344,8 @@ int cube_learned_fallback(const int32_t *d_rhoc, const int64_t *d_idx_b_r, int64
  * file-scope device array.  Enqueued on `stream` (NULL = the default stream)
  * on the current device, without host synchronisation.
  * The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress) and keeps it.  Every call shares the array and
+ * (cudaGetSymbolAddress) and keeps it; make that first call before any stream
+ * capture begins.  Every call shares the array and
  * it keeps the previous call's contents (counters are reset by each call):
  * calls that overlap on the GPU race on it.  Returns CUBE_ERR_CAPACITY beyond
  * CUBE_NOALLOC_MAX_PARTICLES / CUBE_NOALLOC_MAX_CELLS, 64 tiles or 4096
