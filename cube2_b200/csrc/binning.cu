@@ -105,9 +105,23 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t wid = (int64_t)blockIdx.x * kWarps + warp;
   if (wid >= (int64_t)p.t_n * p.R3) return;
-  const int t = p.t_lo + (int)(wid / p.R3);
-  int64_t rem = wid - (int64_t)(t - p.t_lo) * p.R3;
-  const int cx = (int)(rem % p.R), cy = (int)((rem / p.R) % p.R), cz = (int)(rem / ((int64_t)p.R * p.R));
+  // tile and region cell of this warp, in 32-bit arithmetic when the launch's warps fit
+  // (64-bit division is a long software sequence)
+  int t, cx, cy, cz;
+  if ((int64_t)p.t_n * p.R3 <= 0xffffffffLL) {
+    const unsigned w = (unsigned)wid, R = (unsigned)p.R, R3 = (unsigned)p.R3;
+    const unsigned tq = w / R3, rem = w - tq * R3, q = rem / R, qq = q / R;
+    t = p.t_lo + (int)tq;
+    cx = (int)(rem - q * R);
+    cy = (int)(q - qq * R);
+    cz = (int)qq;
+  } else {
+    t = p.t_lo + (int)(wid / p.R3);
+    const int64_t rem = wid - (int64_t)(t - p.t_lo) * p.R3;
+    cx = (int)(rem % p.R);
+    cy = (int)((rem / p.R) % p.R);
+    cz = (int)(rem / ((int64_t)p.R * p.R));
+  }
   const TilePP tp = p.tiles[t];
   const int rcp = tp.rcp, S = tp.S, rcp3 = rcp * rcp * rcp;
   int32_t *hist = sh_hist + warp * p.hist_words;
@@ -162,7 +176,13 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
     }
   };
 
-  for (int q = lane; q < nbins; q += 32) hist[q] = 0;
+  // zero the bins four words at a time (the warp's histogram is 16-byte aligned and at least
+  // 1024 words long, so rounding nbins up to a multiple of four stays inside it)
+  auto zero_bins = [&]() {
+    int4 *h4 = reinterpret_cast<int4 *>(hist);
+    for (int q = lane; q < (nbins + 3) / 4; q += 32) h4[q] = make_int4(0, 0, 0, 0);
+  };
+  zero_bins();
   __syncwarp();
 
   if (spatial) {
@@ -179,20 +199,45 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
       }
     }
     __syncwarp();
-    for (int b = 0; b < rcp3; b++) {  // s3 <= 64 bins per PP sub-cell: two per lane
-      const int q0 = b * s3 + 2 * lane;
-      const int v0 = 2 * lane < s3 ? hist[q0] : 0, v1 = 2 * lane + 1 < s3 ? hist[q0 + 1] : 0;
-      int incl = v0 + v1;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += u;
+    // exclusive prefix of the bins inside each PP sub-cell: the 512 bins (rcp^3 sub-cells of
+    // s3 bins, rcp 2 or 4) are 16 per lane; s3 = 8 restarts twice inside a lane, s3 = 64 spans
+    // four lanes, which a scan over groups of four lanes joins
+    {
+      const int4 *h4 = reinterpret_cast<const int4 *>(hist) + 4 * lane;
+      int4 *p4 = reinterpret_cast<int4 *>(pre) + 4 * lane;
+      int v[16];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int4 u = h4[j];
+        v[4 * j] = u.x;
+        v[4 * j + 1] = u.y;
+        v[4 * j + 2] = u.z;
+        v[4 * j + 3] = u.w;
       }
-      const int ex = incl - v0 - v1;
-      if (2 * lane < s3) pre[q0] = ex;
-      if (2 * lane + 1 < s3) pre[q0 + 1] = ex + v0;
+      int run = 0;
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        if (s3 == 8 && j == 8) run = 0;
+        const int c = v[j];
+        v[j] = run;
+        run += c;
+      }
+      if (s3 == 64) {
+        int incl = run;
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+          const int u = __shfl_up_sync(0xffffffffu, incl, o, 4);
+          if ((lane & 3) >= o) incl += u;
+        }
+        const int off = incl - run;
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[j] += off;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++) p4[j] = make_int4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
     }
     __syncwarp();
-    for (int q = lane; q < nbins; q += 32) hist[q] = 0;
+    zero_bins();
     __syncwarp();
   }
 

@@ -322,7 +322,19 @@ __global__ void __launch_bounds__(256) k_pp_items(PPK p) {
   int64_t g = 0;
   PPItem it{};
   if (c < ncell) {
-    const int x = (int)(c % npg) + rcp, y = (int)((c / npg) % npg) + rcp, z = (int)(c / ((int64_t)npg * npg)) + rcp;
+    // cell coordinates in 32-bit arithmetic when the tile's cells fit (64-bit division is a long
+    // software sequence)
+    int x, y, z;
+    if (ncell <= 0xffffffffLL) {
+      const unsigned u = (unsigned)c, n = (unsigned)npg, q = u / n, qq = q / n;
+      x = (int)(u - q * n) + rcp;
+      y = (int)(q - qq * n) + rcp;
+      z = (int)qq + rcp;
+    } else {
+      x = (int)(c % npg) + rcp;
+      y = (int)((c / npg) % npg) + rcp;
+      z = (int)(c / ((int64_t)npg * npg)) + rcp;
+    }
     g = tp.cell0 + ((int64_t)z * S + y) * S + x;
     i0 = p.cs[g];
     ni = p.cs[g + 1] - i0;
