@@ -185,18 +185,36 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
   zero_bins();
   __syncwarp();
 
+  // Spill-free spatial placement: the histogram pass keeps the bin and float position of its
+  // first kCache x 32 particles in registers and the placement pass reuses them, so those
+  // particles are classified once (a bad key was already flagged by the counting pass).
+  constexpr int kCache = 4;
+  int cbin[kCache];
+  float cpx[kCache], cpy[kCache], cpz[kCache];
+  const bool cached = spatial && nspill == 0;
   if (spatial) {
     // histogram of the bins, then an exclusive prefix per PP sub-cell
-    for (int l0 = 0; l0 < np; l0 += 32) {
-      const int l = l0 + lane;
-      if (l < np) {
-        float x, y, z;
-        bool spilled, bad;
-        int b, bin;
-        int64_t gkey;
-        classify(l, x, y, z, spilled, bad, b, bin, gkey);
-        if (!spilled && !bad) atomicAdd(&hist[bin], 1);
+    auto hist_one = [&](int l, int &bin_home, float &x, float &y, float &z) {
+      bool spilled, bad;
+      int b, bin;
+      int64_t gkey;
+      classify(l, x, y, z, spilled, bad, b, bin, gkey);
+      bin_home = -1;
+      if (!spilled && !bad) {
+        atomicAdd(&hist[bin], 1);
+        bin_home = bin;
       }
+    };
+#pragma unroll
+    for (int it = 0; it < kCache; it++) {
+      cbin[it] = -1;
+      cpx[it] = cpy[it] = cpz[it] = 0.f;
+      if (it * 32 + lane < np) hist_one(it * 32 + lane, cbin[it], cpx[it], cpy[it], cpz[it]);
+    }
+    for (int l = kCache * 32 + lane; l < np; l += 32) {
+      int bh;
+      float x, y, z;
+      hist_one(l, bh, x, y, z);
     }
     __syncwarp();
     // exclusive prefix of the bins inside each PP sub-cell: the 512 bins (rcp^3 sub-cells of
@@ -241,7 +259,41 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_bin(BinK p) {
     __syncwarp();
   }
 
-  for (int l0 = 0; l0 < np; l0 += 32) {
+  int lstart = 0;
+  if (cached) {
+    const int bsh = rcp == 2 ? 6 : 3;  // log2 of the bins per PP sub-cell (rcp is 2 or 4)
+    const int lr = rcp >> 1;            // log2 rcp
+    const int64_t gbase = tp.cell0 + ((int64_t)(rcp * cz) * S + rcp * cy) * S + rcp * cx;
+#pragma unroll
+    for (int it = 0; it < kCache; it++) {
+      if (it * 32 < np) {  // the same for the whole warp
+        const int bin = cbin[it];
+        const bool home = bin >= 0;
+        const unsigned hm = __ballot_sync(0xffffffffu, home);
+        int hb = 0, rank = 0;
+        unsigned peers = 0;
+        if (home) {
+          peers = __match_any_sync(hm, bin);
+          rank = __popc(peers & ((1u << lane) - 1u));
+          hb = hist[bin] + pre[bin];
+        }
+        __syncwarp();
+        if (home) {
+          // the PP cell key of the counting pass, from the sub-cell b of this coarse cell
+          const int b = bin >> bsh, rx = b & (rcp - 1), ry = (b >> lr) & (rcp - 1), rz = b >> (2 * lr);
+          const int64_t gkey = gbase + ((int64_t)rz * S + ry) * S + rx;
+          const int64_t pos = (int64_t)p.cell_start[gkey] + hb + rank;
+          p.spos[pos] = make_float4(__fmul_rn((float)p.rcs, cpx[it]), __fmul_rn((float)p.rcs, cpy[it]),
+                                    __fmul_rn((float)p.rcs, cpz[it]), __int_as_float((int)(base + it * 32 + lane)));
+          if (rank == 0) hist[bin] += __popc(peers);
+        }
+        __syncwarp();
+      }
+    }
+    lstart = kCache * 32;
+  }
+
+  for (int l0 = lstart; l0 < np; l0 += 32) {
     const int l = l0 + lane;
     const bool valid = l < np;
     bool spilled = false, bad = false;

@@ -406,8 +406,9 @@ __device__ __forceinline__ int64_t brick_particle(int k, const BrickRows &br, co
   int i = 0;
   while (i + 1 < br.cb && rcell[lo * (kMaxCb + 1) + i + 1] <= l) i++;
   di = i;
-  dj = lo % br.cb;
-  dk = lo / br.cb;
+  // cb is 1, 2 or 4 (a brick side of 16 mesh points, at least 4 mesh points per coarse cell)
+  dj = lo & (br.cb - 1);
+  dk = lo >> (br.cb >> 1);
   return rbase[lo] + l;
 }
 
