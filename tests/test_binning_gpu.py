@@ -31,10 +31,17 @@ def test_binning_matches_reference_golden(gpu, case):
                       z[f"t{t}_ip_local"])
 
 
+def _spread2(v):
+    """Bits 0 and 1 of v to bits 0 and 3 (one axis of a 2-bit-per-axis Morton index)."""
+    return (v & 1) | ((v & 2) << 2)
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_kick_order_is_a_within_cell_permutation(gpu, case):
     """The kick's spatial order keeps the reference keys and cell_start bit for bit and only
-    permutes particles inside each PP cell (Morton sub-cell, then storage slot)."""
+    permutes particles inside each PP cell, into the order of their Morton sub-cell, then
+    storage slot (t32_edge's crowded coarse cell of 300 particles also covers the particles
+    past the first 128, which the placement pass classifies again)."""
     from cube2_b200.kick import FineKick
     from cube2_b200.layout import RATIO_SF, ixyz3_table
     img, z = load_golden(case)
@@ -42,6 +49,8 @@ def test_kick_order_is_a_within_cell_permutation(gpu, case):
     fk = FineKick(L)
     ires = np.full(L.ns3, 2, np.int32)
     ix = ixyz3_table(L)
+    rcp = int(RATIO_SF[1])  # PP cells per coarse cell at level 2; the space order needs 2 or 4
+    assert rcp in (2, 4)
     for t in range(L.nnt ** 3):
         ref = fk.pp_bin_tile(img, t, ires, ix, RATIO_SF, spatial=False)
         sp = fk.pp_bin_tile(img, t, ires, ix, RATIO_SF, spatial=True)
@@ -55,6 +64,11 @@ def test_kick_order_is_a_within_cell_permutation(gpu, case):
             order_s = np.argsort(sp["ip"][a:b])
             order_r = np.argsort(ref["ip"][a:b])
             np.testing.assert_array_equal(sp["xf"][:, a:b][:, order_s], ref["xf"][:, a:b][:, order_r])
+            # inside the cell: Morton index of the 1/8-coarse-cell sub-cell, then storage slot
+            x = sp["xf"][:, a:b].astype(np.float64) / L.ratio_cs  # coarse-cell units, exact
+            f = np.clip(np.floor(8 * x) - 8 * np.floor(x), 0, 7).astype(np.int64) & (8 // rcp - 1)
+            m = _spread2(f[0]) | (_spread2(f[1]) << 1) | (_spread2(f[2]) << 2)
+            assert np.all(np.diff(m * (1 << 40) + sp["ip"][a:b]) > 0)
 
 
 def test_binning_zeldovich_box_matches_reference(gpu):
