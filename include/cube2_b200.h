@@ -128,7 +128,8 @@ int cube_kick_fine(const int32_t *isort, const int32_t *ires, const int32_t *ixy
  * of device memory) receives the 5 floats of cube_kick_fine and, in word 5,
  * an int32 mask of device-side failures (bit CUBE_ERR_CAPACITY or
  * CUBE_ERR_INVALID; 0 = none) when the stream reaches it.  The small host
- * tables are read during the call. */
+ * tables are read during the call.  d_xp and d_vp may be NULL when n_used is 0
+ * (an image without particles). */
 int cube_kick_fine_device(const int32_t *isort, const int32_t *ires, const int32_t *ixyz3, const float *apm3,
                           const int32_t *ratio_sf, const int32_t *d_rhoc, const int64_t *d_idx_b_r,
                           const int16_t *d_xp, int64_t n_used, const float *const gk[5], float *d_vp, float mass,
