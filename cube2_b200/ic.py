@@ -50,7 +50,8 @@ def zeldovich_lattice(n: int, rms_disp: float, seed: int, slope: float = -2.0):
         psi.append(comp)
     psi = np.stack(psi, axis=-1)  # [z,y,x,3] components (x,y,z)
     rms = np.sqrt(np.mean(np.sum(psi * psi, axis=-1)))
-    psi *= rms_disp / rms
+    if rms > 0:  # a 2^3 lattice carries no displacement (only Nyquist modes): it stays a lattice
+        psi *= rms_disp / rms
     g = np.arange(n) + 0.5
     zz, yy, xx = np.meshgrid(g, g, g, indexing="ij")
     base = np.stack([xx, yy, zz], axis=-1)
