@@ -27,7 +27,7 @@ def gaussian_field(n: int, slope: float, rng: np.random.Generator) -> np.ndarray
     amp = np.zeros_like(k2)
     nz = k2 > 0
     amp[nz] = k2[nz] ** (slope / 4.0)
-    f = np.fft.irfftn(wk * amp, s=(n, n, n))
+    f = np.fft.irfftn(wk * amp, s=(n, n, n), axes=(0, 1, 2))
     f -= f.mean()
     return f / f.std()
 
@@ -46,7 +46,7 @@ def zeldovich_lattice(n: int, rms_disp: float, seed: int, slope: float = -2.0):
     k2[0, 0, 0] = 1.0
     psi = []
     for kc in (kx, ky, kz):
-        comp = np.fft.irfftn(1j * kc * dk / k2 * (n / (2 * np.pi)), s=(n, n, n))
+        comp = np.fft.irfftn(1j * kc * dk / k2 * (n / (2 * np.pi)), s=(n, n, n), axes=(0, 1, 2))
         psi.append(comp)
     psi = np.stack(psi, axis=-1)  # [z,y,x,3] components (x,y,z)
     rms = np.sqrt(np.mean(np.sum(psi * psi, axis=-1)))
