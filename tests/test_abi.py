@@ -164,3 +164,33 @@ def test_device_kick_pointer_checks_without_device(cube_lib):
     assert call(None, 5, _p(out)) == 1
     assert call(_p(img.xp), 5, None) == 1
     assert call(_p(img.xp), -1, _p(out)) == 1
+
+
+def test_graph_create_pointer_checks_without_device(cube_lib):
+    """cube_kick_graph_create applies the same pointer checks as the device kick it captures."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from cube2_b200.kick import CUBE_PM3_PERIODIC, FineKick, _p
+    from cube2_b200.layout import RATIO_SF, apm3_table, ixyz3_table
+    img, _ = load_golden("t32")
+    L = img.layout
+    FineKick(L, pm3_mode=CUBE_PM3_PERIODIC)
+    isort = np.arange(1, L.ns3 + 1, dtype=np.int32)
+    ires = np.full(L.ns3, 2, np.int32)
+    ix = np.ascontiguousarray(ixyz3_table(L), np.int32)
+    apm3, rs = apm3_table(4.0), RATIO_SF.copy()
+    out = np.zeros(8, np.float32)  # stands in for device memory: the checks only test for NULL
+
+    def call(xp, n_used, vp):
+        h = ctypes.c_void_p()
+        st = cube_lib.cube_kick_graph_create(_p(isort), _p(ires), _p(ix), _p(apm3), _p(rs), _p(img.rhoc),
+                                             _p(img.idx_b_r), xp, ctypes.c_int64(n_used), vp,
+                                             ctypes.c_float(1.0), ctypes.c_float(1.0), ctypes.c_float(1.0),
+                                             _p(out), ctypes.byref(h))
+        assert not h.value  # no graph on failure
+        return st
+
+    assert call(None, 0, None) in (3, 6)  # past the checks, no device
+    assert call(None, 5, _p(out)) == 1
+    assert call(_p(img.xp), 5, None) == 1
