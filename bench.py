@@ -118,18 +118,27 @@ class Clocks:
         except subprocess.TimeoutExpired:
             self.proc.kill()
             out, _ = self.proc.communicate()
+        return self.summarize(self.lines[1:] + out.splitlines(), self.uuid)  # the first sample predates the region
+
+    @classmethod
+    def summarize(cls, lines, uuid: str | None = None):
+        """Median SM clock, max SM clock and the throttle reasons seen active, from the sampler's
+        CSV lines (FIELDS order) of the GPU `uuid` (all GPUs when None); None without samples."""
         rows = []
-        for ln in self.lines[1:] + out.splitlines():  # the first sample predates the timed region
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
-            if self.uuid and f[0] != self.uuid:
+            if uuid and f[0] != uuid:
                 continue
             rows.append(f)
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+
+        def num(v):
+            return v.replace(".", "", 1).isdigit()
+        sm = [float(r[1]) for r in rows if num(r[1])]
+        smax = max((float(r[2]) for r in rows if num(r[2])), default=None)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": reasons,
